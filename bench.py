@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the ADMIXTURE hot path on B200: one step = one quasi-Newton iteration of
+admixture_qn! (2 Q + 2 P SQP updates, 2 log-likelihood passes, ZAL extrapolation,
+accept/reject) over a seeded synthetic cohort.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2] [--impl ours|reference]
+
+Metric: genotype*K^2/s per iteration (I*J*K^2 / seconds per iteration), whole job.  Also
+reported: time-to-converge from the EM-primed start (rtol 1e-7), per-pass device times, the
+roofline of the dominant kernel, an end-to-end number through the C ABI with host buffers,
+and the oracle (CPU restatement) timed on the host cores.
+
+Multi-GPU (torchrun): every rank solves its own cohort (seed = rank) -- independent problems,
+no collective on the data path; timing is the max over ranks (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "oracle"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+METRIC = "genotype*K^2/s per iteration (plain FP64 form, 1 B200)"
+UNIT = "genotype*K^2/s"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ttc", action="store_true")
+    return ap.parse_args()
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _traffic(kernel: str, config: str):
+    """DRAM bytes per launch from a committed ncu summary (profiles/traffic.txt), if any."""
+    f = ROOT / "profiles" / "traffic.txt"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.startswith("#") or "=" not in ln:
+            continue
+        kv = dict(x.split("=", 1) for x in ln.split())
+        if kv.get("kernel") == kernel and kv.get("config") == config:
+            return float(kv["dram_bytes_per_launch"])
+    return None
+
+
+def _cpu_sample_spec(oa, spec, J_sample):
+    return spec.scaled(J=J_sample)
+
+
+def cpu_baseline(oa, spec, steps=2):
+    """The oracle (C restatement, OpenMP on all host cores) on a bounded SNP sample of the
+    same cohort: QN iterations from an EM-primed start, metric scaled by the sample."""
+    import oracle
+    J_s = max(500, min(spec.J, 20000))
+    s = _cpu_sample_spec(oa, spec, J_s)
+    g, _, _ = oa.make_cohort(s)
+    x0 = oa.init_x(s.I, s.J, s.K, 5)
+    r = oracle.OracleRun(g.data, s.I, s.J, s.K, 3, x0)
+    r.init_em(1)
+    times = []
+    for it in range(1, steps + 1):
+        t0 = time.perf_counter()
+        r.qn_iteration(it)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    return {"value": s.I * s.J * s.K ** 2 / t, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"oracle admixture_qn iteration on I={s.I}, J={s.J} (SNP subset), K={s.K}; "
+                      f"median of {steps} iteration(s), {t:.2f} s each"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import oracle
+    import openadmixture_b200 as oa
+    spec = oa.COHORTS[args.config]
+    J_s = max(500, min(spec.J, 4000))
+    s = spec.scaled(J=J_s)
+    g, _, _ = oa.make_cohort(s)
+    r = oracle.OracleRun(g.data, s.I, s.J, s.K, 3, oa.init_x(s.I, s.J, s.K, 5))
+    r.init_em(1)
+    it = 0
+    for _ in range(args.warmup):
+        it += 1
+        r.qn_iteration(it)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        it += 1
+        r.qn_iteration(it)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = s.I * s.J * s.K ** 2 / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{spec.name}: I={spec.I} J={spec.J} K={spec.K} (timed on a SNP subset J={J_s})",
+                   "I": spec.I, "J": spec.J, "K": spec.K},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+                         "sample": f"oracle (C restatement of the Julia loops; Julia is not installed) "
+                                   f"QN iterations on I={s.I}, J={J_s}, K={s.K}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import openadmixture_b200 as oa
+    from openadmixture_b200 import _native as N
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    spec = oa.COHORTS[args.config].scaled(seed=rank)
+    t0 = time.perf_counter()
+    g, _, _ = oa.make_cohort(spec)
+    t_gen = time.perf_counter() - t0
+    d = oa.AdmixData(spec.I, spec.J, spec.K, 3, rng=100 + rank)
+    x_init = d.x.copy()
+    t0 = time.perf_counter()
+    d_cu = oa.CuAdmixData(d, g)
+    t_upload = time.perf_counter() - t0
+    oa.init_em(d, g, 5, d_cu=d_cu, quiet=True)
+    x_em, ll_em = d.x.copy(), d.ll_new
+    d_cu.upload(oa.X, x_em)
+    d_cu.set_ll(ll_em)
+    lib = N.admix_lib()
+    stream = torch.cuda.ExternalStream(d_cu.stream())
+    info = N.IterInfo()
+    it = 0
+    for _ in range(args.warmup):
+        it += 1
+        d_cu._chk(lib.admix_qn_iteration(d_cu.handle, it, C_byref(info)))
+    n_kern = d_cu.iteration_kernels()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        it += 1
+        d_cu._chk(lib.admix_qn_iteration(d_cu.handle, it, C_byref(info)))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    work = spec.I * spec.J * spec.K ** 2
+    value = world * work * args.steps / (ms_max / 1e3)
+
+    # per-pass device times (live, CUDA events on the engine's stream)
+    passes = {}
+    for name, pid in (("loglik", N.ADMIX_PASS_LOGLIK), ("q_sweep", N.ADMIX_PASS_QSWEEP),
+                      ("p_sweep", N.ADMIX_PASS_PSWEEP), ("q_qp", N.ADMIX_PASS_QQP), ("p_qp", N.ADMIX_PASS_PQP)):
+        passes[name] = d_cu.time_pass(pid, 5)
+    per_iter = {k: 2 * v for k, v in passes.items()}
+    dom = max(per_iter, key=per_iter.get)
+    kern_name = {"loglik": "k_loglik_f64", "q_sweep": "k_sweep_q_f64", "p_sweep": "k_sweep_p_f64",
+                 "q_qp": "k_qp", "p_qp": "k_qp"}[dom]
+    Ib = (spec.I + 3) // 4
+    K = spec.K
+    bytes_bed = Ib * spec.J
+    # algorithmic bytes per launch: the packed genotypes + the Q/P inputs + outputs
+    alg_bytes = {
+        "loglik": bytes_bed + 8 * K * (spec.I + spec.J),
+        "q_sweep": bytes_bed + 8 * K * (spec.I + spec.J) + 8 * (K * (K + 1) // 2 + K) * spec.I,
+        "p_sweep": bytes_bed + 8 * K * (spec.I + spec.J) + 8 * (K * (K + 1) // 2 + K) * spec.J,
+        "q_qp": 8 * (K * (K + 1) // 2 + 2 * K) * spec.I + 8 * K * spec.I,
+        "p_qp": 8 * (K * (K + 1) // 2 + 2 * K) * spec.J + 8 * K * spec.J,
+    }
+    flops = {   # reference full-K^2 form (cell counts x ops), for context
+        "q_sweep": 2 * spec.I * spec.J * (2 * K * K + 2 * K) + 2 * spec.I * spec.J * K,
+        "p_sweep": 2 * spec.I * spec.J * (K * K + K) + 2 * spec.I * spec.J * K,
+        "loglik": 2 * spec.I * spec.J * K,
+    }
+    hbm, bf16, peak_kind = _peaks()
+    achieved = alg_bytes[dom] / (passes[dom] / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": kern_name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_kind": peak_kind,
+            "traffic": _traffic(kern_name, spec.name),
+            "alg_bytes_per_launch": alg_bytes[dom], "launch_ms": passes[dom]}
+    if dom in flops:
+        roof["fp64_tflops"] = flops[dom] / (passes[dom] / 1e3) / 1e12
+    roof["note"] = ("FP64 plain form: the sweep is bound by the FP64 pipe, not HBM; frac is the HBM "
+                    "fraction of its packed-genotype stream")
+
+    # end-to-end through the C ABI with host buffers (pinned), H2D + D2H inside the timed region
+    qh = torch.from_numpy(np.ascontiguousarray(x_em[: spec.I])).pin_memory()
+    ph = torch.from_numpy(np.ascontiguousarray(x_em[spec.I:])).pin_memory()
+    qo = torch.empty_like(qh).pin_memory(); po = torch.empty_like(ph).pin_memory()
+    import ctypes as C
+    dp = lambda t_: C.cast(C.c_void_p(t_.data_ptr()), C.POINTER(C.c_double))
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True); f1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, args.steps // 2)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        it += 1
+        d_cu._chk(lib.admix_set_x(d_cu.handle, oa.X, dp(qh), dp(ph)))
+        d_cu._chk(lib.admix_qn_iteration(d_cu.handle, it, C_byref(info)))
+        d_cu._chk(lib.admix_get_x(d_cu.handle, oa.X, dp(qo), dp(po)))
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1) / e2e_steps
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te.item())
+    xbytes = 8 * K * (spec.I + spec.J)
+
+    # time to converge from the EM-primed start (rtol 1e-7)
+    ttc = None
+    if not args.no_ttc:
+        d_cu.upload(oa.X, x_em)
+        d_cu.set_ll(ll_em)
+        hist = (N.IterInfo * 1000)()
+        n_done = C.c_int32(); conv = C.c_int32()
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True); g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        d_cu._chk(lib.admix_run_qn(d_cu.handle, 1000, 1e-7, 0, hist, C.byref(n_done), C.byref(conv)))
+        g1.record(stream)
+        torch.cuda.synchronize()
+        ttc = {"seconds": g0.elapsed_time(g1) / 1e3, "iterations": n_done.value, "converged": bool(conv.value),
+               "final_ll": hist[n_done.value - 1].ll_new if n_done.value else None,
+               "from": "5 EM iterations (not timed)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(oa, spec)
+
+    d_cu.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{spec.name}: admixture_qn iteration, I={spec.I} J={spec.J} K={spec.K}, "
+                               f"{spec.miss:.1%} missing, plain FP64 form",
+                   "I": spec.I, "J": spec.J, "K": spec.K, "Q": 3, "form": "plain-fp64",
+                   "l2": f"inputs larger than L2: {bytes_bed / 1e6:.0f} MB packed genotypes streamed per pass",
+                   "per_rank": "independent cohort per rank (seed = rank)"},
+        "e2e": {"value": world * work / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": xbytes,
+                "d2h_bytes_per_step": xbytes + 0, "ms_per_step": e2e_ms,
+                "path": "admix_set_x(host q,p) + admix_qn_iteration + admix_get_x(host q,p)"},
+        "gpu_launches": n_kern * args.steps,
+        "roofline": roof,
+        "passes_ms": passes,
+        "ttc": ttc,
+        "setup_s": {"generate": t_gen, "create_upload": t_upload},
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def C_byref(x):
+    import ctypes
+    return ctypes.byref(x)
+
+
+def main():
+    args = _args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

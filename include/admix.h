@@ -1,0 +1,169 @@
+/*
+ * admix.h -- C ABI of libadmix, the B200 (sm_100a) engine for OpenADMIXTURE.jl's
+ * per-iteration likelihood / gradient / Hessian sweeps, block SQP updates and ZAL
+ * quasi-Newton extrapolation.
+ *
+ * Plain C types only (pointers, sizes, status codes); one opaque handle per cohort.
+ * Every entry point is synchronous: work is stream-ordered on the handle's stream and
+ * the call returns after cudaStreamSynchronize (the reference wraps each GPU call in
+ * CUDA.@sync, cuda/runners.jl:8,30,54,77,99).  A handle is not re-entrant; use one per
+ * host thread.  Every call returns ADMIX_OK (0) or an error code, and the message is
+ * available from admix_last_error().
+ *
+ * Array layout is the reference's (Julia column-major, structs.jl:16-43):
+ *   bed : uint8 [ceil(I/4)] x J, SNP-major, PLINK 2-bit codes, no 3-byte magic
+ *         (the SnpArray data matrix g_la.s.data, cuda/structs.jl:37)
+ *   q   : K x I doubles,  p : K x J doubles   (x = [q p], K x (I+J))
+ *   XtX : K x K x n doubles, Xtz : K x n doubles (n = I for the Q block, J for the P block)
+ */
+#ifndef ADMIX_H
+#define ADMIX_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define ADMIX_OK               0
+#define ADMIX_ERR_ARG          1   /* bad argument (the reference raises AssertionError) */
+#define ADMIX_ERR_CUDA         2   /* CUDA runtime error */
+#define ADMIX_ERR_NOMEM        3   /* device allocation failed */
+#define ADMIX_ERR_UNSUPPORTED  4   /* size or option outside what the library supports */
+#define ADMIX_ERR_STATE        5   /* call made in the wrong state */
+
+/* buffer selectors: the reference's x, x_next, x_next2, x_tmp (structs.jl:16-19) */
+#define ADMIX_X        0
+#define ADMIX_X_NEXT   1
+#define ADMIX_X_NEXT2  2
+#define ADMIX_X_TMP    3
+
+/* admix_create flags */
+#define ADMIX_FLAG_MU_GERSHGORIN  1u  /* simplex tableau adds the Gerschgorin mu of qp.jl:54-58
+                                          (default: mu = 0, what the aliased mul! yields) */
+#define ADMIX_FLAG_MIXED          2u  /* mixed-precision form of the Q/P sweeps */
+
+#define ADMIX_MAX_K 16
+#define ADMIX_MAX_Q 8
+
+typedef struct admix_ctx admix_ctx;
+
+/* One quasi-Newton iteration's record (what algorithms_outer.jl:161-164 prints). */
+typedef struct {
+    double ll_prev;     /* log-likelihood before the iteration */
+    double ll_basic;    /* after two SQP sweeps (x_next2) */
+    double ll_qn;       /* at the projected quasi-Newton point (x_tmp) */
+    double ll_new;      /* accepted value */
+    double reldiff;     /* |ll_new - ll_prev| / |ll_prev| */
+    int32_t iter;       /* iteration number i */
+    int32_t accepted_qn;/* 1 when x_tmp was accepted */
+    int32_t qp_fail_q;  /* simplex QPs that returned 0 (qp.jl:192,202,291) over both Q updates */
+    int32_t qp_fail_p;  /* box QPs that returned 0 over both P updates */
+} admix_iterinfo;
+
+/* --- lifetime ------------------------------------------------------------------ */
+
+/* Allocate the device state and upload the genotype bytes once.
+ * Replaces _cu_admixture_base / CuAdmixData (cuda/structs.jl:16-39, driver.jl:150-155).
+ * K in [1, ADMIX_MAX_K], Q in [1, ADMIX_MAX_Q]. */
+int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
+                 uint32_t flags, admix_ctx **out);
+int admix_destroy(admix_ctx *h);
+/* Last error message of h (or of the calling thread's last failed admix_create when h is NULL). */
+const char *admix_last_error(const admix_ctx *h);
+/* Device bytes held by the handle. */
+int admix_device_bytes(const admix_ctx *h, int64_t *bytes);
+
+/* --- state transfer (copyto_sync!, cuda/transfer.jl:1-7) ------------------------ */
+
+/* Upload / download q (K x I) and p (K x J) of buffer `which`; either pointer may be NULL. */
+int admix_set_x(admix_ctx *h, int32_t which, const double *q, const double *p);
+int admix_get_x(admix_ctx *h, int32_t which, double *q, double *p);
+/* d.ll_new of AdmixData (structs.jl:89-90), used by admixture_qn!'s first iteration. */
+int admix_set_ll(admix_ctx *h, double ll_new);
+int admix_get_ll(admix_ctx *h, double *ll_new);
+
+/* --- sweeps ------------------------------------------------------------------------ */
+
+/* Log-likelihood of buffer `which` (loglikelihood(d_cu, g_cu), cuda/runners.jl:13-20;
+ * loglikelihood(g::SnpLinAlg, ...), algorithms_inner.jl:27-35).  FP64 accumulation. */
+int admix_loglik(admix_ctx *h, int32_t which, double *out);
+
+/* EM priming half-steps on buffer ADMIX_X (em_q!/em_p!, cuda/runners.jl:22-67;
+ * algorithms_inner.jl:68-141): q_next = EM_Q(q, p); p_next = EM_P(q, p). */
+int admix_em_q(admix_ctx *h);
+int admix_em_p(admix_ctx *h);
+/* init_em! (algorithms_outer.jl:12-45): `iters` EM iterations, ll_hist[iters] (may be NULL),
+ * then sets ll_new. */
+int admix_init_em(admix_ctx *h, int32_t iters, double *ll_hist);
+
+/* Gradient / Hessian sweep of the Q block at (q of which_q, p of which_p), written to the
+ * host in the reference layout (update_q_cuda!, cuda/runners.jl:69-89;
+ * update_q_loop_skipmissing!, loops.jl:867-894).  XtX: K x K x I, Xtz: K x I; either may be NULL. */
+int admix_grad_hess_q(admix_ctx *h, int32_t which_q, int32_t which_p, double *XtX, double *Xtz);
+/* Same for the P block (update_p_cuda!, cuda/runners.jl:91-111; loops.jl:923-950).
+ * XtX: K x K x J, Xtz: K x J. */
+int admix_grad_hess_p(admix_ctx *h, int32_t which_q, int32_t which_p, double *XtX, double *Xtz);
+
+/* --- block SQP updates (update_q! / update_p!, algorithms_inner.jl:167-310) ------ */
+
+/* update2 = 0: q_next = SQP_Q(q, p);        update2 = 1: q_next2 = SQP_Q(q_next, p_next).
+ * qp_status (length I, may be NULL) receives quadratic_program!'s return value per problem. */
+int admix_update_q(admix_ctx *h, int32_t update2, int32_t *qp_status);
+/* update2 = 0: p_next = SQP_P(q_next, p);   update2 = 1: p_next2 = SQP_P(q_next2, p_next). */
+int admix_update_p(admix_ctx *h, int32_t update2, int32_t *qp_status);
+
+/* --- outer loop (admixture_qn!, algorithms_outer.jl:63-193, mode = :ZAL) ----------- */
+
+/* One full iteration i on the device: 2 Q + 2 P SQP updates, loglik, ZAL secant update
+ * (quasi_newton.jl:5-9,29-31), projection (projections.jl), loglik, accept/reject. */
+int admix_qn_iteration(admix_ctx *h, int32_t iter, admix_iterinfo *out);
+/* Iterations iter_offset+1 .. n_iter until reldiff < rtol.  hist (n_iter entries, may be
+ * NULL) receives one record per iteration run. */
+int admix_run_qn(admix_ctx *h, int32_t n_iter, double rtol, int32_t iter_offset,
+                 admix_iterinfo *hist, int32_t *n_done, int32_t *converged);
+
+/* --- instrumentation ------------------------------------------------------------------- */
+
+/* The cudaStream_t (as void*) all of the handle's work is ordered on, so a caller can record
+ * events on it or order its own work after the engine's. */
+int admix_stream(admix_ctx *h, void **stream);
+
+/* Pass identifiers for admix_time_pass */
+#define ADMIX_PASS_LOGLIK   0   /* decode + qp + log reduction over x (loops.jl:517-539) */
+#define ADMIX_PASS_QSWEEP   1   /* Q-block gradient / Hessian sweep (loops.jl:867-894) */
+#define ADMIX_PASS_PSWEEP   2   /* P-block gradient / Hessian sweep (loops.jl:923-950) */
+#define ADMIX_PASS_QQP      3   /* batched simplex QPs + projection of the Q block */
+#define ADMIX_PASS_PQP      4   /* batched box QPs + projection of the P block */
+#define ADMIX_PASS_EM       5   /* one EM priming iteration (em_q + em_p) */
+
+/* Device time of `reps` back-to-back launches of one pass on the current buffers, measured
+ * with CUDA events on the handle's stream; *ms_per_launch receives the mean.  The QP passes
+ * solve the problems of the last sweep again (their outputs go to x_tmp). */
+int admix_time_pass(admix_ctx *h, int32_t pass, int32_t reps, double *ms_per_launch);
+
+/* Number of kernel launches in one captured quasi-Newton iteration (graph kernel nodes). */
+int admix_iteration_kernels(admix_ctx *h, int32_t *count);
+
+/* --- genotype decode ----------------------------------------------------------------- */
+
+/* Missing-code (01) counts per SNP (length J) and per individual (length I); either may
+ * be NULL.  Bit-exact integer counts of the decode rule of loops.jl:529-534. */
+int admix_decode_counts(admix_ctx *h, int64_t *miss_per_snp, int64_t *miss_per_ind);
+
+/* --- stateless device-pointer entry point --------------------------------------------- */
+
+/* loglikelihood(g::CuArray{UInt8,2}, q::CuArray, p::CuArray, I, J) (cuda/runners.jl:2-11)
+ * on caller-owned device memory.  d_work must hold admix_loglik_dev_workspace(I, J, K)
+ * bytes; the result (one double) is written to d_out.  `stream` is a cudaStream_t
+ * (NULL = legacy default stream); the call is asynchronous on that stream. */
+size_t admix_loglik_dev_workspace(int64_t I, int64_t J, int32_t K);
+int admix_loglik_dev(const uint8_t *d_bed, int64_t I, int64_t J, int32_t K,
+                     const double *d_q, const double *d_p, double *d_out,
+                     void *d_work, size_t work_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

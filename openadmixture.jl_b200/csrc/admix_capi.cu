@@ -1,0 +1,591 @@
+/*
+ * admix_capi.cu -- the C ABI of libadmix: device-resident state of one cohort and the
+ * orchestration of the reference's GPU-facing calls.
+ *
+ * The reference keeps Q/P on the host and copies them to the device around every sweep
+ * (algorithms_inner.jl:192-194, 268-270; algorithms_outer.jl:28-33, 119-123, 144-148).
+ * Here the four iterates x, x_next, x_next2, x_tmp (structs.jl:16-19), the secant matrices
+ * U, V (structs.jl:175-178), the sweep accumulators and the log-likelihood bookkeeping all
+ * stay in HBM; a quasi-Newton iteration is one captured CUDA graph and returns a 64-byte
+ * record to the host.
+ */
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <math.h>
+#include <vector>
+#include "../../include/admix.h"
+#include "common.cuh"
+#include "kernels.h"
+
+struct admix_ctx {
+    int64_t I = 0, J = 0, Ib = 0;
+    int K = 0, Q = 0;
+    uint32_t flags = 0;
+    int dev = 0, sms = 148;
+    cudaStream_t st = nullptr;
+    uint8_t *bed = nullptr;
+    double *xbuf = nullptr;          /* 4 * K(I+J): x, x_next, x_next2, x_tmp */
+    double *x[4] = {nullptr, nullptr, nullptr, nullptr};
+    double *parts_q = nullptr, *parts_p = nullptr;
+    double *U = nullptr, *V = nullptr, *vt = nullptr;
+    int32_t *status_q = nullptr, *status_p = nullptr;
+    double *ll_partial = nullptr, *qn_partial = nullptr;
+    DevScalars *sc = nullptr;
+    DevScalars *sc_host = nullptr;   /* pinned mirror */
+    int32_t *iter_host = nullptr;    /* pinned */
+    unsigned long long *counts = nullptr;
+    LoglikPlan llp;
+    SweepPlan sq, sp;
+    QNPlan qnp;
+    size_t bytes = 0;
+    cudaGraphExec_t iter_graph = nullptr;
+    char err[512] = {0};
+};
+
+static thread_local char g_err[512];
+
+static int fail(admix_ctx *h, int code, const char *fmt, ...)
+{
+    char *dst = h ? h->err : g_err;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(dst, 512, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define CK(h, call)                                                                        \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail((h), ADMIX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+static bool valid_which(int w) { return w >= 0 && w < 4; }
+static double *Qof(admix_ctx *h, int w) { return h->x[w]; }
+static double *Pof(admix_ctx *h, int w) { return h->x[w] + (size_t)h->K * h->I; }
+
+/* V' of svd(ones(1,K), full=true) (structs.jl:180) as LAPACK builds it: one Householder
+ * reflector H = I - tau v v' from dlarfg on ones(K), generated by dorgl2. */
+static void vt_ones(int K, double *vt)
+{
+    for (int a = 0; a < K * K; ++a) vt[a] = 0.0;
+    if (K == 1) { vt[0] = 1.0; return; }
+    const double alpha = 1.0, xnorm = sqrt((double)(K - 1));
+    const double w = fmax(fabs(alpha), fabs(xnorm)), z = fmin(fabs(alpha), fabs(xnorm));
+    const double nrm = w * sqrt(1.0 + (z / w) * (z / w));
+    const double beta = -copysign(nrm, alpha);
+    const double tau = (beta - alpha) / beta;
+    const double vs = 1.0 / (alpha - beta);
+    vt[0] = 1.0 - tau;
+    for (int c = 1; c < K; ++c) vt[K * c] = -tau * vs;
+    for (int r = 1; r < K; ++r)
+        for (int c = 0; c < K; ++c) {
+            const double vc = (c == 0) ? 1.0 : vs;
+            vt[r + K * c] = ((r == c) ? 1.0 : 0.0) + vs * (-tau * vc);
+        }
+}
+
+template <typename T>
+static int dalloc(admix_ctx *h, T **p, size_t count)
+{
+    const size_t b = sizeof(T) * (count ? count : 1);
+    cudaError_t e = cudaMalloc((void **)p, b);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(h, ADMIX_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", b, cudaGetErrorString(e));
+    }
+    h->bytes += b;
+    return ADMIX_OK;
+}
+
+static void release(admix_ctx *h)
+{
+    if (!h) return;
+    if (h->iter_graph) cudaGraphExecDestroy(h->iter_graph);
+    void *dps[] = {h->bed, h->xbuf, h->parts_q, h->parts_p, h->U, h->V, h->vt, h->status_q,
+                   h->status_p, h->ll_partial, h->qn_partial, h->sc, h->counts};
+    for (void *p : dps)
+        if (p) cudaFree(p);
+    if (h->sc_host) cudaFreeHost(h->sc_host);
+    if (h->iter_host) cudaFreeHost(h->iter_host);
+    if (h->st) cudaStreamDestroy(h->st);
+}
+
+extern "C" {
+
+const char *admix_last_error(const admix_ctx *h) { return h ? h->err : g_err; }
+
+int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed, uint32_t flags,
+                 admix_ctx **out)
+{
+    if (!out) return fail(nullptr, ADMIX_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (I < 1 || J < 1) return fail(nullptr, ADMIX_ERR_ARG, "I and J must be >= 1 (I=%lld, J=%lld)", (long long)I, (long long)J);
+    if (K < 1 || K > ADMIX_MAX_K) return fail(nullptr, ADMIX_ERR_UNSUPPORTED, "K=%d outside [1, %d]", K, ADMIX_MAX_K);
+    if (Q < 1 || Q > ADMIX_MAX_Q) return fail(nullptr, ADMIX_ERR_UNSUPPORTED, "Q=%d outside [1, %d]", Q, ADMIX_MAX_Q);
+    if (!bed) return fail(nullptr, ADMIX_ERR_ARG, "bed is NULL");
+    if (flags & ~(ADMIX_FLAG_MU_GERSHGORIN | ADMIX_FLAG_MIXED))
+        return fail(nullptr, ADMIX_ERR_ARG, "unknown flags 0x%x", flags);
+    if (flags & ADMIX_FLAG_MIXED)
+        return fail(nullptr, ADMIX_ERR_UNSUPPORTED, "ADMIX_FLAG_MIXED is not available in this build");
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev == 0)
+        return fail(nullptr, ADMIX_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(ce));
+
+    admix_ctx *h = new admix_ctx();
+    h->I = I; h->J = J; h->K = K; h->Q = Q; h->flags = flags;
+    h->Ib = (I + 3) / 4;
+    int rc;
+#define TRY(x) do { rc = (x); if (rc != ADMIX_OK) { strncpy(g_err, h->err, sizeof(g_err) - 1); release(h); delete h; return rc; } } while (0)
+#define TRYC(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { fail(nullptr, ADMIX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); release(h); delete h; return ADMIX_ERR_CUDA; } } while (0)
+    TRYC(cudaGetDevice(&h->dev));
+    TRYC(cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->dev));
+    TRYC(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    TRYC(prepare_sweeps(K));
+    TRYC(prepare_qp(K));
+
+    const int64_t nx = (int64_t)K * (I + J);
+    const int T = K * (K + 1) / 2, E = T + K;
+    h->llp = plan_loglik(I, J, h->sms);
+    h->sq = plan_sweep_q(K, I, J, h->sms);
+    h->sp = plan_sweep_p(K, I, J, h->sms);
+    h->qnp = plan_qn(nx, h->sms);
+
+    TRY(dalloc(h, &h->bed, (size_t)h->Ib * J));
+    TRY(dalloc(h, &h->xbuf, (size_t)4 * nx));
+    for (int w = 0; w < 4; ++w) h->x[w] = h->xbuf + (size_t)w * nx;
+    TRY(dalloc(h, &h->parts_q, (size_t)h->sq.S * I * E));
+    TRY(dalloc(h, &h->parts_p, (size_t)h->sp.S * J * E));
+    TRY(dalloc(h, &h->U, (size_t)nx * Q));
+    TRY(dalloc(h, &h->V, (size_t)nx * Q));
+    TRY(dalloc(h, &h->vt, (size_t)K * K));
+    TRY(dalloc(h, &h->status_q, (size_t)I));
+    TRY(dalloc(h, &h->status_p, (size_t)J));
+    TRY(dalloc(h, &h->ll_partial, (size_t)h->llp.gx * h->llp.gy));
+    TRY(dalloc(h, &h->qn_partial, (size_t)h->qnp.blocks * (Q * Q + Q)));
+    TRY(dalloc(h, &h->sc, 1));
+    TRY(dalloc(h, &h->counts, (size_t)(I + J)));
+    TRYC(cudaMallocHost((void **)&h->sc_host, sizeof(DevScalars)));
+    TRYC(cudaMallocHost((void **)&h->iter_host, sizeof(int32_t)));
+
+    TRYC(cudaMemcpyAsync(h->bed, bed, (size_t)h->Ib * J, cudaMemcpyHostToDevice, h->st));
+    TRYC(cudaMemsetAsync(h->xbuf, 0, sizeof(double) * 4 * nx, h->st));
+    TRYC(cudaMemsetAsync(h->U, 0, sizeof(double) * nx * Q, h->st));
+    TRYC(cudaMemsetAsync(h->V, 0, sizeof(double) * nx * Q, h->st));
+    std::vector<double> vt((size_t)K * K);
+    vt_ones(K, vt.data());
+    TRYC(cudaMemcpyAsync(h->vt, vt.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice, h->st));
+    DevScalars z;
+    memset(&z, 0, sizeof(z));
+    z.ll_new = NAN; z.ll_prev = NAN;
+    TRYC(cudaMemcpyAsync(h->sc, &z, sizeof(z), cudaMemcpyHostToDevice, h->st));
+    TRYC(cudaStreamSynchronize(h->st));
+#undef TRY
+#undef TRYC
+    *out = h;
+    return ADMIX_OK;
+}
+
+int admix_destroy(admix_ctx *h)
+{
+    if (!h) return ADMIX_OK;
+    if (h->st) cudaStreamSynchronize(h->st);
+    release(h);
+    delete h;
+    return ADMIX_OK;
+}
+
+int admix_device_bytes(const admix_ctx *h, int64_t *bytes)
+{
+    if (!h || !bytes) return ADMIX_ERR_ARG;
+    *bytes = (int64_t)h->bytes;
+    return ADMIX_OK;
+}
+
+int admix_set_x(admix_ctx *h, int32_t which, const double *q, const double *p)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (!valid_which(which)) return fail(h, ADMIX_ERR_ARG, "invalid buffer selector %d", which);
+    if (q) CK(h, cudaMemcpyAsync(Qof(h, which), q, sizeof(double) * h->K * h->I, cudaMemcpyHostToDevice, h->st));
+    if (p) CK(h, cudaMemcpyAsync(Pof(h, which), p, sizeof(double) * h->K * h->J, cudaMemcpyHostToDevice, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+int admix_get_x(admix_ctx *h, int32_t which, double *q, double *p)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (!valid_which(which)) return fail(h, ADMIX_ERR_ARG, "invalid buffer selector %d", which);
+    if (q) CK(h, cudaMemcpyAsync(q, Qof(h, which), sizeof(double) * h->K * h->I, cudaMemcpyDeviceToHost, h->st));
+    if (p) CK(h, cudaMemcpyAsync(p, Pof(h, which), sizeof(double) * h->K * h->J, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+int admix_set_ll(admix_ctx *h, double ll_new)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    CK(h, cudaMemcpyAsync(&h->sc->ll_new, &ll_new, sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+int admix_get_ll(admix_ctx *h, double *ll_new)
+{
+    if (!h || !ll_new) return fail(h, ADMIX_ERR_ARG, "NULL argument");
+    CK(h, cudaMemcpyAsync(ll_new, &h->sc->ll_new, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+} /* extern "C" */
+
+/* ---- stream-ordered building blocks (no synchronisation) ---- */
+
+static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst)
+{
+    return launch_loglik_f64(h->K, h->bed, h->I, h->J, Qof(h, which), Pof(h, which), h->llp,
+                             h->ll_partial, dst, h->st);
+}
+
+/* update_q!: q_out = project_q(q + QP(H_q, -Xtz_q)) */
+static cudaError_t enq_update_q(admix_ctx *h, int update2)
+{
+    const int wq = update2 ? ADMIX_X_NEXT : ADMIX_X;
+    const int wp = update2 ? ADMIX_X_NEXT : ADMIX_X;
+    const int wo = update2 ? ADMIX_X_NEXT2 : ADMIX_X_NEXT;
+    cudaError_t e = launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
+    if (e != cudaSuccess) return e;
+    return launch_qp(h->K, true, h->I, h->parts_q, h->sq.S, Qof(h, wq), Qof(h, wo), h->status_q,
+                     &h->sc->fail_q, h->vt, (h->flags & ADMIX_FLAG_MU_GERSHGORIN) ? 1 : 0, h->st);
+}
+
+/* update_p!: p_out = project_p(p + QP(H_p, -Xtz_p)), with q = q_next (update2 = 0) or q_next2 */
+static cudaError_t enq_update_p(admix_ctx *h, int update2)
+{
+    const int wq = update2 ? ADMIX_X_NEXT2 : ADMIX_X_NEXT;
+    const int wp = update2 ? ADMIX_X_NEXT : ADMIX_X;
+    const int wo = update2 ? ADMIX_X_NEXT2 : ADMIX_X_NEXT;
+    cudaError_t e = launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
+    if (e != cudaSuccess) return e;
+    return launch_qp(h->K, false, h->J, h->parts_p, h->sp.S, Pof(h, wp), Pof(h, wo), h->status_p,
+                     &h->sc->fail_p, h->vt, 0, h->st);
+}
+
+static cudaError_t enq_em(admix_ctx *h)
+{
+    /* em_q! then em_p! (mode :base, both from (q, p)), then p, q <- next (algorithms_outer.jl:23-30) */
+    cudaError_t e = launch_sweep_q_f64(h->K, 1, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st);
+    if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st);
+    if (e == cudaSuccess) e = launch_sweep_p_f64(h->K, 1, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st);
+    if (e == cudaSuccess) e = launch_emp_finalize(h->J, h->K, h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st);
+    return e;
+}
+
+/* one admixture_qn! iteration, stream-ordered; sc->iter must already hold i */
+static cudaError_t enq_iteration(admix_ctx *h)
+{
+    const int64_t nx = (int64_t)h->K * (h->I + h->J);
+    cudaError_t e = launch_iter_begin(h->sc, h->st);
+    if (e == cudaSuccess) e = enq_update_q(h, 0);
+    if (e == cudaSuccess) e = enq_update_p(h, 0);
+    if (e == cudaSuccess) e = enq_update_q(h, 1);
+    if (e == cudaSuccess) e = enq_update_p(h, 1);
+    if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_NEXT2, &h->sc->ll_basic);
+    if (e == cudaSuccess) e = launch_qn(h->Q, h->I, h->J, h->K, h->x[ADMIX_X], h->x[ADMIX_X_NEXT], h->x[ADMIX_X_NEXT2],
+                                        h->U, h->V, h->x[ADMIX_X_TMP], h->qn_partial, h->qnp, h->sc, h->sms, h->st);
+    if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_TMP, &h->sc->ll_qn);
+    if (e == cudaSuccess) e = launch_accept(nx, h->x[ADMIX_X_TMP], h->x[ADMIX_X_NEXT2], h->x[ADMIX_X], h->sc, h->sms, h->st);
+    return e;
+}
+
+static int read_scalars(admix_ctx *h)
+{
+    CK(h, cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+extern "C" {
+
+int admix_loglik(admix_ctx *h, int32_t which, double *out)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (!valid_which(which) || !out) return fail(h, ADMIX_ERR_ARG, "invalid argument");
+    CK(h, enq_loglik(h, which, &h->sc->ll_tmp));
+    CK(h, cudaMemcpyAsync(out, &h->sc->ll_tmp, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+int admix_em_q(admix_ctx *h)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    CK(h, launch_sweep_q_f64(h->K, 1, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st));
+    CK(h, launch_emq_finalize(h->I, h->K, h->J, h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+int admix_em_p(admix_ctx *h)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    CK(h, launch_sweep_p_f64(h->K, 1, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st));
+    CK(h, launch_emp_finalize(h->J, h->K, h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+int admix_init_em(admix_ctx *h, int32_t iters, double *ll_hist)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (iters < 0) return fail(h, ADMIX_ERR_ARG, "iters must be >= 0");
+    for (int it = 0; it < iters; ++it) {
+        CK(h, enq_em(h));
+        CK(h, cudaMemcpyAsync(Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), sizeof(double) * h->K * h->J, cudaMemcpyDeviceToDevice, h->st));
+        CK(h, cudaMemcpyAsync(Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), sizeof(double) * h->K * h->I, cudaMemcpyDeviceToDevice, h->st));
+        CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_tmp));
+        if (ll_hist) CK(h, cudaMemcpyAsync(ll_hist + it, &h->sc->ll_tmp, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    }
+    CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+static int grad_hess_common(admix_ctx *h, bool qside, int32_t wq, int32_t wp, double *XtX, double *Xtz)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (!valid_which(wq) || !valid_which(wp)) return fail(h, ADMIX_ERR_ARG, "invalid buffer selector");
+    const int64_t nprob = qside ? h->I : h->J;
+    const int K = h->K;
+    double *d_XtX = nullptr, *d_Xtz = nullptr;
+    if (cudaMalloc((void **)&d_XtX, sizeof(double) * K * K * nprob) != cudaSuccess ||
+        cudaMalloc((void **)&d_Xtz, sizeof(double) * K * nprob) != cudaSuccess) {
+        if (d_XtX) cudaFree(d_XtX);
+        return fail(h, ADMIX_ERR_NOMEM, "dump buffers: cudaMalloc failed");
+    }
+    cudaError_t e;
+    if (qside) {
+        e = launch_sweep_q_f64(K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
+        if (e == cudaSuccess) e = launch_expand_hess(nprob, K, h->sq.S, h->parts_q, d_XtX, d_Xtz, h->sms, h->st);
+    } else {
+        e = launch_sweep_p_f64(K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
+        if (e == cudaSuccess) e = launch_expand_hess(nprob, K, h->sp.S, h->parts_p, d_XtX, d_Xtz, h->sms, h->st);
+    }
+    if (e == cudaSuccess && XtX) e = cudaMemcpyAsync(XtX, d_XtX, sizeof(double) * K * K * nprob, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess && Xtz) e = cudaMemcpyAsync(Xtz, d_Xtz, sizeof(double) * K * nprob, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    cudaFree(d_XtX);
+    cudaFree(d_Xtz);
+    if (e != cudaSuccess) return fail(h, ADMIX_ERR_CUDA, "grad/hess sweep failed: %s", cudaGetErrorString(e));
+    return ADMIX_OK;
+}
+
+int admix_grad_hess_q(admix_ctx *h, int32_t which_q, int32_t which_p, double *XtX, double *Xtz)
+{
+    return grad_hess_common(h, true, which_q, which_p, XtX, Xtz);
+}
+
+int admix_grad_hess_p(admix_ctx *h, int32_t which_q, int32_t which_p, double *XtX, double *Xtz)
+{
+    return grad_hess_common(h, false, which_q, which_p, XtX, Xtz);
+}
+
+int admix_update_q(admix_ctx *h, int32_t update2, int32_t *qp_status)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    CK(h, enq_update_q(h, update2 ? 1 : 0));
+    if (qp_status) CK(h, cudaMemcpyAsync(qp_status, h->status_q, sizeof(int32_t) * h->I, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+int admix_update_p(admix_ctx *h, int32_t update2, int32_t *qp_status)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    CK(h, enq_update_p(h, update2 ? 1 : 0));
+    if (qp_status) CK(h, cudaMemcpyAsync(qp_status, h->status_p, sizeof(int32_t) * h->J, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+static int ensure_graph(admix_ctx *h)
+{
+    if (h->iter_graph) return ADMIX_OK;
+    cudaGraph_t g = nullptr;
+    CK(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enq_iteration(h);
+    cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(h, ADMIX_ERR_CUDA, "iteration capture failed: %s / %s", cudaGetErrorString(e), cudaGetErrorString(e2));
+    }
+    e = cudaGraphInstantiate(&h->iter_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->iter_graph = nullptr;
+        return fail(h, ADMIX_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    }
+    return ADMIX_OK;
+}
+
+static int run_one(admix_ctx *h, int32_t iter, admix_iterinfo *out)
+{
+    int rc = ensure_graph(h);
+    if (rc != ADMIX_OK) return rc;
+    *h->iter_host = iter;
+    CK(h, cudaMemcpyAsync(&h->sc->iter, h->iter_host, sizeof(int32_t), cudaMemcpyHostToDevice, h->st));
+    CK(h, cudaGraphLaunch(h->iter_graph, h->st));
+    rc = read_scalars(h);
+    if (rc != ADMIX_OK) return rc;
+    const DevScalars &s = *h->sc_host;
+    if (out) {
+        out->ll_prev = s.ll_prev; out->ll_basic = s.ll_basic; out->ll_qn = s.ll_qn;
+        out->ll_new = s.ll_new; out->reldiff = s.reldiff; out->iter = iter;
+        out->accepted_qn = s.accepted; out->qp_fail_q = s.fail_q; out->qp_fail_p = s.fail_p;
+    }
+    return ADMIX_OK;
+}
+
+int admix_qn_iteration(admix_ctx *h, int32_t iter, admix_iterinfo *out)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (iter < 1) return fail(h, ADMIX_ERR_ARG, "iteration number must be >= 1 (got %d)", iter);
+    return run_one(h, iter, out);
+}
+
+int admix_run_qn(admix_ctx *h, int32_t n_iter, double rtol, int32_t iter_offset,
+                 admix_iterinfo *hist, int32_t *n_done, int32_t *converged)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (iter_offset < 0) return fail(h, ADMIX_ERR_ARG, "iter_offset must be >= 0");
+    int rc = read_scalars(h);
+    if (rc != ADMIX_OK) return rc;
+    if (isnan(h->sc_host->ll_new)) {   /* algorithms_outer.jl:76-83 */
+        CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new));
+        CK(h, cudaStreamSynchronize(h->st));
+    }
+    int done = 0, conv = 0;
+    for (int it = iter_offset + 1; it <= n_iter; ++it) {
+        admix_iterinfo info;
+        rc = run_one(h, it, &info);
+        if (rc != ADMIX_OK) return rc;
+        if (hist) hist[done] = info;
+        ++done;
+        if (info.reldiff < rtol) { conv = 1; break; }
+    }
+    if (n_done) *n_done = done;
+    if (converged) *converged = conv;
+    return ADMIX_OK;
+}
+
+int admix_stream(admix_ctx *h, void **stream)
+{
+    if (!h || !stream) return fail(h, ADMIX_ERR_ARG, "NULL argument");
+    *stream = (void *)h->st;
+    return ADMIX_OK;
+}
+
+int admix_time_pass(admix_ctx *h, int32_t pass, int32_t reps, double *ms_per_launch)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (reps < 1 || !ms_per_launch) return fail(h, ADMIX_ERR_ARG, "reps must be >= 1 and ms_per_launch non-NULL");
+    if (pass < ADMIX_PASS_LOGLIK || pass > ADMIX_PASS_EM) return fail(h, ADMIX_ERR_ARG, "unknown pass %d", pass);
+    const int mu = (h->flags & ADMIX_FLAG_MU_GERSHGORIN) ? 1 : 0;
+    auto one = [&]() -> cudaError_t {
+        switch (pass) {
+        case ADMIX_PASS_LOGLIK: return enq_loglik(h, ADMIX_X, &h->sc->ll_tmp);
+        case ADMIX_PASS_QSWEEP: return launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st);
+        case ADMIX_PASS_PSWEEP: return launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st);
+        case ADMIX_PASS_QQP: return launch_qp(h->K, true, h->I, h->parts_q, h->sq.S, Qof(h, ADMIX_X), Qof(h, ADMIX_X_TMP), h->status_q, nullptr, h->vt, mu, h->st);
+        case ADMIX_PASS_PQP: return launch_qp(h->K, false, h->J, h->parts_p, h->sp.S, Pof(h, ADMIX_X), Pof(h, ADMIX_X_TMP), h->status_p, nullptr, h->vt, 0, h->st);
+        default: return enq_em(h);
+        }
+    };
+    cudaEvent_t e0, e1;
+    CK(h, cudaEventCreate(&e0));
+    CK(h, cudaEventCreate(&e1));
+    cudaError_t e = one();   /* warm-up launch */
+    if (e == cudaSuccess) e = cudaEventRecord(e0, h->st);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = one();
+    if (e == cudaSuccess) e = cudaEventRecord(e1, h->st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail(h, ADMIX_ERR_CUDA, "timing pass %d failed: %s", pass, cudaGetErrorString(e));
+    *ms_per_launch = (double)ms / reps;
+    return ADMIX_OK;
+}
+
+int admix_iteration_kernels(admix_ctx *h, int32_t *count)
+{
+    if (!h || !count) return fail(h, ADMIX_ERR_ARG, "NULL argument");
+    cudaGraph_t g = nullptr;
+    CK(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enq_iteration(h);
+    cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(h, ADMIX_ERR_CUDA, "capture failed");
+    }
+    size_t n = 0;
+    e = cudaGraphGetNodes(g, nullptr, &n);
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (e == cudaSuccess && n) e = cudaGraphGetNodes(g, nodes.data(), &n);
+    int32_t k = 0;
+    for (size_t t = 0; t < n && e == cudaSuccess; ++t) {
+        cudaGraphNodeType ty;
+        if (cudaGraphNodeGetType(nodes[t], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++k;
+    }
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(h, ADMIX_ERR_CUDA, "graph query failed: %s", cudaGetErrorString(e));
+    *count = k;
+    return ADMIX_OK;
+}
+
+int admix_decode_counts(admix_ctx *h, int64_t *miss_per_snp, int64_t *miss_per_ind)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    CK(h, cudaMemsetAsync(h->counts, 0, sizeof(unsigned long long) * (h->I + h->J), h->st));
+    CK(h, launch_decode_counts(h->bed, h->I, h->J, h->counts + h->I, h->counts, h->sms, h->st));
+    if (miss_per_snp) CK(h, cudaMemcpyAsync(miss_per_snp, h->counts + h->I, sizeof(int64_t) * h->J, cudaMemcpyDeviceToHost, h->st));
+    if (miss_per_ind) CK(h, cudaMemcpyAsync(miss_per_ind, h->counts, sizeof(int64_t) * h->I, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+size_t admix_loglik_dev_workspace(int64_t I, int64_t J, int32_t K)
+{
+    (void)K;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const LoglikPlan pl = plan_loglik(I, J, sms);
+    return sizeof(double) * (size_t)pl.gx * pl.gy;
+}
+
+int admix_loglik_dev(const uint8_t *d_bed, int64_t I, int64_t J, int32_t K, const double *d_q,
+                     const double *d_p, double *d_out, void *d_work, size_t work_bytes, void *stream)
+{
+    if (!d_bed || !d_q || !d_p || !d_out || !d_work) return fail(nullptr, ADMIX_ERR_ARG, "NULL device pointer");
+    if (I < 1 || J < 1) return fail(nullptr, ADMIX_ERR_ARG, "I and J must be >= 1");
+    if (K < 1 || K > ADMIX_MAX_K) return fail(nullptr, ADMIX_ERR_UNSUPPORTED, "K=%d outside [1, %d]", K, ADMIX_MAX_K);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return fail(nullptr, ADMIX_ERR_CUDA, "no current CUDA device");
+    const LoglikPlan pl = plan_loglik(I, J, sms);
+    if (work_bytes < sizeof(double) * (size_t)pl.gx * pl.gy)
+        return fail(nullptr, ADMIX_ERR_ARG, "workspace of %zu bytes is below the %zu required", work_bytes,
+                    sizeof(double) * (size_t)pl.gx * pl.gy);
+    cudaError_t e = launch_loglik_f64(K, d_bed, I, J, d_q, d_p, pl, (double *)d_work, d_out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(nullptr, ADMIX_ERR_CUDA, "loglik launch failed: %s", cudaGetErrorString(e));
+    return ADMIX_OK;
+}
+
+} /* extern "C" */

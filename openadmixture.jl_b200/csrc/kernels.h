@@ -1,0 +1,53 @@
+/*
+ * kernels.h -- host-side launchers of libadmix's device kernels (internal).
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <algorithm>
+#include "common.cuh"
+
+struct LoglikPlan { int gx = 1, gy = 1; int64_t jslice = 1; };
+struct SweepPlan  { int gx = 1, S = 1; int64_t slice = 1; };
+
+LoglikPlan plan_loglik(int64_t I, int64_t J, int sms);
+SweepPlan plan_sweep_q(int K, int64_t I, int64_t J, int sms);
+SweepPlan plan_sweep_p(int K, int64_t I, int64_t J, int sms);
+
+/* FP64 sweeps (sweeps_f64.cu) */
+cudaError_t prepare_sweeps(int K);
+cudaError_t launch_loglik_f64(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+                              const double *p, const LoglikPlan &pl, double *partial, double *out,
+                              cudaStream_t st);
+cudaError_t launch_sweep_q_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J,
+                               const double *q, const double *p, const SweepPlan &pl, double *out,
+                               cudaStream_t st);
+cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J,
+                               const double *q, const double *p, const SweepPlan &pl, double *out,
+                               cudaStream_t st);
+cudaError_t launch_emq_finalize(int64_t I, int K, int64_t J, int S, const double *parts,
+                                const double *q, double *q_next, int sms, cudaStream_t st);
+cudaError_t launch_emp_finalize(int64_t J, int K, int S, const double *parts, const double *p,
+                                double *p_next, int sms, cudaStream_t st);
+cudaError_t launch_expand_hess(int64_t nprob, int K, int S, const double *parts, double *XtX,
+                               double *Xtz, int sms, cudaStream_t st);
+cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J,
+                                 unsigned long long *miss_snp, unsigned long long *miss_ind,
+                                 int sms, cudaStream_t st);
+
+/* batched QP + projection (qp_batch.cu) */
+cudaError_t prepare_qp(int K);
+cudaError_t launch_qp(int K, bool simplex, int64_t nprob, const double *parts, int S,
+                      const double *x, double *x_next, int32_t *status, int32_t *fail_count,
+                      const double *vt, int mu_mode, cudaStream_t st);
+
+/* quasi-Newton (qn.cu) */
+struct QNPlan { int blocks = 1; };
+QNPlan plan_qn(int64_t n, int sms);
+cudaError_t launch_qn(int Q, int64_t I, int64_t J, int K, const double *x0, const double *x1,
+                      const double *x2, double *U, double *V, double *x_tmp, double *partial,
+                      const QNPlan &pl, DevScalars *sc, int sms, cudaStream_t st);
+cudaError_t launch_iter_begin(DevScalars *sc, cudaStream_t st);
+cudaError_t launch_accept(int64_t n, const double *x_tmp, const double *x_next2, double *x,
+                          DevScalars *sc, int sms, cudaStream_t st);
+cudaError_t launch_copy(int64_t n, const double *src, double *dst, int sms, cudaStream_t st);

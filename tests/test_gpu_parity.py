@@ -1,0 +1,262 @@
+"""GPU parity: every libadmix entry point against the oracle (and the golden fixtures) on the
+same inputs.  Tolerances: integer decode bit-exact; FP64 sweeps 1e-10 relative (per entry,
+relative to the entry or, for sums with cancellation, to the largest entry of its row);
+SQP updates 1e-9 absolute on Q/P in [0, 1]; full runs 1e-6 relative on the final
+log-likelihood."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+
+
+def _cohort(oa, I, J, K, seed=1, cfg="c1", **kw):
+    spec = oa.COHORTS[cfg].scaled(I=I, J=J, K=K, seed=seed, **kw)
+    g, qt, pt = oa.make_cohort(spec)
+    return g
+
+
+def _handle(oa, g, K, Q=3, x=None, seed=3, flags=0):
+    d = oa.AdmixData(g.I, g.J, K, Q, rng=seed)
+    if x is not None:
+        d.x[:] = x
+    d_cu = oa.CuAdmixData(d, g, flags=flags)
+    d_cu.upload(oa.X, d.x)
+    return d, d_cu
+
+
+def _row_rel(a, b):
+    """max |a-b| / max(|b| row-wise max): relative error against each problem's own scale."""
+    a = a.reshape(a.shape[0], -1); b = b.reshape(b.shape[0], -1)
+    scale = np.abs(b).max(axis=1, keepdims=True)
+    return float(np.max(np.abs(a - b) / np.maximum(scale, 1e-300)))
+
+
+# ------------------------------------------------------------------ golden fixtures
+
+def test_golden_decode_and_loglik(oa):
+    for name in ("small_k3", "small_k5"):
+        z = load_golden(name)
+        I, J, K = int(z["I"]), int(z["J"]), int(z["K"])
+        g = oa.Genotypes(z["bed"], I, J)
+        d, d_cu = _handle(oa, g, K, x=z["x0"])
+        snp, ind = d_cu.decode_counts()
+        assert np.array_equal(snp, z["miss_snp"]) and np.array_equal(ind, z["miss_ind"])
+        assert rel_err(d_cu.loglik(oa.X), z["ll_x0"]) < FP64_TOL
+        d_cu.close()
+
+
+def test_golden_em_sweeps_and_sqp(oa):
+    for name in ("small_k3", "small_k5"):
+        z = load_golden(name)
+        I, J, K = int(z["I"]), int(z["J"]), int(z["K"])
+        g = oa.Genotypes(z["bed"], I, J)
+        d, d_cu = _handle(oa, g, K, x=z["x0"])
+        oa.em_q(d_cu); oa.em_p(d_cu)
+        xn = d_cu.download(oa.X_NEXT)
+        assert rel_err(xn[:I], z["q_em"]) < FP64_TOL
+        assert rel_err(xn[I:], z["p_em"]) < FP64_TOL
+        xe = np.vstack([z["q_em"], z["p_em"]])
+        d_cu.upload(oa.X, xe)
+        H, zz = d_cu.grad_hess_q(oa.X, oa.X)
+        assert _row_rel(H, z["XtX_q"]) < FP64_TOL and _row_rel(zz, z["Xtz_q"]) < FP64_TOL
+        H, zz = d_cu.grad_hess_p(oa.X, oa.X)
+        assert _row_rel(H, z["XtX_p"]) < FP64_TOL and _row_rel(zz, z["Xtz_p"]) < FP64_TOL
+        d.x[:] = xe
+        st = oa.update_q(d, g, False, d_cu=d_cu)
+        assert np.array_equal(st, z["st_q"])
+        assert np.max(np.abs(d.x_next[:I] - z["q_sqp"])) < 1e-9
+        st = oa.update_p(d, g, False, d_cu=d_cu)
+        assert np.array_equal(st, z["st_p"])
+        assert np.max(np.abs(d.x_next[I:] - z["p_sqp"])) < 1e-9
+        # four QN iterations
+        d.x[:] = xe
+        d.ll_new = float(z["ll_em"])
+        recs = oa.admixture_qn(d, g, 4, 0.0, d_cu=d_cu, quiet=True)
+        got = np.array([[r[k] for k in ("ll_prev", "ll_basic", "ll_qn", "ll_new")] for r in recs])
+        assert rel_err(got, z["qn_info"][:, :4]) < 1e-9
+        assert np.max(np.abs(d.x - z["x_qn4"])) < 1e-7
+        d_cu.close()
+
+
+# ------------------------------------------------------------------ vs oracle, many K
+
+@pytest.mark.parametrize("K", [1, 2, 3, 5, 8, 9, 12, 16])
+def test_sweeps_match_oracle(oa, orc, K):
+    g = _cohort(oa, I=523, J=1031, K=K, seed=K)          # ragged last byte (523 % 4 = 3)
+    d, d_cu = _handle(oa, g, K, seed=K + 10)
+    I, J = g.I, g.J
+    q, p = np.ascontiguousarray(d.x[:I]), np.ascontiguousarray(d.x[I:])
+    assert rel_err(d_cu.loglik(oa.X), orc.loglik(g.data, I, J, K, q, p)) < FP64_TOL
+    H, z = d_cu.grad_hess_q(oa.X, oa.X)
+    Ho, zo = orc.grad_hess_q(g.data, I, J, K, q, p)
+    assert _row_rel(H, Ho) < FP64_TOL and _row_rel(z, zo) < FP64_TOL
+    H, z = d_cu.grad_hess_p(oa.X, oa.X)
+    Ho, zo = orc.grad_hess_p(g.data, I, J, K, q, p)
+    assert _row_rel(H, Ho) < FP64_TOL and _row_rel(z, zo) < FP64_TOL
+    oa.em_q(d_cu); oa.em_p(d_cu)
+    xn = d_cu.download(oa.X_NEXT)
+    assert rel_err(xn[:I], orc.em_q(g.data, I, J, K, q, p)) < FP64_TOL
+    assert rel_err(xn[I:], orc.em_p(g.data, I, J, K, q, p)) < FP64_TOL
+    snp, ind = d_cu.decode_counts()
+    snp_o, ind_o = orc.decode_counts(g.data, I, J)
+    assert np.array_equal(snp, snp_o) and np.array_equal(ind, ind_o)
+    d_cu.close()
+
+
+@pytest.mark.parametrize("K,flags", [(3, 0), (6, 0), (6, 1), (12, 0)])
+def test_init_em_and_sqp_updates_match_oracle(oa, orc, K, flags):
+    g = _cohort(oa, I=401, J=2003, K=K, seed=20 + K)
+    d, d_cu = _handle(oa, g, K, seed=4, flags=flags)
+    r = orc.OracleRun(g.data, g.I, g.J, K, 3, d.x, mu_mode=flags & 1)
+    ll_o = r.init_em(5)
+    ll_g = oa.init_em(d, g, 5, d_cu=d_cu, quiet=True)
+    assert rel_err(ll_g, ll_o) < 1e-9
+    assert np.max(np.abs(d.x - r.x)) < 1e-9
+    # one SQP half-step each way from identical inputs
+    d.x[:] = r.x
+    st_q = oa.update_q(d, g, False, d_cu=d_cu)
+    st_qo = r.update_q(False)
+    assert np.mean(st_q == st_qo) > 0.999
+    assert np.max(np.abs(d.x_next[: g.I] - r.x_next[: g.I])) < 1e-9
+    st_p = oa.update_p(d, g, False, d_cu=d_cu)
+    st_po = r.update_p(False)
+    assert np.mean(st_p == st_po) > 0.999
+    assert np.max(np.abs(d.x_next[g.I:] - r.x_next[g.I:])) < 1e-9
+    d_cu.close()
+
+
+@pytest.mark.parametrize("K,Q", [(3, 3), (4, 1), (5, 5)])
+def test_qn_iterations_match_oracle(oa, orc, K, Q):
+    g = _cohort(oa, I=300, J=1500, K=K, seed=30 + K)
+    d, d_cu = _handle(oa, g, K, Q=Q, seed=5)
+    r = orc.OracleRun(g.data, g.I, g.J, K, Q, d.x)
+    r.init_em(3)
+    d.x[:] = r.x
+    d.ll_new = r.ll_new
+    recs = oa.admixture_qn(d, g, 6, 0.0, d_cu=d_cu, quiet=True)
+    for it, rec in enumerate(recs, start=1):
+        o = r.qn_iteration(it)
+        for k in ("ll_prev", "ll_basic", "ll_qn", "ll_new"):
+            assert rel_err(rec[k], o[k]) < 1e-8, (it, k, rec[k], o[k])
+    assert np.max(np.abs(d.x - r.x)) < 1e-6
+    d_cu.close()
+
+
+def test_run_admixture_converges_like_oracle(oa, orc, tmp_path):
+    spec = oa.COHORTS["c1"].scaled(I=600, J=4000, seed=8)
+    g, _, _ = oa.make_cohort(spec)
+    path = oa.write_bed(tmp_path / "c1s.bed", g)
+    d, _, _ = oa.run_admixture(str(path), 3, rng=11, quiet=True)
+    x0 = oa.init_x(g.I, g.J, 3, 11)
+    r = orc.OracleRun(g.data, g.I, g.J, 3, 3, x0)
+    r.init_em(5)
+    hist, conv = r.admixture_qn(1000, 1e-7)
+    assert conv
+    assert rel_err(d.ll_new, r.ll_new) < 1e-6
+
+
+def test_loglik_dev_entry_matches_handle(oa):
+    import torch
+    from openadmixture_b200 import _native as N
+    g = _cohort(oa, I=777, J=3001, K=4, seed=2)
+    d, d_cu = _handle(oa, g, 4)
+    want = d_cu.loglik(oa.X)
+    dev = torch.device("cuda:0")
+    bed = torch.from_numpy(g.data).to(dev)
+    q = torch.from_numpy(np.ascontiguousarray(d.x[: g.I])).to(dev)
+    p = torch.from_numpy(np.ascontiguousarray(d.x[g.I:])).to(dev)
+    out = torch.zeros(1, dtype=torch.float64, device=dev)
+    lib = N.admix_lib()
+    nbytes = lib.admix_loglik_dev_workspace(g.I, g.J, 4)
+    work = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = lib.admix_loglik_dev(C.c_void_p(bed.data_ptr()), g.I, g.J, 4, C.c_void_p(q.data_ptr()),
+                              C.c_void_p(p.data_ptr()), C.c_void_p(out.data_ptr()),
+                              C.c_void_p(work.data_ptr()), nbytes, C.c_void_p(stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert out.item() == want          # same kernel, same plan: bit-identical
+    rc = lib.admix_loglik_dev(C.c_void_p(bed.data_ptr()), g.I, g.J, 4, C.c_void_p(q.data_ptr()),
+                              C.c_void_p(p.data_ptr()), C.c_void_p(out.data_ptr()),
+                              C.c_void_p(work.data_ptr()), 8, C.c_void_p(stream))
+    assert rc == N.ADMIX_ERR_ARG
+    d_cu.close()
+
+
+def test_error_paths(oa):
+    from openadmixture_b200 import _native as N
+    g = _cohort(oa, I=40, J=50, K=2)
+    d, d_cu = _handle(oa, g, 2)
+    lib = N.admix_lib()
+    v = C.c_double()
+    assert lib.admix_loglik(d_cu.handle, 7, C.byref(v)) == N.ADMIX_ERR_ARG
+    assert b"selector" in lib.admix_last_error(d_cu.handle)
+    assert lib.admix_qn_iteration(d_cu.handle, 0, None) == N.ADMIX_ERR_ARG
+    with pytest.raises(oa.AdmixError):
+        d_cu.loglik(9)
+    d_cu.close()
+
+
+def test_deterministic_across_runs(oa):
+    g = _cohort(oa, I=1000, J=5000, K=5, seed=3)
+    outs = []
+    for _ in range(2):
+        d, d_cu = _handle(oa, g, 5, seed=1)
+        oa.init_em(d, g, 2, d_cu=d_cu, quiet=True)
+        oa.admixture_qn(d, g, 3, 0.0, d_cu=d_cu, quiet=True)
+        outs.append((d.ll_new, d.x.copy()))
+        d_cu.close()
+    assert outs[0][0] == outs[1][0] and np.array_equal(outs[0][1], outs[1][1])
+
+
+# ------------------------------------------------------------------ full-size properties
+
+def test_c2_size_properties(oa):
+    """At the drop-in cohort's full size (I=10k, J=100k, K=5): missing counts equal a numpy
+    popcount of the bytes, the log-likelihood is additive over SNP blocks, EM increases it,
+    and the Q-side Hessian maps q to the gradient (XtX_q q = Xtz_q when sum q = 1)."""
+    import torch
+    from openadmixture_b200 import _native as N
+    spec = oa.COHORTS["c2"]
+    g, _, _ = oa.make_cohort(spec)
+    d, d_cu = _handle(oa, g, spec.K, seed=2)
+    snp, ind = d_cu.decode_counts()
+    b = g.data
+    miss = (b & ~(b >> 1) & 0x55)
+    pc = np.unpackbits(miss[:, :, None], axis=2).sum(axis=(1, 2))
+    assert np.array_equal(snp, pc.astype(np.int64))
+    assert ind.sum() == snp.sum()
+    ll = d_cu.loglik(oa.X)
+    lib = N.admix_lib()
+    dev = torch.device("cuda:0")
+    qd = torch.from_numpy(np.ascontiguousarray(d.x[: g.I])).to(dev)
+    parts = []
+    for j0, j1 in ((0, 37_000), (37_000, spec.J)):
+        bed = torch.from_numpy(np.ascontiguousarray(g.data[j0:j1])).to(dev)
+        pd = torch.from_numpy(np.ascontiguousarray(d.x[g.I + j0: g.I + j1])).to(dev)
+        out = torch.zeros(1, dtype=torch.float64, device=dev)
+        nb = lib.admix_loglik_dev_workspace(g.I, j1 - j0, spec.K)
+        work = torch.empty(nb, dtype=torch.uint8, device=dev)
+        assert lib.admix_loglik_dev(C.c_void_p(bed.data_ptr()), g.I, j1 - j0, spec.K, C.c_void_p(qd.data_ptr()),
+                                    C.c_void_p(pd.data_ptr()), C.c_void_p(out.data_ptr()),
+                                    C.c_void_p(work.data_ptr()), nb, None) == 0
+        torch.cuda.synchronize()
+        parts.append(out.item())
+    assert rel_err(sum(parts), ll) < 1e-12
+    hist = oa.init_em(d, g, 3, d_cu=d_cu, quiet=True)
+    assert hist[0] > ll and hist[1] > hist[0] and hist[2] > hist[1]
+    d_cu.upload(oa.X, d.x)
+    H, z = d_cu.grad_hess_q(oa.X, oa.X)
+    q = d.x[: g.I]
+    qn = q / q.sum(1, keepdims=True)
+    d.x[: g.I] = qn
+    d_cu.upload(oa.X, d.x)
+    H, z = d_cu.grad_hess_q(oa.X, oa.X)
+    assert _row_rel(np.einsum("ikl,il->ik", H, qn), z) < 1e-10
+    d_cu.close()
