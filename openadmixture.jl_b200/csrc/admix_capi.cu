@@ -315,7 +315,8 @@ extern "C" {
 int admix_loglik(admix_ctx *h, int32_t which, double *out)
 {
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
-    if (!valid_which(which) || !out) return fail(h, ADMIX_ERR_ARG, "invalid argument");
+    if (!valid_which(which)) return fail(h, ADMIX_ERR_ARG, "invalid buffer selector %d", which);
+    if (!out) return fail(h, ADMIX_ERR_ARG, "out is NULL");
     CK(h, enq_loglik(h, which, &h->sc->ll_tmp));
     CK(h, cudaMemcpyAsync(out, &h->sc->ll_tmp, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaStreamSynchronize(h->st));

@@ -229,7 +229,8 @@ def test_c2_size_properties(oa):
     snp, ind = d_cu.decode_counts()
     b = g.data
     miss = (b & ~(b >> 1) & 0x55)
-    pc = np.unpackbits(miss[:, :, None], axis=2).sum(axis=(1, 2))
+    lut = np.array([bin(v).count("1") for v in range(256)], dtype=np.uint8)
+    pc = lut[miss].sum(axis=1, dtype=np.int64)
     assert np.array_equal(snp, pc.astype(np.int64))
     assert ind.sum() == snp.sum()
     ll = d_cu.loglik(oa.X)
