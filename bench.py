@@ -43,7 +43,30 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ttc", action="store_true")
+    ap.add_argument("--pass-only", default=None,
+                    choices=["loglik", "q_sweep", "p_sweep", "q_qp", "p_qp", "em"],
+                    help="set up the cohort and launch one pass warmup+steps times (for profilers)")
     return ap.parse_args()
+
+
+def run_pass_only(args):
+    """One pass of the hot path launched 1 + steps times on the cohort (no EM, no QN loop):
+    the command the per-kernel ncu captures run."""
+    import torch
+    import openadmixture_b200 as oa
+    from openadmixture_b200 import _native as N
+    torch.cuda.set_device(0)
+    spec = oa.COHORTS[args.config]
+    g, _, _ = oa.make_cohort(spec)
+    d = oa.AdmixData(spec.I, spec.J, spec.K, 3, rng=100)
+    with oa.CuAdmixData(d, g) as d_cu:
+        pid = {"loglik": N.ADMIX_PASS_LOGLIK, "q_sweep": N.ADMIX_PASS_QSWEEP, "p_sweep": N.ADMIX_PASS_PSWEEP,
+               "q_qp": N.ADMIX_PASS_QQP, "p_qp": N.ADMIX_PASS_PQP, "em": N.ADMIX_PASS_EM}[args.pass_only]
+        if pid in (N.ADMIX_PASS_QQP, N.ADMIX_PASS_PQP):   # give the QPs real sweep outputs
+            d_cu.time_pass(N.ADMIX_PASS_QSWEEP if pid == N.ADMIX_PASS_QQP else N.ADMIX_PASS_PSWEEP, 1)
+        ms = d_cu.time_pass(pid, max(1, args.steps))
+    print(json.dumps({"pass": args.pass_only, "config": spec.name, "ms_per_launch": ms}), flush=True)
+    return 0
 
 
 def _peaks():
@@ -360,6 +383,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.pass_only:
+        return run_pass_only(args)
     return run_ours(args, rank, world, local_rank)
 
 
