@@ -163,6 +163,20 @@ int admix_loglik_dev(const uint8_t *d_bed, int64_t I, int64_t J, int32_t K,
                      const double *d_q, const double *d_p, double *d_out,
                      void *d_work, size_t work_bytes, void *stream);
 
+/* No counterpart in the reference.  admix_loglik_dev for callers that cannot allocate device
+ * memory (their device memory comes only from a pool they do not control, or they must not
+ * pay cudaMalloc's implicit synchronisation): the partial sums live in a fixed array inside
+ * the library, ADMIX_NOALLOC_MAX_PARTIALS doubles (256 KiB) held by every GPU that loads it.
+ * Cohorts needing more partial sums (I beyond about 33 million) are rejected with
+ * ADMIX_ERR_UNSUPPORTED.  The first call on a device looks up the array's device address
+ * (make it before any stream capture).  All calls share the array: calls that overlap on the
+ * GPU race, so serialise them.  Asynchronous on `stream`; errors are reported by
+ * admix_noalloc_last_error(). */
+#define ADMIX_NOALLOC_MAX_PARTIALS 32768
+int admix_loglik_dev_noalloc(const uint8_t *d_bed, int64_t I, int64_t J, int32_t K,
+                             const double *d_q, const double *d_p, double *d_out, void *stream);
+const char *admix_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

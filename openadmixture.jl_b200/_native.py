@@ -80,6 +80,8 @@ ADMIX_SIGNATURES = {
     "admix_iteration_kernels": (C.c_int, [_P, _I32]),
     "admix_loglik_dev_workspace": (C.c_size_t, [C.c_int64, C.c_int64, C.c_int32]),
     "admix_loglik_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_size_t, _P]),
+    "admix_loglik_dev_noalloc": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
+    "admix_noalloc_last_error": (C.c_char_p, []),
 }
 
 SYNTH_SIGNATURES = {

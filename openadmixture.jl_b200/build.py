@@ -1,6 +1,6 @@
 """Build the in-tree native libraries for sm_100a.
 
-    lib/libadmix.so        the C-ABI engine (include/admix.h): csrc/{admix_capi,sweeps_f64,qp_batch,qn}.cu
+    lib/libadmix.so        the C-ABI engine (include/admix.h): csrc/{admix_capi,sweeps_f64,qp_batch,qn,loglik_noalloc}.cu
     lib/libadmix_synth.so  seeded synthetic-cohort generator (csrc/synth.cu), host + device
 
 Each translation unit is compiled separately (in parallel) with nvcc for
@@ -22,7 +22,7 @@ OBJ = PKG / "_build"
 REPO = PKG.parent
 INCLUDE = REPO / "include"
 
-ENGINE_SOURCES = ["admix_capi.cu", "sweeps_f64.cu", "qp_batch.cu", "qn.cu"]
+ENGINE_SOURCES = ["admix_capi.cu", "sweeps_f64.cu", "qp_batch.cu", "qn.cu", "loglik_noalloc.cu"]
 SYNTH_SOURCES = ["synth.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
