@@ -41,6 +41,8 @@ def _args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--config", default="c2")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
+                    help="plain: FP64 sweeps; mixed: tensor-core BF16 Hessian, FP32 gradient")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ttc", action="store_true")
     ap.add_argument("--pass-only", default=None,
@@ -59,7 +61,8 @@ def run_pass_only(args):
     spec = oa.COHORTS[args.config]
     g, _, _ = oa.make_cohort(spec)
     d = oa.AdmixData(spec.I, spec.J, spec.K, 3, rng=100)
-    with oa.CuAdmixData(d, g) as d_cu:
+    flags = oa.ADMIX_FLAG_MIXED if args.form == "mixed" else 0
+    with oa.CuAdmixData(d, g, flags=flags) as d_cu:
         pid = {"loglik": N.ADMIX_PASS_LOGLIK, "q_sweep": N.ADMIX_PASS_QSWEEP, "p_sweep": N.ADMIX_PASS_PSWEEP,
                "q_qp": N.ADMIX_PASS_QQP, "p_qp": N.ADMIX_PASS_PQP, "em": N.ADMIX_PASS_EM}[args.pass_only]
         if pid in (N.ADMIX_PASS_QQP, N.ADMIX_PASS_PQP):   # give the QPs real sweep outputs
@@ -222,7 +225,8 @@ def run_ours(args, rank, world, local_rank):
     d = oa.AdmixData(spec.I, spec.J, spec.K, 3, rng=100 + rank)
     x_init = d.x.copy()
     t0 = time.perf_counter()
-    d_cu = oa.CuAdmixData(d, g)
+    flags = oa.ADMIX_FLAG_MIXED if args.form == "mixed" else 0
+    d_cu = oa.CuAdmixData(d, g, flags=flags)
     t_upload = time.perf_counter() - t0
     oa.init_em(d, g, 5, d_cu=d_cu, quiet=True)
     x_em, ll_em = d.x.copy(), d.ll_new
@@ -267,7 +271,7 @@ def run_ours(args, rank, world, local_rank):
         passes[name] = d_cu.time_pass(pid, 5)
     per_iter = {k: 2 * v for k, v in passes.items()}
     dom = max(per_iter, key=per_iter.get)
-    kern_name = {"loglik": "k_loglik_f64", "q_sweep": "k_sweep_q_f64", "p_sweep": "k_sweep_p_f64",
+    kern_name = {"loglik": "k_loglik_f64", "q_sweep": "k_sweep_q_mixed" if args.form == "mixed" else "k_sweep_q_f64", "p_sweep": "k_sweep_p_f64",
                  "q_qp": "k_qp", "p_qp": "k_qp"}[dom]
     Ib = (spec.I + 3) // 4
     K = spec.K

@@ -37,7 +37,7 @@ struct admix_ctx {
     int32_t *iter_host = nullptr;    /* pinned */
     unsigned long long *counts = nullptr;
     LoglikPlan llp;
-    SweepPlan sq, sp;
+    SweepPlan sq, sp, sqm;          /* sqm: mixed-precision Q sweep */
     QNPlan qnp;
     size_t bytes = 0;
     cudaGraphExec_t iter_graph = nullptr;
@@ -129,8 +129,6 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
     if (!bed) return fail(nullptr, ADMIX_ERR_ARG, "bed is NULL");
     if (flags & ~(ADMIX_FLAG_MU_GERSHGORIN | ADMIX_FLAG_MIXED))
         return fail(nullptr, ADMIX_ERR_ARG, "unknown flags 0x%x", flags);
-    if (flags & ADMIX_FLAG_MIXED)
-        return fail(nullptr, ADMIX_ERR_UNSUPPORTED, "ADMIX_FLAG_MIXED is not available in this build");
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
     if (ce != cudaSuccess || ndev == 0)
@@ -147,18 +145,20 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
     TRYC(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
     TRYC(prepare_sweeps(K));
     TRYC(prepare_qp(K));
+    if (flags & ADMIX_FLAG_MIXED) TRYC(prepare_mixed(K));
 
     const int64_t nx = (int64_t)K * (I + J);
     const int T = K * (K + 1) / 2, E = T + K;
     h->llp = plan_loglik(I, J, h->sms);
     h->sq = plan_sweep_q(K, I, J, h->sms);
     h->sp = plan_sweep_p(K, I, J, h->sms);
+    h->sqm = plan_sweep_q_mixed(K, I, J, h->sms);
     h->qnp = plan_qn(nx, h->sms);
 
     TRY(dalloc(h, &h->bed, (size_t)h->Ib * J));
     TRY(dalloc(h, &h->xbuf, (size_t)4 * nx));
     for (int w = 0; w < 4; ++w) h->x[w] = h->xbuf + (size_t)w * nx;
-    TRY(dalloc(h, &h->parts_q, (size_t)h->sq.S * I * E));
+    TRY(dalloc(h, &h->parts_q, (size_t)std::max(h->sq.S, (flags & ADMIX_FLAG_MIXED) ? h->sqm.S : 1) * I * E));
     TRY(dalloc(h, &h->parts_p, (size_t)h->sp.S * J * E));
     TRY(dalloc(h, &h->U, (size_t)nx * Q));
     TRY(dalloc(h, &h->V, (size_t)nx * Q));
@@ -252,15 +252,28 @@ static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst)
                              h->ll_partial, dst, h->st);
 }
 
+/* Q-side gradient / Hessian sweep into parts_q; returns the number of slices written. */
+static cudaError_t enq_sweep_q(admix_ctx *h, int wq, int wp, int *S)
+{
+    if (h->flags & ADMIX_FLAG_MIXED) {
+        *S = h->sqm.S;
+        return launch_sweep_q_mixed(h->K, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sqm, h->parts_q,
+                                    &h->sc->tc_err, h->st);
+    }
+    *S = h->sq.S;
+    return launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
+}
+
 /* update_q!: q_out = project_q(q + QP(H_q, -Xtz_q)) */
 static cudaError_t enq_update_q(admix_ctx *h, int update2)
 {
     const int wq = update2 ? ADMIX_X_NEXT : ADMIX_X;
     const int wp = update2 ? ADMIX_X_NEXT : ADMIX_X;
     const int wo = update2 ? ADMIX_X_NEXT2 : ADMIX_X_NEXT;
-    cudaError_t e = launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
+    int S = 1;
+    cudaError_t e = enq_sweep_q(h, wq, wp, &S);
     if (e != cudaSuccess) return e;
-    return launch_qp(h->K, true, h->I, h->parts_q, h->sq.S, Qof(h, wq), Qof(h, wo), h->status_q,
+    return launch_qp(h->K, true, h->I, h->parts_q, S, Qof(h, wq), Qof(h, wo), h->status_q,
                      &h->sc->fail_q, h->vt, (h->flags & ADMIX_FLAG_MU_GERSHGORIN) ? 1 : 0, h->st);
 }
 
@@ -371,8 +384,9 @@ static int grad_hess_common(admix_ctx *h, bool qside, int32_t wq, int32_t wp, do
     }
     cudaError_t e;
     if (qside) {
-        e = launch_sweep_q_f64(K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
-        if (e == cudaSuccess) e = launch_expand_hess(nprob, K, h->sq.S, h->parts_q, d_XtX, d_Xtz, h->sms, h->st);
+        int S = 1;
+        e = enq_sweep_q(h, wq, wp, &S);
+        if (e == cudaSuccess) e = launch_expand_hess(nprob, K, S, h->parts_q, d_XtX, d_Xtz, h->sms, h->st);
     } else {
         e = launch_sweep_p_f64(K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
         if (e == cudaSuccess) e = launch_expand_hess(nprob, K, h->sp.S, h->parts_p, d_XtX, d_Xtz, h->sms, h->st);
@@ -500,9 +514,9 @@ int admix_time_pass(admix_ctx *h, int32_t pass, int32_t reps, double *ms_per_lau
     auto one = [&]() -> cudaError_t {
         switch (pass) {
         case ADMIX_PASS_LOGLIK: return enq_loglik(h, ADMIX_X, &h->sc->ll_tmp);
-        case ADMIX_PASS_QSWEEP: return launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st);
+        case ADMIX_PASS_QSWEEP: { int S; return enq_sweep_q(h, ADMIX_X, ADMIX_X, &S); }
         case ADMIX_PASS_PSWEEP: return launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st);
-        case ADMIX_PASS_QQP: return launch_qp(h->K, true, h->I, h->parts_q, h->sq.S, Qof(h, ADMIX_X), Qof(h, ADMIX_X_TMP), h->status_q, nullptr, h->vt, mu, h->st);
+        case ADMIX_PASS_QQP: return launch_qp(h->K, true, h->I, h->parts_q, (h->flags & ADMIX_FLAG_MIXED) ? h->sqm.S : h->sq.S, Qof(h, ADMIX_X), Qof(h, ADMIX_X_TMP), h->status_q, nullptr, h->vt, mu, h->st);
         case ADMIX_PASS_PQP: return launch_qp(h->K, false, h->J, h->parts_p, h->sp.S, Pof(h, ADMIX_X), Pof(h, ADMIX_X_TMP), h->status_p, nullptr, h->vt, 0, h->st);
         default: return enq_em(h);
         }

@@ -17,7 +17,8 @@ struct DevScalars {
     int32_t accepted;
     int32_t fail_q, fail_p;
     int32_t qn_singular;
-    int32_t pad[3];
+    int32_t tc_err;                /* set by a tensor-core kernel whose bounded wait ran out */
+    int32_t pad[2];
 };
 
 /* 2-bit code -> genotype value (loops.jl:2-5): 00->0, 01->0 (missing), 10->1, 11->2 */

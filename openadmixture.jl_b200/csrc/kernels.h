@@ -35,6 +35,13 @@ cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J,
                                  unsigned long long *miss_snp, unsigned long long *miss_ind,
                                  int sms, cudaStream_t st);
 
+/* mixed-precision sweeps on tensor cores (sweeps_mixed.cu) */
+cudaError_t prepare_mixed(int K);
+SweepPlan plan_sweep_q_mixed(int K, int64_t I, int64_t J, int sms);
+cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+                                 const double *p, const SweepPlan &pl, double *out, int *err,
+                                 cudaStream_t st);
+
 /* batched QP + projection (qp_batch.cu) */
 cudaError_t prepare_qp(int K);
 cudaError_t launch_qp(int K, bool simplex, int64_t nprob, const double *parts, int S,
