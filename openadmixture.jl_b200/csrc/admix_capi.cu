@@ -37,7 +37,7 @@ struct admix_ctx {
     int32_t *iter_host = nullptr;    /* pinned */
     unsigned long long *counts = nullptr;
     LoglikPlan llp;
-    SweepPlan sq, sp, sqm;          /* sqm: mixed-precision Q sweep */
+    SweepPlan sq, sp, sqm, spm, llm; /* *m: mixed-precision Q sweep, P sweep, loglik */
     QNPlan qnp;
     size_t bytes = 0;
     cudaGraphExec_t iter_graph = nullptr;
@@ -153,19 +153,21 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
     h->sq = plan_sweep_q(K, I, J, h->sms);
     h->sp = plan_sweep_p(K, I, J, h->sms);
     h->sqm = plan_sweep_q_mixed(K, I, J, h->sms);
+    h->spm = plan_sweep_p_mixed(K, I, J, h->sms);
+    h->llm = plan_loglik_mixed(I, J, h->sms);
     h->qnp = plan_qn(nx, h->sms);
 
     TRY(dalloc(h, &h->bed, (size_t)h->Ib * J));
     TRY(dalloc(h, &h->xbuf, (size_t)4 * nx));
     for (int w = 0; w < 4; ++w) h->x[w] = h->xbuf + (size_t)w * nx;
     TRY(dalloc(h, &h->parts_q, (size_t)std::max(h->sq.S, (flags & ADMIX_FLAG_MIXED) ? h->sqm.S : 1) * I * E));
-    TRY(dalloc(h, &h->parts_p, (size_t)h->sp.S * J * E));
+    TRY(dalloc(h, &h->parts_p, (size_t)std::max(h->sp.S, (flags & ADMIX_FLAG_MIXED) ? h->spm.S : 1) * J * E));
     TRY(dalloc(h, &h->U, (size_t)nx * Q));
     TRY(dalloc(h, &h->V, (size_t)nx * Q));
     TRY(dalloc(h, &h->vt, (size_t)K * K));
     TRY(dalloc(h, &h->status_q, (size_t)I));
     TRY(dalloc(h, &h->status_p, (size_t)J));
-    TRY(dalloc(h, &h->ll_partial, (size_t)h->llp.gx * h->llp.gy));
+    TRY(dalloc(h, &h->ll_partial, std::max((size_t)h->llp.gx * h->llp.gy, (size_t)h->llm.gx * h->llm.S)));
     TRY(dalloc(h, &h->qn_partial, (size_t)h->qnp.blocks * (Q * Q + Q)));
     TRY(dalloc(h, &h->sc, 1));
     TRY(dalloc(h, &h->counts, (size_t)(I + J)));
@@ -246,8 +248,12 @@ int admix_get_ll(admix_ctx *h, double *ll_new)
 
 /* ---- stream-ordered building blocks (no synchronisation) ---- */
 
-static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst)
+/* FP64 log-likelihood (the verifier); fast = 1 selects the FP32-cell form in mixed mode */
+static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst, bool fast = false)
 {
+    if (fast && (h->flags & ADMIX_FLAG_MIXED))
+        return launch_loglik_mixed(h->K, h->bed, h->I, h->J, Qof(h, which), Pof(h, which), h->llm,
+                                   h->ll_partial, dst, h->st);
     return launch_loglik_f64(h->K, h->bed, h->I, h->J, Qof(h, which), Pof(h, which), h->llp,
                              h->ll_partial, dst, h->st);
 }
@@ -262,6 +268,18 @@ static cudaError_t enq_sweep_q(admix_ctx *h, int wq, int wp, int *S)
     }
     *S = h->sq.S;
     return launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
+}
+
+/* P-side gradient / Hessian sweep into parts_p; returns the number of slices written. */
+static cudaError_t enq_sweep_p(admix_ctx *h, int wq, int wp, int *S)
+{
+    if (h->flags & ADMIX_FLAG_MIXED) {
+        *S = h->spm.S;
+        return launch_sweep_p_mixed(h->K, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->spm, h->parts_p,
+                                    &h->sc->tc_err, h->st);
+    }
+    *S = h->sp.S;
+    return launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
 }
 
 /* update_q!: q_out = project_q(q + QP(H_q, -Xtz_q)) */
@@ -283,9 +301,10 @@ static cudaError_t enq_update_p(admix_ctx *h, int update2)
     const int wq = update2 ? ADMIX_X_NEXT2 : ADMIX_X_NEXT;
     const int wp = update2 ? ADMIX_X_NEXT : ADMIX_X;
     const int wo = update2 ? ADMIX_X_NEXT2 : ADMIX_X_NEXT;
-    cudaError_t e = launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
+    int S = 1;
+    cudaError_t e = enq_sweep_p(h, wq, wp, &S);
     if (e != cudaSuccess) return e;
-    return launch_qp(h->K, false, h->J, h->parts_p, h->sp.S, Pof(h, wp), Pof(h, wo), h->status_p,
+    return launch_qp(h->K, false, h->J, h->parts_p, S, Pof(h, wp), Pof(h, wo), h->status_p,
                      &h->sc->fail_p, h->vt, 0, h->st);
 }
 
@@ -308,10 +327,10 @@ static cudaError_t enq_iteration(admix_ctx *h)
     if (e == cudaSuccess) e = enq_update_p(h, 0);
     if (e == cudaSuccess) e = enq_update_q(h, 1);
     if (e == cudaSuccess) e = enq_update_p(h, 1);
-    if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_NEXT2, &h->sc->ll_basic);
+    if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_NEXT2, &h->sc->ll_basic, true);
     if (e == cudaSuccess) e = launch_qn(h->Q, h->I, h->J, h->K, h->x[ADMIX_X], h->x[ADMIX_X_NEXT], h->x[ADMIX_X_NEXT2],
                                         h->U, h->V, h->x[ADMIX_X_TMP], h->qn_partial, h->qnp, h->sc, h->sms, h->st);
-    if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_TMP, &h->sc->ll_qn);
+    if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_TMP, &h->sc->ll_qn, true);
     if (e == cudaSuccess) e = launch_accept(nx, h->x[ADMIX_X_TMP], h->x[ADMIX_X_NEXT2], h->x[ADMIX_X], h->sc, h->sms, h->st);
     return e;
 }
@@ -388,8 +407,9 @@ static int grad_hess_common(admix_ctx *h, bool qside, int32_t wq, int32_t wp, do
         e = enq_sweep_q(h, wq, wp, &S);
         if (e == cudaSuccess) e = launch_expand_hess(nprob, K, S, h->parts_q, d_XtX, d_Xtz, h->sms, h->st);
     } else {
-        e = launch_sweep_p_f64(K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
-        if (e == cudaSuccess) e = launch_expand_hess(nprob, K, h->sp.S, h->parts_p, d_XtX, d_Xtz, h->sms, h->st);
+        int S = 1;
+        e = enq_sweep_p(h, wq, wp, &S);
+        if (e == cudaSuccess) e = launch_expand_hess(nprob, K, S, h->parts_p, d_XtX, d_Xtz, h->sms, h->st);
     }
     if (e == cudaSuccess && XtX) e = cudaMemcpyAsync(XtX, d_XtX, sizeof(double) * K * K * nprob, cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess && Xtz) e = cudaMemcpyAsync(Xtz, d_Xtz, sizeof(double) * K * nprob, cudaMemcpyDeviceToHost, h->st);
@@ -513,11 +533,11 @@ int admix_time_pass(admix_ctx *h, int32_t pass, int32_t reps, double *ms_per_lau
     const int mu = (h->flags & ADMIX_FLAG_MU_GERSHGORIN) ? 1 : 0;
     auto one = [&]() -> cudaError_t {
         switch (pass) {
-        case ADMIX_PASS_LOGLIK: return enq_loglik(h, ADMIX_X, &h->sc->ll_tmp);
+        case ADMIX_PASS_LOGLIK: return enq_loglik(h, ADMIX_X, &h->sc->ll_tmp, true);
         case ADMIX_PASS_QSWEEP: { int S; return enq_sweep_q(h, ADMIX_X, ADMIX_X, &S); }
-        case ADMIX_PASS_PSWEEP: return launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st);
+        case ADMIX_PASS_PSWEEP: { int S; return enq_sweep_p(h, ADMIX_X, ADMIX_X, &S); }
         case ADMIX_PASS_QQP: return launch_qp(h->K, true, h->I, h->parts_q, (h->flags & ADMIX_FLAG_MIXED) ? h->sqm.S : h->sq.S, Qof(h, ADMIX_X), Qof(h, ADMIX_X_TMP), h->status_q, nullptr, h->vt, mu, h->st);
-        case ADMIX_PASS_PQP: return launch_qp(h->K, false, h->J, h->parts_p, h->sp.S, Pof(h, ADMIX_X), Pof(h, ADMIX_X_TMP), h->status_p, nullptr, h->vt, 0, h->st);
+        case ADMIX_PASS_PQP: return launch_qp(h->K, false, h->J, h->parts_p, (h->flags & ADMIX_FLAG_MIXED) ? h->spm.S : h->sp.S, Pof(h, ADMIX_X), Pof(h, ADMIX_X_TMP), h->status_p, nullptr, h->vt, 0, h->st);
         default: return enq_em(h);
         }
     };

@@ -42,6 +42,15 @@ cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J
                                  const double *p, const SweepPlan &pl, double *out, int *err,
                                  cudaStream_t st);
 
+SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms);
+cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+                                 const double *p, const SweepPlan &pl, double *out, int *err,
+                                 cudaStream_t st);
+SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms);
+cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+                                const double *p, const SweepPlan &pl, double *partial, double *out,
+                                cudaStream_t st);
+
 /* batched QP + projection (qp_batch.cu) */
 cudaError_t prepare_qp(int K);
 cudaError_t launch_qp(int K, bool simplex, int64_t nprob, const double *parts, int S,

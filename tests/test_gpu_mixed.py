@@ -64,3 +64,40 @@ def test_mixed_run_reaches_fp64_optimum(oa, K):
             h.upload(oa.X, d.x)
             finals.append(h.loglik(oa.X))     # FP64 verifier
     assert rel_err(finals[1], finals[0]) < 1e-6
+
+
+@pytest.mark.parametrize("K", [1, 2, 3, 5, 8, 12, 16])
+def test_mixed_p_sweep_matches_fp64(oa, K):
+    g, d, h64, hmx = _pair(oa, I=1037, J=517, K=K, seed=80 + K)   # partial individual chunk and SNP tile
+    H0, z0 = h64.grad_hess_p(oa.X, oa.X)
+    H1, z1 = hmx.grad_hess_p(oa.X, oa.X)
+    assert np.all(np.isfinite(H1)) and np.all(np.isfinite(z1))
+    assert _row_rel(z1, z0) < 1e-4
+    assert _row_rel(H1, H0) < HESS_TOL
+    h64.close(); hmx.close()
+
+
+def test_mixed_p_sweep_c2_size(oa):
+    g, d, h64, hmx = _pair(oa, I=10_000, J=100_000, K=5, seed=3, cfg="c2")
+    H0, z0 = h64.grad_hess_p(oa.X, oa.X)
+    H1, z1 = hmx.grad_hess_p(oa.X, oa.X)
+    assert _row_rel(z1, z0) < 1e-4
+    assert _row_rel(H1, H0) < HESS_TOL
+    h64.close(); hmx.close()
+
+
+@pytest.mark.parametrize("K,I,J", [(3, 777, 2001), (8, 1000, 3000), (12, 333, 1500)])
+def test_mixed_loglik_in_iteration_matches_fp64_verifier(oa, K, I, J):
+    """In the mixed form the iteration's log-likelihoods use FP32 cells with an FP64 reduction;
+    they agree with the FP64 verifier (admix_loglik) to 1e-8 relative (FP32 rounding of q and p
+    moves each cell's log by ~1e-7 relative, correlated along rows and columns)."""
+    spec = oa.COHORTS["c1"].scaled(I=I, J=J, K=K, seed=90 + K)
+    g, _, _ = oa.make_cohort(spec)
+    d = oa.AdmixData(I, J, K, 3, rng=4)
+    with oa.CuAdmixData(d, g, flags=oa.ADMIX_FLAG_MIXED) as h:
+        oa.init_em(d, g, 2, d_cu=h, quiet=True)
+        recs = oa.admixture_qn(d, g, 2, 0.0, d_cu=h, quiet=True)
+        ll_basic = recs[-1]["ll_basic"]
+        ll_qn = recs[-1]["ll_qn"]
+        assert rel_err(ll_basic, h.loglik(oa.X_NEXT2)) < 1e-8
+        assert rel_err(ll_qn, h.loglik(oa.X_TMP)) < 1e-8
