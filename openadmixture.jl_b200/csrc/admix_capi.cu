@@ -21,6 +21,7 @@
 
 struct admix_ctx {
     int64_t I = 0, J = 0, Ib = 0;
+    int64_t pitch = 0;               /* column stride of the device genotypes: Ib rounded up to 16 */
     int K = 0, Q = 0;
     uint32_t flags = 0;
     int dev = 0, sms = 148;
@@ -137,6 +138,7 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
     admix_ctx *h = new admix_ctx();
     h->I = I; h->J = J; h->K = K; h->Q = Q; h->flags = flags;
     h->Ib = (I + 3) / 4;
+    h->pitch = (h->Ib + 15) / 16 * 16;
     int rc;
 #define TRY(x) do { rc = (x); if (rc != ADMIX_OK) { strncpy(g_err, h->err, sizeof(g_err) - 1); release(h); delete h; return rc; } } while (0)
 #define TRYC(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { fail(nullptr, ADMIX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); release(h); delete h; return ADMIX_ERR_CUDA; } } while (0)
@@ -157,7 +159,7 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
     h->llm = plan_loglik_mixed(I, J, h->sms);
     h->qnp = plan_qn(nx, h->sms);
 
-    TRY(dalloc(h, &h->bed, (size_t)h->Ib * J));
+    TRY(dalloc(h, &h->bed, (size_t)h->pitch * J + 64));
     TRY(dalloc(h, &h->xbuf, (size_t)4 * nx));
     for (int w = 0; w < 4; ++w) h->x[w] = h->xbuf + (size_t)w * nx;
     TRY(dalloc(h, &h->parts_q, (size_t)std::max(h->sq.S, (flags & ADMIX_FLAG_MIXED) ? h->sqm.S : 1) * I * E));
@@ -174,7 +176,12 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
     TRYC(cudaMallocHost((void **)&h->sc_host, sizeof(DevScalars)));
     TRYC(cudaMallocHost((void **)&h->iter_host, sizeof(int32_t)));
 
-    TRYC(cudaMemcpyAsync(h->bed, bed, (size_t)h->Ib * J, cudaMemcpyHostToDevice, h->st));
+    /* genotypes in HBM: columns at a 16-byte pitch, padding bytes and the padding bits of each
+     * column's last byte set to the missing code 01 (never read by the reference's loops) */
+    TRYC(cudaMemsetAsync(h->bed, 0x55, (size_t)h->pitch * J + 64, h->st));
+    TRYC(cudaMemcpy2DAsync(h->bed, (size_t)h->pitch, bed, (size_t)h->Ib, (size_t)h->Ib, (size_t)J,
+                           cudaMemcpyHostToDevice, h->st));
+    TRYC(launch_mask_tail(h->bed, I, J, h->pitch, h->sms, h->st));
     TRYC(cudaMemsetAsync(h->xbuf, 0, sizeof(double) * 4 * nx, h->st));
     TRYC(cudaMemsetAsync(h->U, 0, sizeof(double) * nx * Q, h->st));
     TRYC(cudaMemsetAsync(h->V, 0, sizeof(double) * nx * Q, h->st));
@@ -252,9 +259,9 @@ int admix_get_ll(admix_ctx *h, double *ll_new)
 static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst, bool fast = false)
 {
     if (fast && (h->flags & ADMIX_FLAG_MIXED))
-        return launch_loglik_mixed(h->K, h->bed, h->I, h->J, Qof(h, which), Pof(h, which), h->llm,
+        return launch_loglik_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, which), Pof(h, which), h->llm,
                                    h->ll_partial, dst, h->st);
-    return launch_loglik_f64(h->K, h->bed, h->I, h->J, Qof(h, which), Pof(h, which), h->llp,
+    return launch_loglik_f64(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, which), Pof(h, which), h->llp,
                              h->ll_partial, dst, h->st);
 }
 
@@ -263,11 +270,11 @@ static cudaError_t enq_sweep_q(admix_ctx *h, int wq, int wp, int *S)
 {
     if (h->flags & ADMIX_FLAG_MIXED) {
         *S = h->sqm.S;
-        return launch_sweep_q_mixed(h->K, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sqm, h->parts_q,
+        return launch_sweep_q_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sqm, h->parts_q,
                                     &h->sc->tc_err, h->st);
     }
     *S = h->sq.S;
-    return launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
+    return launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
 }
 
 /* P-side gradient / Hessian sweep into parts_p; returns the number of slices written. */
@@ -275,11 +282,11 @@ static cudaError_t enq_sweep_p(admix_ctx *h, int wq, int wp, int *S)
 {
     if (h->flags & ADMIX_FLAG_MIXED) {
         *S = h->spm.S;
-        return launch_sweep_p_mixed(h->K, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->spm, h->parts_p,
+        return launch_sweep_p_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->spm, h->parts_p,
                                     &h->sc->tc_err, h->st);
     }
     *S = h->sp.S;
-    return launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
+    return launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
 }
 
 /* update_q!: q_out = project_q(q + QP(H_q, -Xtz_q)) */
@@ -311,9 +318,9 @@ static cudaError_t enq_update_p(admix_ctx *h, int update2)
 static cudaError_t enq_em(admix_ctx *h)
 {
     /* em_q! then em_p! (mode :base, both from (q, p)), then p, q <- next (algorithms_outer.jl:23-30) */
-    cudaError_t e = launch_sweep_q_f64(h->K, 1, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st);
+    cudaError_t e = launch_sweep_q_f64(h->K, 1, h->bed, h->I, h->J, h->pitch, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st);
     if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st);
-    if (e == cudaSuccess) e = launch_sweep_p_f64(h->K, 1, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st);
+    if (e == cudaSuccess) e = launch_sweep_p_f64(h->K, 1, h->bed, h->I, h->J, h->pitch, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st);
     if (e == cudaSuccess) e = launch_emp_finalize(h->J, h->K, h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st);
     return e;
 }
@@ -358,7 +365,7 @@ int admix_loglik(admix_ctx *h, int32_t which, double *out)
 int admix_em_q(admix_ctx *h)
 {
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
-    CK(h, launch_sweep_q_f64(h->K, 1, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st));
+    CK(h, launch_sweep_q_f64(h->K, 1, h->bed, h->I, h->J, h->pitch, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st));
     CK(h, launch_emq_finalize(h->I, h->K, h->J, h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st));
     CK(h, cudaStreamSynchronize(h->st));
     return ADMIX_OK;
@@ -367,7 +374,7 @@ int admix_em_q(admix_ctx *h)
 int admix_em_p(admix_ctx *h)
 {
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
-    CK(h, launch_sweep_p_f64(h->K, 1, h->bed, h->I, h->J, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st));
+    CK(h, launch_sweep_p_f64(h->K, 1, h->bed, h->I, h->J, h->pitch, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st));
     CK(h, launch_emp_finalize(h->J, h->K, h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st));
     CK(h, cudaStreamSynchronize(h->st));
     return ADMIX_OK;
@@ -588,7 +595,7 @@ int admix_decode_counts(admix_ctx *h, int64_t *miss_per_snp, int64_t *miss_per_i
 {
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
     CK(h, cudaMemsetAsync(h->counts, 0, sizeof(unsigned long long) * (h->I + h->J), h->st));
-    CK(h, launch_decode_counts(h->bed, h->I, h->J, h->counts + h->I, h->counts, h->sms, h->st));
+    CK(h, launch_decode_counts(h->bed, h->I, h->J, h->pitch, h->counts + h->I, h->counts, h->sms, h->st));
     if (miss_per_snp) CK(h, cudaMemcpyAsync(miss_per_snp, h->counts + h->I, sizeof(int64_t) * h->J, cudaMemcpyDeviceToHost, h->st));
     if (miss_per_ind) CK(h, cudaMemcpyAsync(miss_per_ind, h->counts, sizeof(int64_t) * h->I, cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaStreamSynchronize(h->st));
@@ -618,7 +625,7 @@ int admix_loglik_dev(const uint8_t *d_bed, int64_t I, int64_t J, int32_t K, cons
     if (work_bytes < sizeof(double) * (size_t)pl.gx * pl.gy)
         return fail(nullptr, ADMIX_ERR_ARG, "workspace of %zu bytes is below the %zu required", work_bytes,
                     sizeof(double) * (size_t)pl.gx * pl.gy);
-    cudaError_t e = launch_loglik_f64(K, d_bed, I, J, d_q, d_p, pl, (double *)d_work, d_out, (cudaStream_t)stream);
+    cudaError_t e = launch_loglik_f64(K, d_bed, I, J, (I + 3) / 4, d_q, d_p, pl, (double *)d_work, d_out, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail(nullptr, ADMIX_ERR_CUDA, "loglik launch failed: %s", cudaGetErrorString(e));
     return ADMIX_OK;
 }

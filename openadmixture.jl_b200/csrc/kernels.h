@@ -16,13 +16,13 @@ SweepPlan plan_sweep_p(int K, int64_t I, int64_t J, int sms);
 
 /* FP64 sweeps (sweeps_f64.cu) */
 cudaError_t prepare_sweeps(int K);
-cudaError_t launch_loglik_f64(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+cudaError_t launch_loglik_f64(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                               const double *p, const LoglikPlan &pl, double *partial, double *out,
                               cudaStream_t st);
-cudaError_t launch_sweep_q_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J,
+cudaError_t launch_sweep_q_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                const double *q, const double *p, const SweepPlan &pl, double *out,
                                cudaStream_t st);
-cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J,
+cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                const double *q, const double *p, const SweepPlan &pl, double *out,
                                cudaStream_t st);
 cudaError_t launch_emq_finalize(int64_t I, int K, int64_t J, int S, const double *parts,
@@ -31,25 +31,27 @@ cudaError_t launch_emp_finalize(int64_t J, int K, int S, const double *parts, co
                                 double *p_next, int sms, cudaStream_t st);
 cudaError_t launch_expand_hess(int64_t nprob, int K, int S, const double *parts, double *XtX,
                                double *Xtz, int sms, cudaStream_t st);
-cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J,
+cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                  unsigned long long *miss_snp, unsigned long long *miss_ind,
                                  int sms, cudaStream_t st);
 
 /* mixed-precision sweeps on tensor cores (sweeps_mixed.cu) */
 cudaError_t prepare_mixed(int K);
 SweepPlan plan_sweep_q_mixed(int K, int64_t I, int64_t J, int sms);
-cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                  const double *p, const SweepPlan &pl, double *out, int *err,
                                  cudaStream_t st);
 
 SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms);
-cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                  const double *p, const SweepPlan &pl, double *out, int *err,
                                  cudaStream_t st);
 SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms);
-cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                 const double *p, const SweepPlan &pl, double *partial, double *out,
                                 cudaStream_t st);
+
+cudaError_t launch_mask_tail(uint8_t *bed, int64_t I, int64_t J, int64_t pitch, int sms, cudaStream_t st);
 
 /* batched QP + projection (qp_batch.cu) */
 cudaError_t prepare_qp(int K);

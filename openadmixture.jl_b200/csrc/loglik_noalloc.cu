@@ -76,7 +76,7 @@ extern "C" int admix_loglik_dev_noalloc(const uint8_t *d_bed, int64_t I, int64_t
         }
         scratch = g_scratch[dev];
     }
-    cudaError_t e = launch_loglik_f64(K, d_bed, I, J, d_q, d_p, pl, (double *)scratch, d_out,
+    cudaError_t e = launch_loglik_f64(K, d_bed, I, J, (I + 3) / 4, d_q, d_p, pl, (double *)scratch, d_out,
                                       (cudaStream_t)stream);
     if (e != cudaSuccess) return noalloc_fail(ADMIX_ERR_CUDA, cudaGetErrorString(e));
     return ADMIX_OK;

@@ -20,7 +20,7 @@
  * the reference's g log qp + (2-g) log(1-qp) up to rounding). */
 template <int K>
 __global__ void __launch_bounds__(256)
-k_loglik_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
+k_loglik_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib, int64_t pitch,
              const double *__restrict__ q, const double *__restrict__ p,
              int64_t jslice, double *__restrict__ partial)
 {
@@ -46,9 +46,9 @@ k_loglik_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
         for (int t = threadIdx.x; t < n * K; t += blockDim.x) ps[t] = p[(size_t)K * jc + t];
         __syncthreads();
         if (b < Ib) {
-            const uint8_t *col = bed + (size_t)jc * Ib + b;
+            const uint8_t *col = bed + (size_t)jc * pitch + b;
             for (int jj = 0; jj < n; ++jj) {
-                const unsigned byte = __ldg(col + (size_t)jj * Ib);
+                const unsigned byte = __ldg(col + (size_t)jj * pitch);
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     const int c = (byte >> (2 * s)) & 3;
@@ -103,7 +103,7 @@ struct QSide {
 
 template <int K, int MODE>
 __global__ void __launch_bounds__(128)
-k_sweep_q_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
+k_sweep_q_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
               const double *__restrict__ q, const double *__restrict__ p,
               int64_t jslice, double *__restrict__ out)
 {
@@ -150,7 +150,7 @@ k_sweep_q_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
         }
         __syncthreads();
         for (int jj = 0; jj < n; ++jj) {
-            const int c = valid ? ((__ldg(colbase + (size_t)(jc + jj) * Ib) >> sh) & 3) : 1;
+            const int c = valid ? ((__ldg(colbase + (size_t)(jc + jj) * pitch) >> sh) & 3) : 1;
             double qp = 0.0;
 #pragma unroll
             for (int k = 0; k < K; ++k) qp = fma(qi[k], P[jj * K + k], qp);
@@ -217,7 +217,7 @@ struct PSide {
 
 template <int K, int MODE>
 __global__ void __launch_bounds__(128)
-k_sweep_p_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
+k_sweep_p_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
               const double *__restrict__ q, const double *__restrict__ p,
               int64_t islice, double *__restrict__ out)
 {
@@ -237,7 +237,7 @@ k_sweep_p_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
 #pragma unroll
     for (int l = 0; l < L; ++l) acc[l] = 0.0;
     const int ebase = sub * L;
-    const uint8_t *col = bed + (size_t)(valid ? j : 0) * Ib;
+    const uint8_t *col = bed + (size_t)(valid ? j : 0) * pitch;
 
     for (int64_t ic = i0; ic < i1; ic += IC) {
         const int n = (int)min((int64_t)IC, i1 - ic);
@@ -348,7 +348,7 @@ __global__ void k_expand_hess(int64_t nprob, int K, int S, const double *__restr
 /* Missing-code counts, bit-exact: code 01 <=> low bit 1, high bit 0.  Thread = one byte
  * column position b over a slice of SNPs; padding bits of the last byte are masked. */
 __global__ void __launch_bounds__(256)
-k_decode_counts(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib, int64_t jslice,
+k_decode_counts(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib, int64_t pitch, int64_t jslice,
                 unsigned long long *__restrict__ miss_snp, unsigned long long *__restrict__ miss_ind)
 {
     const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -360,7 +360,7 @@ k_decode_counts(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
     for (int64_t j = j0; j < j1; ++j) {
         unsigned m = 0;
         if (valid) {
-            const unsigned byte = __ldg(bed + (size_t)j * Ib + b);
+            const unsigned byte = __ldg(bed + (size_t)j * pitch + b);
             m = byte & ~(byte >> 1) & mask;
             c[0] += m & 1u; c[1] += (m >> 2) & 1u; c[2] += (m >> 4) & 1u; c[3] += (m >> 6) & 1u;
         }
@@ -378,13 +378,13 @@ k_decode_counts(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
 /* ===================================================================== launchers */
 
 template <int K>
-static cudaError_t launch_loglik_t(const uint8_t *bed, int64_t I, int64_t J, const double *q,
+static cudaError_t launch_loglik_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                    const double *p, const LoglikPlan &pl, double *partial, double *out,
                                    cudaStream_t st)
 {
     const int64_t Ib = (I + 3) / 4;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.gy);
-    k_loglik_f64<K><<<grid, 256, 0, st>>>(bed, I, J, Ib, q, p, pl.jslice, partial);
+    k_loglik_f64<K><<<grid, 256, 0, st>>>(bed, I, J, Ib, pitch, q, p, pl.jslice, partial);
     k_sum_partials<<<1, 1024, 0, st>>>(partial, (int64_t)pl.gx * pl.gy, out);
     return cudaGetLastError();
 }
@@ -403,12 +403,12 @@ LoglikPlan plan_loglik(int64_t I, int64_t J, int sms)
     return pl;
 }
 
-cudaError_t launch_loglik_f64(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
+cudaError_t launch_loglik_f64(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                               const double *p, const LoglikPlan &pl, double *partial, double *out,
                               cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_loglik_t<KK>(bed, I, J, q, p, pl, partial, out, st));
+    ADMIX_DISPATCH_K(K, e = launch_loglik_t<KK>(bed, I, J, pitch, q, p, pl, partial, out, st));
     return e;
 }
 
@@ -443,42 +443,42 @@ SweepPlan plan_sweep_p(int K, int64_t I, int64_t J, int sms)
 }
 
 template <int K, int MODE>
-static cudaError_t launch_sweep_q_t(const uint8_t *bed, int64_t I, int64_t J, const double *q,
+static cudaError_t launch_sweep_q_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                     const double *p, const SweepPlan &pl, double *out, cudaStream_t st)
 {
     using C = QSide<K, MODE>;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_q_f64<K, MODE><<<grid, 128, C::smem, st>>>(bed, I, J, (I + 3) / 4, q, p, pl.slice, out);
+    k_sweep_q_f64<K, MODE><<<grid, 128, C::smem, st>>>(bed, I, J, pitch, q, p, pl.slice, out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sweep_q_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J,
+cudaError_t launch_sweep_q_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                const double *q, const double *p, const SweepPlan &pl, double *out,
                                cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    if (mode == 0) { ADMIX_DISPATCH_K(K, (e = launch_sweep_q_t<KK, 0>(bed, I, J, q, p, pl, out, st))); }
-    else { ADMIX_DISPATCH_K(K, (e = launch_sweep_q_t<KK, 1>(bed, I, J, q, p, pl, out, st))); }
+    if (mode == 0) { ADMIX_DISPATCH_K(K, (e = launch_sweep_q_t<KK, 0>(bed, I, J, pitch, q, p, pl, out, st))); }
+    else { ADMIX_DISPATCH_K(K, (e = launch_sweep_q_t<KK, 1>(bed, I, J, pitch, q, p, pl, out, st))); }
     return e;
 }
 
 template <int K, int MODE>
-static cudaError_t launch_sweep_p_t(const uint8_t *bed, int64_t I, int64_t J, const double *q,
+static cudaError_t launch_sweep_p_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                     const double *p, const SweepPlan &pl, double *out, cudaStream_t st)
 {
     using C = PSide<K, MODE>;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_p_f64<K, MODE><<<grid, 128, C::smem, st>>>(bed, I, J, (I + 3) / 4, q, p, pl.slice, out);
+    k_sweep_p_f64<K, MODE><<<grid, 128, C::smem, st>>>(bed, I, J, pitch, q, p, pl.slice, out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J,
+cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                const double *q, const double *p, const SweepPlan &pl, double *out,
                                cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    if (mode == 0) { ADMIX_DISPATCH_K(K, (e = launch_sweep_p_t<KK, 0>(bed, I, J, q, p, pl, out, st))); }
-    else { ADMIX_DISPATCH_K(K, (e = launch_sweep_p_t<KK, 1>(bed, I, J, q, p, pl, out, st))); }
+    if (mode == 0) { ADMIX_DISPATCH_K(K, (e = launch_sweep_p_t<KK, 0>(bed, I, J, pitch, q, p, pl, out, st))); }
+    else { ADMIX_DISPATCH_K(K, (e = launch_sweep_p_t<KK, 1>(bed, I, J, pitch, q, p, pl, out, st))); }
     return e;
 }
 
@@ -510,7 +510,7 @@ cudaError_t launch_expand_hess(int64_t nprob, int K, int S, const double *parts,
     return cudaGetLastError();
 }
 
-cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J,
+cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                  unsigned long long *miss_snp, unsigned long long *miss_ind,
                                  int sms, cudaStream_t st)
 {
@@ -519,7 +519,7 @@ cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J,
     int64_t gy = std::max<int64_t>(1, std::min<int64_t>(((int64_t)sms * 8 + gx - 1) / gx, J));
     const int64_t jslice = (J + gy - 1) / gy;
     gy = (J + jslice - 1) / jslice;
-    k_decode_counts<<<dim3(gx, (unsigned)gy), 256, 0, st>>>(bed, I, J, Ib, jslice, miss_snp, miss_ind);
+    k_decode_counts<<<dim3(gx, (unsigned)gy), 256, 0, st>>>(bed, I, J, Ib, pitch, jslice, miss_snp, miss_ind);
     return cudaGetLastError();
 }
 
@@ -540,4 +540,25 @@ cudaError_t prepare_sweeps(int K)
     cudaError_t e = cudaErrorInvalidValue;
     ADMIX_DISPATCH_K(K, e = prepare_sweeps_t<KK>());
     return e;
+}
+
+/* Padding of the last genotype byte of every column (individuals >= I) set to the missing code
+ * 01, so kernels that read whole 16-byte groups need no per-individual bound checks.  The
+ * reference never reads those bits (its loops stop at I), so this changes no result. */
+__global__ void k_mask_tail(uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch)
+{
+    const int64_t Ib = (I + 3) / 4;
+    const int r = (int)(I & 3);
+    const unsigned keep = (1u << (2 * r)) - 1u;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < J; j += (int64_t)gridDim.x * blockDim.x) {
+        uint8_t *b = bed + (size_t)j * pitch + (Ib - 1);
+        *b = (uint8_t)((*b & keep) | (0x55u & ~keep));
+    }
+}
+
+cudaError_t launch_mask_tail(uint8_t *bed, int64_t I, int64_t J, int64_t pitch, int sms, cudaStream_t st)
+{
+    if ((I & 3) == 0) return cudaSuccess;
+    k_mask_tail<<<grid_for(J, sms), 256, 0, st>>>(bed, I, J, pitch);
+    return cudaGetLastError();
 }

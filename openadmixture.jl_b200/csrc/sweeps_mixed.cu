@@ -1,23 +1,26 @@
 /*
- * sweeps_mixed.cu -- the mixed-precision ("chosen") form of the Q-block gradient / Hessian
- * sweep (update_q_loop_skipmissing!, loops.jl:867-894) on sm_100a tensor cores.
+ * sweeps_mixed.cu -- the mixed-precision ("chosen") form of the gradient / Hessian sweeps and
+ * of the log-likelihood pass on sm_100a tensor cores.
  *
- *   XtX_q[i] = sum_j w1_ij p_j p_j' + w2_ij pbar_j pbar_j'        (the Hessian, K x K)
- *   Xtz_q[i] = sum_j z1_ij p_j + z2_ij pbar_j                    (the gradient)
+ * Q side (update_q_loop_skipmissing!, loops.jl:867-894):
+ *   XtX_q[i] = sum_j w1_ij p_j p_j' + w2_ij pbar_j pbar_j',  Xtz_q[i] = sum_j z1_ij p_j + z2_ij pbar_j
  *   z1 = nm g / qp, z2 = nm (2-g) / (1-qp), w1 = z1 / qp, w2 = z2 / (1-qp), pbar = 1 - p
+ * P side (update_p_loop_skipmissing!, loops.jl:923-950):
+ *   XtX_p[j] = sum_i (w1 + w2)_ij q_i q_i',  Xtz_p[j] = sum_i (z1 - z2)_ij q_i
  *
- * The Hessian is a GEMM: rows = 128 individuals of the CTA, reduction over SNPs, columns =
- * the K(K+1)/2 packed pairs (k <= k2):  D = [W1 | W2] x [P(x)P ; Pbar(x)Pbar].  Each 64-SNP chunk
- * the 256 threads (two per individual, 32 SNPs each) decode the genotypes, compute qp and
- * 1-qp = sum_k q_k (1-p_k) in FP32 (paired __ffma2_rn over two SNPs), one reciprocal per cell,
- * the weights, and the gradient in FP32 (chunk sums added into FP64); they write w1 and w2 as
- * BF16 into the A tiles and the pair products as BF16 into the B tiles.  One thread issues
- * eight tcgen05.mma (4 K-steps x 2 terms) accumulating in FP32 in TMEM; A/B tiles are double
- * buffered, the MMA of chunk c overlapping the production of chunk c+1, with completion
- * signalled through an mbarrier.  The epilogue reads the accumulator with tcgen05.ld and writes
- * the same FP64 partial layout as the FP64 sweep, so the QP kernels consume either.
+ * Each Hessian is a GEMM whose rows are the 128 problems of a CTA (individuals or SNPs), whose
+ * reduction runs over the other axis and whose columns are the K(K+1)/2 packed pairs k <= k2.
+ * CUDA cores produce the BF16 weight tile (A) and the BF16 pair-product tile (B) of each chunk in
+ * shared memory -- qp and 1-qp = sum_k q_k (1-p_k) in FP32 with paired __ffma2_rn, one
+ * reciprocal per cell, the gradient in FP32 summed into FP64 per chunk -- and one thread issues
+ * tcgen05.mma into an FP32 accumulator in tensor memory.  Tiles are double buffered, so the MMAs
+ * of chunk c run while chunk c+1 is produced; completion is signalled on an mbarrier.  The
+ * epilogue reads the accumulator with tcgen05.ld and writes the FP64 partial layout of the FP64
+ * sweeps, so the QP kernels consume either.
  *
- * Requires sum_k q_k = 1 (true for every projected Q the SQP updates see).
+ * Genotypes are read from the handle's padded layout: columns at a pitch that is a multiple of
+ * 16 bytes, padding bytes and padding bits coded missing (01), so whole 16-byte groups can be
+ * loaded without per-individual bound checks.  Requires sum_k q_k = 1 (every projected Q).
  */
 #include "common.cuh"
 #include "kernels.h"
@@ -25,9 +28,38 @@
 
 namespace {
 
-constexpr int MQ_JC = 32;          /* SNPs per chunk = MMA K extent per chunk (2 K-steps) */
-constexpr int MQ_THREADS = 128;    /* one thread per individual = per accumulator row */
-constexpr uint32_t MQ_WAIT_LIMIT = 1u << 22;   /* polls; an MMA batch completes in microseconds */
+constexpr uint32_t MX_WAIT_LIMIT = 1u << 22;   /* polls; an MMA batch completes in microseconds */
+
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+/* Code-pair table: index c0 | c1 << 2 of two cells -> (nm g, nm g, nm (2-g), nm (2-g));
+ * codes 00 -> (0, 2), 01 (missing) -> (0, 0), 10 -> (1, 1), 11 -> (2, 0).  Stored 8 times so
+ * lane l of a quarter-warp always reads bank group l: entry e, copy l at float4 index 8e + l. */
+__device__ __forceinline__ void code_table_init(float4 *tab, int tid, int nthreads)
+{
+    const float A1[4] = {0.f, 0.f, 1.f, 2.f}, A2[4] = {2.f, 0.f, 1.f, 0.f};
+    for (int t = tid; t < 128; t += nthreads) {
+        const int e = t >> 3, c0 = e & 3, c1 = e >> 2;
+        tab[t] = make_float4(A1[c0], A1[c1], A2[c0], A2[c1]);
+    }
+}
+
+/* 8 individuals' codes of two SNP columns interleaved byte-wise: [a0 b0 a1 b1 ...] */
+__device__ __forceinline__ uint4 interleave8(uint2 a, uint2 b)
+{
+    return make_uint4(__byte_perm(a.x, b.x, 0x5140), __byte_perm(a.x, b.x, 0x7362),
+                      __byte_perm(a.y, b.y, 0x5140), __byte_perm(a.y, b.y, 0x7362));
+}
+
+/* ===================================================================== Q side */
+
+constexpr int MQ_JC = 32;          /* SNPs per chunk = 2 MMA K-steps */
+constexpr int MQ_THREADS = 128;    /* one thread per individual = accumulator row */
 
 template <int K>
 struct MQ {
@@ -42,45 +74,34 @@ struct MQ {
     static constexpr uint32_t GBUF = MQ_JC * 32;                /* genotype bytes of one chunk */
     static constexpr uint32_t OFF_P = 2 * STAGE_BYTES;          /* two P buffers */
     static constexpr uint32_t OFF_G = OFF_P + 2 * PBUF;         /* two G buffers, [pair][byte][2] */
-    static constexpr uint32_t OFF_TAB = OFF_G + 2 * GBUF;       /* float4 [16] code-pair weights */
-    static constexpr uint32_t SMEM = OFF_TAB + 16 * 16 + 1024;  /* + alignment slack */
-    /* descriptor strides: A core matrices 128 B apart along M, 2048 B along K;
-     * B core matrices 128 B apart along N, 16 N bytes along K */
+    static constexpr uint32_t OFF_TAB = OFF_G + 2 * GBUF;       /* float4 [16][8] code table */
+    static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024; /* + alignment slack */
+    /* A core matrices 128 B apart along M, 2048 B along K; B 128 B along N, 16 N bytes along K */
     static constexpr uint32_t A_LBO = 2048, A_SBO = 128;
     static constexpr uint32_t B_LBO = 16 * N, B_SBO = 128;
-    static constexpr int PREF_P = (K * MQ_JC + MQ_THREADS - 1) / MQ_THREADS;   /* p values per thread */
+    static constexpr int PREF_P = (K * MQ_JC + MQ_THREADS - 1) / MQ_THREADS;
 };
 
-__device__ __forceinline__ float rcp_approx(float x)
-{
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
-/* Global loads of one chunk's inputs into registers (issued a chunk ahead). */
+/* One chunk's inputs in registers (loaded a chunk ahead): threads 0..63 hold 8 bytes of each of
+ * the SNP pair's two columns (pair t >> 2, bytes 8 (t & 3) .. +7 of the CTA's 32); every thread
+ * holds up to PREF_P allele frequencies. */
 template <int K>
-struct ChunkRegs {
-    uint32_t g[2];                 /* 8 genotype bytes: columns 2*(tid/32)+{0,1}... see load */
+struct QChunk {
+    uint2 ga, gb;
     double pv[MQ<K>::PREF_P];
 };
 
 template <int K>
-__device__ __forceinline__ void chunk_load(ChunkRegs<K> &cr, const uint8_t *__restrict__ bed, int64_t Ib,
-                                           const double *__restrict__ p, int64_t i0, int64_t jc, int n, int tid)
+__device__ __forceinline__ void qchunk_load(QChunk<K> &cr, const uint8_t *__restrict__ bed, int64_t pitch,
+                                            const double *__restrict__ p, int64_t i0, int64_t jc, int n, int tid)
 {
-    /* genotype bytes: thread (b = tid & 31, q4 = tid >> 5) loads byte b of columns 8*q4 .. 8*q4+7 */
-    const int b = tid & 31, q4 = tid >> 5;
-    const int64_t bi = i0 / 4 + b;
-    uint32_t w[2] = {0u, 0u};
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-        const int jj = q4 * 8 + u;
-        const uint32_t v = (jj < n && bi < Ib) ? (uint32_t)__ldg(bed + (size_t)(jc + jj) * Ib + bi) : 0x55u;
-        w[u >> 2] |= v << (8 * (u & 3));
+    if (tid < 64) {
+        const int m = tid >> 2, qb = tid & 3;
+        const size_t off = (size_t)(i0 / 4) + 8 * qb;
+        const uint2 miss = make_uint2(0x55555555u, 0x55555555u);
+        cr.ga = (2 * m < n) ? __ldg((const uint2 *)(bed + (size_t)(jc + 2 * m) * pitch + off)) : miss;
+        cr.gb = (2 * m + 1 < n) ? __ldg((const uint2 *)(bed + (size_t)(jc + 2 * m + 1) * pitch + off)) : miss;
     }
-    cr.g[0] = w[0];
-    cr.g[1] = w[1];
 #pragma unroll
     for (int u = 0; u < MQ<K>::PREF_P; ++u) {
         const int t = tid + u * MQ_THREADS;          /* t = jj * K + k over the chunk's K*JC values */
@@ -89,15 +110,13 @@ __device__ __forceinline__ void chunk_load(ChunkRegs<K> &cr, const uint8_t *__re
     }
 }
 
-/* Registers -> shared buffers: p / 1-p as FP32 [k][jj], genotypes as [pair m][byte b][2]. */
+/* registers -> shared: p / 1-p as FP32 [k][jj]; genotypes as [pair m][byte b][2] */
 template <int K>
-__device__ __forceinline__ void chunk_store(const ChunkRegs<K> &cr, float *Pb, uint8_t *Gb, int tid)
+__device__ __forceinline__ void qchunk_store(const QChunk<K> &cr, float *Pb, uint8_t *Gb, int tid)
 {
-    const int b = tid & 31, q4 = tid >> 5;
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-        const int jj = q4 * 8 + u;
-        Gb[((jj >> 1) * 32 + b) * 2 + (jj & 1)] = (uint8_t)(cr.g[u >> 2] >> (8 * (u & 3)));
+    if (tid < 64) {
+        const int m = tid >> 2, qb = tid & 3;
+        *(uint4 *)(Gb + (m * 32 + 8 * qb) * 2) = interleave8(cr.ga, cr.gb);
     }
 #pragma unroll
     for (int u = 0; u < MQ<K>::PREF_P; ++u) {
@@ -112,7 +131,7 @@ __device__ __forceinline__ void chunk_store(const ChunkRegs<K> &cr, float *Pb, u
 
 template <int K>
 __global__ void __launch_bounds__(MQ_THREADS)
-k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
+k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                 const double *__restrict__ q, const double *__restrict__ p, int64_t jslice,
                 double *__restrict__ out, int *__restrict__ err)
 {
@@ -130,7 +149,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
     const int64_t j0 = (int64_t)blockIdx.y * jslice;
     const int64_t j1 = min(J, j0 + jslice);
     const int nchunk = (int)((j1 - j0 + MQ_JC - 1) / MQ_JC);
-    float4 *tab = (float4 *)(sm + C::OFF_TAB);
+    const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
 
     if (warp == 0) tmem_alloc_warp(&tmem_holder, C::NCOLS);
     if (tid == 0) {
@@ -138,19 +157,13 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
         mbar_init(&mbar[1], 1);
         mbar_fence_init();
     }
-    if (tid < 16) {
-        /* code pair (c0 | c1 << 2) -> (nm g, nm g, nm (2-g), nm (2-g)) of the two cells;
-         * codes 00 -> (0, 2), 01 (missing) -> (0, 0), 10 -> (1, 1), 11 -> (2, 0) */
-        const float A1[4] = {0.f, 0.f, 1.f, 2.f}, A2[4] = {2.f, 0.f, 1.f, 0.f};
-        const int c0 = tid & 3, c1 = tid >> 2;
-        tab[tid] = make_float4(A1[c0], A1[c1], A2[c0], A2[c1]);
-    }
-    ChunkRegs<K> cr;
+    code_table_init((float4 *)(sm + C::OFF_TAB), tid, MQ_THREADS);
+    QChunk<K> cr;
     if (nchunk > 0) {
-        chunk_load<K>(cr, bed, Ib, p, i0, j0, (int)min((int64_t)MQ_JC, j1 - j0), tid);
-        chunk_store<K>(cr, (float *)(sm + C::OFF_P), sm + C::OFF_G, tid);
+        qchunk_load<K>(cr, bed, pitch, p, i0, j0, (int)min((int64_t)MQ_JC, j1 - j0), tid);
+        qchunk_store<K>(cr, (float *)(sm + C::OFF_P), sm + C::OFF_G, tid);
     }
-    if (nchunk > 1) chunk_load<K>(cr, bed, Ib, p, i0, j0 + MQ_JC, (int)min((int64_t)MQ_JC, j1 - j0 - MQ_JC), tid);
+    if (nchunk > 1) qchunk_load<K>(cr, bed, pitch, p, i0, j0 + MQ_JC, (int)min((int64_t)MQ_JC, j1 - j0 - MQ_JC), tid);
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
@@ -166,7 +179,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
 #pragma unroll
     for (int k = 0; k < K; ++k) gd[k] = 0.0;
     const int sh = valid ? (int)(i & 3) * 2 : 0;
-    const uint32_t gmask = valid ? 0xFFFFu : 0u;        /* invalid rows read code pair 01|01 -> missing */
+    const uint32_t gmask = valid ? 0xFFFFu : 0u;        /* rows beyond I read code pair 01|01 */
     constexpr uint32_t idesc = idesc_bf16_f32(128, N);
     bool ok = true;
 
@@ -177,13 +190,12 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
         const float *Pb = (const float *)(sm + C::OFF_P + s * C::PBUF);
         const uint8_t *Gb = sm + C::OFF_G + s * C::GBUF;
         if (c >= 2 && ok) {                                     /* MMAs of chunk c-2 read this stage */
-            if (!mbar_wait_bounded(&mbar[s], (uint32_t)(((c - 2) >> 1) & 1), MQ_WAIT_LIMIT)) {
+            if (!mbar_wait_bounded(&mbar[s], (uint32_t)(((c - 2) >> 1) & 1), MX_WAIT_LIMIT)) {
                 ok = false;
                 if (tid == 0) atomicOr(err, 1);
             }
         }
-        /* B tiles: bf16 pair products; task (term, kc, nn) writes row nn's 8 SNPs of k-chunk kc
-         * at kc*16N + 16nn (consecutive tasks -> consecutive 16-byte rows) */
+        /* B tiles: task (term, kc, nn) writes pair nn's 8 SNPs of k-chunk kc at kc*16N + 16nn */
         for (int t = tid; t < 2 * 4 * N; t += MQ_THREADS) {
             const int term = t / (4 * N), rem = t - term * 4 * N;
             const int kc = rem / N, nn = rem - kc * N;
@@ -195,9 +207,8 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int jj = kc * 8 + 2 * e;
-                    const float lo = src[ka * MQ_JC + jj] * src[kb * MQ_JC + jj];
-                    const float hi = src[ka * MQ_JC + jj + 1] * src[kb * MQ_JC + jj + 1];
-                    w[e] = pack_bf16x2(lo, hi);
+                    w[e] = pack_bf16x2(src[ka * MQ_JC + jj] * src[kb * MQ_JC + jj],
+                                       src[ka * MQ_JC + jj + 1] * src[kb * MQ_JC + jj + 1]);
                 }
             }
             *(uint4 *)(Bt + term * C::B_BYTES + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -205,7 +216,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
         /* producer: this thread's individual, the chunk's 32 SNPs as 16 pairs */
         const float2 *P2 = (const float2 *)Pb;                  /* [k][pair] */
         const float2 *Pb2 = (const float2 *)(Pb + K * MQ_JC);
-        const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);  /* [pair][byte]: both SNPs of a pair */
+        const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);  /* [pair][byte]: both SNPs */
         float2 ga[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) ga[k] = make_float2(0.f, 0.f);
@@ -217,7 +228,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
                 const int m = kc * 4 + e;                       /* SNPs 2m, 2m+1 of the chunk */
                 const uint32_t gw = ((uint32_t)G2[m * 32] & gmask) | (~gmask & 0x5555u);
                 const uint32_t tb = gw >> sh;
-                const float4 a = tab[(tb & 3u) | ((tb >> 6) & 12u)];
+                const float4 a = tab[8 * ((tb & 3u) | ((tb >> 6) & 12u))];
                 float2 qp = make_float2(0.f, 0.f), om = make_float2(0.f, 0.f);
                 float2 pv[K], pbv[K];
 #pragma unroll
@@ -247,12 +258,11 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
         }
 #pragma unroll
         for (int k = 0; k < K; ++k) gd[k] += (double)ga[k].x + (double)ga[k].y;
-        /* next chunk's inputs: registers -> the other buffer; then prefetch the one after */
         if (c + 1 < nchunk) {
-            chunk_store<K>(cr, (float *)(sm + C::OFF_P + (s ^ 1) * C::PBUF), sm + C::OFF_G + (s ^ 1) * C::GBUF, tid);
+            qchunk_store<K>(cr, (float *)(sm + C::OFF_P + (s ^ 1) * C::PBUF), sm + C::OFF_G + (s ^ 1) * C::GBUF, tid);
             if (c + 2 < nchunk) {
                 const int64_t jn = j0 + (int64_t)(c + 2) * MQ_JC;
-                chunk_load<K>(cr, bed, Ib, p, i0, jn, (int)min((int64_t)MQ_JC, j1 - jn), tid);
+                qchunk_load<K>(cr, bed, pitch, p, i0, jn, (int)min((int64_t)MQ_JC, j1 - jn), tid);
             }
         }
         fence_async_smem();
@@ -272,11 +282,11 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
             tc_commit(&mbar[s]);
         }
     }
-    /* wait for the last MMAs of both stages (bounded even after a failed wait, so the TMEM
-     * is not released under an MMA still in flight) */
+    /* wait for the last MMAs of both stages (bounded even after a failed wait, so the TMEM is
+     * not released under an MMA still in flight) */
     for (int c = max(0, nchunk - 2); c < nchunk; ++c) {
         const int s = c & 1;
-        if (!mbar_wait_bounded(&mbar[s], (uint32_t)((c >> 1) & 1), ok ? MQ_WAIT_LIMIT : 1024u)) {
+        if (!mbar_wait_bounded(&mbar[s], (uint32_t)((c >> 1) & 1), ok ? MX_WAIT_LIMIT : 1024u)) {
             ok = false;
             if (tid == 0) atomicOr(err, 1);
         }
@@ -308,15 +318,9 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
 }
 
 /* ===================================================================== P side
- *
- * update_p_loop_skipmissing! (loops.jl:923-950):
- *   XtX_p[j] = sum_i c_ij q_i q_i',  c = nm (g/qp^2 + (2-g)/(1-qp)^2)
- *   Xtz_p[j] = sum_i z_ij q_i,       z = nm (g/qp - (2-g)/(1-qp))
- * GEMM rows = 128 SNPs of the CTA (thread = SNP), reduction over individuals in chunks of 32,
- * columns = the K(K+1)/2 pairs: D = C x QQ'.  A thread reads its own column's 8 genotype bytes
- * per chunk (32 individuals); the 4 bits of an individual pair index the code table directly.
- */
-constexpr int MP_IC = 32;
+ * Thread = SNP row; individuals in chunks of 64 (one 16-byte load of the thread's own column);
+ * the 4 bits of an individual pair index the code table directly. */
+constexpr int MP_IC = 64;
 constexpr int MP_THREADS = 128;
 
 template <int K>
@@ -325,46 +329,35 @@ struct MP {
     static constexpr int N = ((T + 15) / 16) * 16;
     static constexpr uint32_t NCOLS = tmem_cols_for(N);
     static constexpr int E = T + K;
-    static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* one BF16 weight tile: 8 KB */
+    static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* one BF16 weight tile: 16 KB */
     static constexpr uint32_t B_BYTES = N * MP_IC * 2;
     static constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
     static constexpr uint32_t QBUF = K * MP_IC * 4;             /* q of one chunk, FP32 [k][i] */
     static constexpr uint32_t OFF_Q = 2 * STAGE_BYTES;
     static constexpr uint32_t OFF_TAB = OFF_Q + 2 * QBUF;
-    static constexpr uint32_t SMEM = OFF_TAB + 16 * 16 + 1024;
+    static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024;
     static constexpr uint32_t A_LBO = 2048, A_SBO = 128;
     static constexpr uint32_t B_LBO = 16 * N, B_SBO = 128;
     static constexpr int PREF_Q = (K * MP_IC + MP_THREADS - 1) / MP_THREADS;
 };
 
-/* 8 genotype bytes of column j for individuals ic .. ic+31, individuals >= I forced missing */
-__device__ __forceinline__ uint2 pcol_load(const uint8_t *__restrict__ bed, int64_t I, int64_t Ib, int64_t j,
-                                           bool valid, int64_t ic)
+/* 64 individuals' codes of SNP column j from individual ic (a multiple of 64) */
+__device__ __forceinline__ uint4 col_load64(const uint8_t *__restrict__ bed, int64_t pitch, int64_t j, bool valid,
+                                            int64_t ic)
 {
-    uint32_t w[2] = {0x55555555u, 0x55555555u};
-    if (valid) {
-        const uint8_t *col = bed + (size_t)j * Ib;
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int64_t bi = ic / 4 + u;
-            uint32_t v = 0x55u;
-            if (bi < Ib) {
-                v = __ldg(col + bi);
-                const int64_t nvalid = I - 4 * bi;            /* individuals of this byte below I */
-                if (nvalid < 4) {
-                    const uint32_t keep = (1u << (2 * (int)nvalid)) - 1u;
-                    v = (v & keep) | (0x55u & ~keep);
-                }
-            }
-            w[u >> 2] = (w[u >> 2] & ~(0xFFu << (8 * (u & 3)))) | (v << (8 * (u & 3)));
-        }
-    }
-    return make_uint2(w[0], w[1]);
+    return valid ? __ldg((const uint4 *)(bed + (size_t)j * pitch + (size_t)(ic / 4)))
+                 : make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
+}
+
+__device__ __forceinline__ uint32_t pair_code(const uint4 &g, int m)
+{
+    const uint32_t w = (m < 8) ? g.x : ((m < 16) ? g.y : ((m < 24) ? g.z : g.w));
+    return (w >> (4 * (m & 7))) & 15u;
 }
 
 template <int K>
 __global__ void __launch_bounds__(MP_THREADS)
-k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
+k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                 const double *__restrict__ q, const double *__restrict__ p, int64_t islice,
                 double *__restrict__ out, int *__restrict__ err)
 {
@@ -381,7 +374,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
     const int64_t ia = (int64_t)blockIdx.y * islice;
     const int64_t ib = min(I, ia + islice);
     const int nchunk = (int)((ib - ia + MP_IC - 1) / MP_IC);
-    float4 *tab = (float4 *)(sm + C::OFF_TAB);
+    const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
 
     if (warp == 0) tmem_alloc_warp(&tmem_holder, C::NCOLS);
     if (tid == 0) {
@@ -389,12 +382,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
         mbar_init(&mbar[1], 1);
         mbar_fence_init();
     }
-    if (tid < 16) {
-        const float A1[4] = {0.f, 0.f, 1.f, 2.f}, A2[4] = {2.f, 0.f, 1.f, 0.f};
-        const int c0 = tid & 3, c1 = tid >> 2;
-        tab[tid] = make_float4(A1[c0], A1[c1], A2[c0], A2[c1]);
-    }
-    /* q chunk staging: registers one chunk ahead, shared double buffer [k][i] */
+    code_table_init((float4 *)(sm + C::OFF_TAB), tid, MP_THREADS);
     double qr[C::PREF_Q];
     auto qload = [&](int64_t ic) {
 #pragma unroll
@@ -414,15 +402,15 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
             }
         }
     };
-    uint2 gcur = make_uint2(0x55555555u, 0x55555555u), gnext = gcur;
+    uint4 gcur = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), gnext = gcur;
     if (nchunk > 0) {
         qload(ia);
         qstore((float *)(sm + C::OFF_Q));
-        gcur = pcol_load(bed, I, Ib, j, valid, ia);
+        gcur = col_load64(bed, pitch, j, valid, ia);
     }
     if (nchunk > 1) {
         qload(ia + MP_IC);
-        gnext = pcol_load(bed, I, Ib, j, valid, ia + MP_IC);
+        gnext = col_load64(bed, pitch, j, valid, ia + MP_IC);
     }
     tc_fence_before_sync();
     __syncthreads();
@@ -449,13 +437,13 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
         uint8_t *Bt = At + C::A_BYTES;
         const float *Qb = (const float *)(sm + C::OFF_Q + s * C::QBUF);
         if (c >= 2 && ok) {
-            if (!mbar_wait_bounded(&mbar[s], (uint32_t)(((c - 2) >> 1) & 1), MQ_WAIT_LIMIT)) {
+            if (!mbar_wait_bounded(&mbar[s], (uint32_t)(((c - 2) >> 1) & 1), MX_WAIT_LIMIT)) {
                 ok = false;
                 if (tid == 0) atomicOr(err, 1);
             }
         }
         /* B tile: QQ[n][i] = q_ka(i) q_kb(i) in BF16, task (kc, nn) -> 16-byte row chunk */
-        for (int t = tid; t < 4 * N; t += MP_THREADS) {
+        for (int t = tid; t < 8 * N; t += MP_THREADS) {
             const int kc = t / N, nn = t - kc * N;
             uint32_t w[4] = {0u, 0u, 0u, 0u};
             if (nn < T) {
@@ -475,13 +463,12 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
 #pragma unroll
         for (int k = 0; k < K; ++k) ga[k] = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int kc = 0; kc < 4; ++kc) {
+        for (int kc = 0; kc < 8; ++kc) {
             uint32_t cp[4];
-            const uint32_t gw = kc < 2 ? gcur.x : gcur.y;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const int m = kc * 4 + e;                       /* individuals 2m, 2m+1 of the chunk */
-                const float4 a = tab[(gw >> (4 * (m & 7))) & 15u];
+                const float4 a = tab[8 * pair_code(gcur, m)];
                 float2 qp = make_float2(0.f, 0.f), om = make_float2(0.f, 0.f);
                 float2 qv[K];
 #pragma unroll
@@ -511,7 +498,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
             if (c + 2 < nchunk) {
                 const int64_t icn = ia + (int64_t)(c + 2) * MP_IC;
                 qload(icn);
-                gnext = pcol_load(bed, I, Ib, j, valid, icn);
+                gnext = col_load64(bed, pitch, j, valid, icn);
             }
         }
         fence_async_smem();
@@ -520,7 +507,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
             tc_fence_after_sync();
             const uint32_t abase = smem_u32(At), bbase = smem_u32(Bt);
 #pragma unroll
-            for (int ks = 0; ks < 2; ++ks) {
+            for (int ks = 0; ks < 4; ++ks) {
                 const uint64_t ad = umma_desc_kmajor(abase + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
                 const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
                 tc_mma_bf16(tmem, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
@@ -530,7 +517,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
     }
     for (int c = max(0, nchunk - 2); c < nchunk; ++c) {
         const int s = c & 1;
-        if (!mbar_wait_bounded(&mbar[s], (uint32_t)((c >> 1) & 1), ok ? MQ_WAIT_LIMIT : 1024u)) {
+        if (!mbar_wait_bounded(&mbar[s], (uint32_t)((c >> 1) & 1), ok ? MX_WAIT_LIMIT : 1024u)) {
             ok = false;
             if (tid == 0) atomicOr(err, 1);
         }
@@ -561,18 +548,16 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
 }
 
 /* ===================================================================== loglik
- *
  * loglikelihood_loop_skipmissing (loops.jl:517-539) with FP32 cells: thread = SNP, individuals
- * in pairs; each cell contributes the factor qp^g (1-qp)^(2-g) (1 when missing), two cells'
- * factors are multiplied in FP32 and folded into an FP64 running product whose exponent is
- * moved into an integer every 12 pairs; one FP64 log per thread at the end.  The products are
- * rounded to nearest, so the error is a random walk far below the convergence test's resolution.
- */
-constexpr int ML_IC = 64;          /* individuals per chunk (16 genotype bytes per SNP) */
+ * in pairs; each cell contributes qp^g (1-qp)^(2-g) (1 when missing), two cells' factors are
+ * multiplied in FP32 and folded into an FP64 running product whose exponent moves into an
+ * integer every 12 pairs; one FP64 log per thread at the end.  Every product is rounded to
+ * nearest, so the rounding error is a random walk far below the convergence test's resolution. */
+constexpr int ML_IC = 64;
 
 template <int K>
 __global__ void __launch_bounds__(128)
-k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib,
+k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                const double *__restrict__ q, const double *__restrict__ p, int64_t islice,
                double *__restrict__ partial)
 {
@@ -593,9 +578,8 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib
         const float pb = (float)(1.0 - pv);
         pbd[k] = make_float2(pb, pb);
     }
-    /* inputs of the next chunk are loaded into registers while this one is consumed */
     float qr[PREF];
-    uint2 gn[2];
+    uint4 gnext = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), g = gnext;
     auto load = [&](int64_t ic) {
 #pragma unroll
         for (int u = 0; u < PREF; ++u) {
@@ -603,8 +587,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib
             const int ii = t / K;
             qr[u] = (t < K * ML_IC && ic + ii < ib) ? (float)q[(size_t)K * ic + t] : 1.0f / K;
         }
-        gn[0] = pcol_load(bed, I, Ib, j, valid, ic);
-        gn[1] = pcol_load(bed, I, Ib, j, valid, ic + 32);
+        gnext = col_load64(bed, pitch, j, valid, ic);
     };
     auto store = [&](int s) {
 #pragma unroll
@@ -616,8 +599,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib
             }
         }
     };
-    uint2 g[2] = {make_uint2(0x55555555u, 0x55555555u), make_uint2(0x55555555u, 0x55555555u)};
-    if (nchunk > 0) { load(ia); store(0); g[0] = gn[0]; g[1] = gn[1]; }
+    if (nchunk > 0) { load(ia); store(0); g = gnext; }
     if (nchunk > 1) load(ia + ML_IC);
     __syncthreads();
     double prod = 1.0;
@@ -626,8 +608,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib
         const int s = c & 1;
 #pragma unroll
         for (int m = 0; m < ML_IC / 2; ++m) {
-            const uint32_t word = (m < 16) ? ((m < 8) ? g[0].x : g[0].y) : ((m < 24) ? g[1].x : g[1].y);
-            const uint32_t code4 = (word >> (4 * (m & 7))) & 15u;
+            const uint32_t code4 = pair_code(g, m);
             float2 qp = make_float2(0.f, 0.f), om = make_float2(0.f, 0.f);
 #pragma unroll
             for (int k = 0; k < K; ++k) {
@@ -653,7 +634,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib
         prod = __longlong_as_double((bits & ~(0x7FFLL << 52)) | (1023LL << 52));
         if (c + 1 < nchunk) {
             store(s ^ 1);
-            g[0] = gn[0]; g[1] = gn[1];
+            g = gnext;
             if (c + 2 < nchunk) load(ia + (int64_t)(c + 2) * ML_IC);
         }
         __syncthreads();
@@ -684,31 +665,46 @@ cudaError_t prepare_mixed_t()
 }
 
 template <int K>
-cudaError_t launch_p_mixed_t(const uint8_t *bed, int64_t I, int64_t J, const double *q, const double *p,
-                             const SweepPlan &pl, double *out, int *err, cudaStream_t st)
+cudaError_t launch_q_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
+                             const double *p, const SweepPlan &pl, double *out, int *err, cudaStream_t st)
 {
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_p_mixed<K><<<grid, MP_THREADS, MP<K>::SMEM, st>>>(bed, I, J, (I + 3) / 4, q, p, pl.slice, out, err);
+    k_sweep_q_mixed<K><<<grid, MQ_THREADS, MQ<K>::SMEM, st>>>(bed, I, J, pitch, q, p, pl.slice, out, err);
     return cudaGetLastError();
 }
 
 template <int K>
-cudaError_t launch_ll_mixed_t(const uint8_t *bed, int64_t I, int64_t J, const double *q, const double *p,
-                              const SweepPlan &pl, double *partial, double *out, cudaStream_t st)
+cudaError_t launch_p_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
+                             const double *p, const SweepPlan &pl, double *out, int *err, cudaStream_t st)
 {
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_loglik_mixed<K><<<grid, 128, 0, st>>>(bed, I, J, (I + 3) / 4, q, p, pl.slice, partial);
+    k_sweep_p_mixed<K><<<grid, MP_THREADS, MP<K>::SMEM, st>>>(bed, I, J, pitch, q, p, pl.slice, out, err);
+    return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_ll_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
+                              const double *p, const SweepPlan &pl, double *partial, double *out, cudaStream_t st)
+{
+    dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
+    k_loglik_mixed<K><<<grid, 128, 0, st>>>(bed, I, J, pitch, q, p, pl.slice, partial);
     k_sum_partials_mixed<<<1, 1024, 0, st>>>(partial, (int64_t)pl.gx * pl.S, out);
     return cudaGetLastError();
 }
 
-template <int K>
-cudaError_t launch_q_mixed_t(const uint8_t *bed, int64_t I, int64_t J, const double *q, const double *p,
-                             const SweepPlan &pl, double *out, int *err, cudaStream_t st)
+/* slices over the second axis: enough CTAs to cover the GPU, each slice a multiple of `unit` */
+SweepPlan plan_rows(int64_t rows, int64_t cols, int sms, int per_sm, int64_t unit)
 {
-    dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_q_mixed<K><<<grid, MQ_THREADS, MQ<K>::SMEM, st>>>(bed, I, J, (I + 3) / 4, q, p, pl.slice, out, err);
-    return cudaGetLastError();
+    SweepPlan pl;
+    pl.gx = (int)((rows + 127) / 128);
+    const int64_t target = (int64_t)sms * per_sm;
+    int64_t S = (target + pl.gx - 1) / pl.gx;
+    S = std::max<int64_t>(1, std::min<int64_t>(S, (cols + 4 * unit - 1) / (4 * unit)));
+    int64_t slice = (cols + S - 1) / S;
+    slice = (slice + unit - 1) / unit * unit;
+    pl.slice = slice;
+    pl.S = (int)((cols + slice - 1) / slice);
+    return pl;
 }
 
 } // namespace
@@ -720,73 +716,45 @@ cudaError_t prepare_mixed(int K)
     return e;
 }
 
-/* One CTA per 128 individuals and SNP slice; slices chosen so the grid covers the GPU. */
+/* One CTA per 128 individuals and SNP slice. */
 SweepPlan plan_sweep_q_mixed(int K, int64_t I, int64_t J, int sms)
 {
     (void)K;
-    SweepPlan pl;
-    pl.gx = (int)((I + 127) / 128);
-    const int64_t target = (int64_t)sms * 4;
-    int64_t S = (target + pl.gx - 1) / pl.gx;
-    S = std::max<int64_t>(1, std::min<int64_t>(S, (J + 255) / 256));
-    pl.slice = (J + S - 1) / S;
-    pl.S = (int)((J + pl.slice - 1) / pl.slice);
-    return pl;
+    return plan_rows(I, J, sms, 4, MQ_JC);
 }
 
-cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
-                                 const double *p, const SweepPlan &pl, double *out, int *err,
-                                 cudaStream_t st)
-{
-    cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_q_mixed_t<KK>(bed, I, J, q, p, pl, out, err, st));
-    return e;
-}
-
-/* One CTA per 128 SNPs and individual slice (slices are multiples of 32 individuals). */
+/* One CTA per 128 SNPs and individual slice (slices are multiples of 64 individuals). */
 SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms)
 {
     (void)K;
-    SweepPlan pl;
-    pl.gx = (int)((J + 127) / 128);
-    const int64_t target = (int64_t)sms * 4;
-    int64_t S = (target + pl.gx - 1) / pl.gx;
-    S = std::max<int64_t>(1, std::min<int64_t>(S, (I + 255) / 256));
-    int64_t slice = (I + S - 1) / S;
-    slice = (slice + 31) / 32 * 32;
-    pl.slice = slice;
-    pl.S = (int)((I + slice - 1) / slice);
-    return pl;
-}
-
-cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
-                                 const double *p, const SweepPlan &pl, double *out, int *err,
-                                 cudaStream_t st)
-{
-    cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_p_mixed_t<KK>(bed, I, J, q, p, pl, out, err, st));
-    return e;
+    return plan_rows(J, I, sms, 4, MP_IC);
 }
 
 SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms)
 {
-    SweepPlan pl;
-    pl.gx = (int)((J + 127) / 128);
-    const int64_t target = (int64_t)sms * 8;
-    int64_t S = (target + pl.gx - 1) / pl.gx;
-    S = std::max<int64_t>(1, std::min<int64_t>(S, (I + 255) / 256));
-    int64_t slice = (I + S - 1) / S;
-    slice = (slice + 63) / 64 * 64;
-    pl.slice = slice;
-    pl.S = (int)((I + slice - 1) / slice);
-    return pl;
+    return plan_rows(J, I, sms, 8, ML_IC);
 }
 
-cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, const double *q,
-                                const double *p, const SweepPlan &pl, double *partial, double *out,
-                                cudaStream_t st)
+cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
+                                 const double *p, const SweepPlan &pl, double *out, int *err, cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_ll_mixed_t<KK>(bed, I, J, q, p, pl, partial, out, st));
+    ADMIX_DISPATCH_K(K, e = launch_q_mixed_t<KK>(bed, I, J, pitch, q, p, pl, out, err, st));
+    return e;
+}
+
+cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
+                                 const double *p, const SweepPlan &pl, double *out, int *err, cudaStream_t st)
+{
+    cudaError_t e = cudaErrorInvalidValue;
+    ADMIX_DISPATCH_K(K, e = launch_p_mixed_t<KK>(bed, I, J, pitch, q, p, pl, out, err, st));
+    return e;
+}
+
+cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
+                                const double *p, const SweepPlan &pl, double *partial, double *out, cudaStream_t st)
+{
+    cudaError_t e = cudaErrorInvalidValue;
+    ADMIX_DISPATCH_K(K, e = launch_ll_mixed_t<KK>(bed, I, J, pitch, q, p, pl, partial, out, st));
     return e;
 }

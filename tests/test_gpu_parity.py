@@ -261,3 +261,23 @@ def test_c2_size_properties(oa):
     H, z = d_cu.grad_hess_q(oa.X, oa.X)
     assert _row_rel(np.einsum("ikl,il->ik", H, qn), z) < 1e-10
     d_cu.close()
+
+
+@pytest.mark.parametrize("flags", [0, 2])
+def test_padding_bits_of_the_input_are_ignored(oa, flags):
+    """The reference's loops stop at individual I, so whatever the file holds in the padding
+    bits of each column's last byte must not change any result (FP64 and mixed forms)."""
+    g = _cohort(oa, I=1027, J=700, K=4, seed=6)            # 1027 % 4 = 3: one padding field
+    dirty = g.data.copy()
+    dirty[:, -1] |= 0xC0                                    # padding field set to code 11
+    gd = oa.Genotypes(dirty, g.I, g.J)
+    vals = []
+    for gg in (g, gd):
+        d, d_cu = _handle(oa, gg, 4, seed=8, flags=flags)
+        snp, ind = d_cu.decode_counts()
+        H, z = d_cu.grad_hess_q(oa.X, oa.X)
+        vals.append((d_cu.loglik(oa.X), snp, ind, H, z))
+        d_cu.close()
+    assert vals[0][0] == vals[1][0]
+    assert np.array_equal(vals[0][1], vals[1][1]) and np.array_equal(vals[0][2], vals[1][2])
+    assert np.array_equal(vals[0][3], vals[1][3]) and np.array_equal(vals[0][4], vals[1][4])
