@@ -30,7 +30,7 @@ for _p in (ROOT, ROOT / "oracle"):
     if str(_p) not in sys.path:
         sys.path.insert(0, str(_p))
 
-METRIC = "genotype*K^2/s per iteration (plain FP64 form, 1 B200)"
+METRIC = "genotype*K^2/s per iteration (chosen form; plain FP64 form timed beside it), 1 B200"
 UNIT = "genotype*K^2/s"
 
 
@@ -41,10 +41,11 @@ def _args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--config", default="c2")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain", choices=["plain", "mixed"],
+    ap.add_argument("--form", default="mixed", choices=["plain", "mixed"],
                     help="plain: FP64 sweeps; mixed: tensor-core BF16 Hessian, FP32 gradient")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ttc", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 form beside the chosen one")
     ap.add_argument("--pass-only", default=None,
                     choices=["loglik", "q_sweep", "p_sweep", "q_qp", "p_qp", "em"],
                     help="set up the cohort and launch one pass warmup+steps times (for profilers)")
@@ -59,7 +60,11 @@ def run_pass_only(args):
     from openadmixture_b200 import _native as N
     torch.cuda.set_device(0)
     spec = oa.COHORTS[args.config]
-    g, _, _ = oa.make_cohort(spec)
+    if spec.I * spec.J > 2_000_000_000:
+        qt, pt = oa.truth(spec)
+        g = oa.genotypes_device(spec, qt, pt)
+    else:
+        g, _, _ = oa.make_cohort(spec)
     d = oa.AdmixData(spec.I, spec.J, spec.K, 3, rng=100)
     flags = oa.ADMIX_FLAG_MIXED if args.form == "mixed" else 0
     with oa.CuAdmixData(d, g, flags=flags) as d_cu:
@@ -150,11 +155,16 @@ def _cpu_sample_spec(oa, spec, J_sample):
     return spec.scaled(J=J_sample)
 
 
+def _cpu_sample_J(spec, cells=2e8):
+    """SNP subset for the CPU runs: about `cells` genotype cells per pass."""
+    return int(max(200, min(spec.J, cells / spec.I)))
+
+
 def cpu_baseline(oa, spec, steps=2):
     """The oracle (C restatement, OpenMP on all host cores) on a bounded SNP sample of the
     same cohort: QN iterations from an EM-primed start, metric scaled by the sample."""
     import oracle
-    J_s = max(500, min(spec.J, 20000))
+    J_s = _cpu_sample_J(spec)
     s = _cpu_sample_spec(oa, spec, J_s)
     g, _, _ = oa.make_cohort(s)
     x0 = oa.init_x(s.I, s.J, s.K, 5)
@@ -177,7 +187,7 @@ def run_reference(args, rank, world):
     import oracle
     import openadmixture_b200 as oa
     spec = oa.COHORTS[args.config]
-    J_s = max(500, min(spec.J, 4000))
+    J_s = _cpu_sample_J(spec, 4e7)
     s = spec.scaled(J=J_s)
     g, _, _ = oa.make_cohort(s)
     r = oracle.OracleRun(g.data, s.I, s.J, s.K, 3, oa.init_x(s.I, s.J, s.K, 5))
@@ -220,7 +230,11 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     spec = oa.COHORTS[args.config].scaled(seed=rank)
     t0 = time.perf_counter()
-    g, _, _ = oa.make_cohort(spec)
+    if spec.I * spec.J > 2_000_000_000:          # large cohorts: draw the genotypes on the GPU
+        qt, pt = oa.truth(spec)
+        g = oa.genotypes_device(spec, qt, pt)
+    else:
+        g, _, _ = oa.make_cohort(spec)
     t_gen = time.perf_counter() - t0
     d = oa.AdmixData(spec.I, spec.J, spec.K, 3, rng=100 + rank)
     x_init = d.x.copy()
@@ -271,7 +285,10 @@ def run_ours(args, rank, world, local_rank):
         passes[name] = d_cu.time_pass(pid, 5)
     per_iter = {k: 2 * v for k, v in passes.items()}
     dom = max(per_iter, key=per_iter.get)
-    kern_name = {"loglik": "k_loglik_f64", "q_sweep": "k_sweep_q_mixed" if args.form == "mixed" else "k_sweep_q_f64", "p_sweep": "k_sweep_p_f64",
+    mx = args.form == "mixed"
+    kern_name = {"loglik": "k_loglik_mixed" if mx else "k_loglik_f64",
+                 "q_sweep": "k_sweep_q_mixed" if mx else "k_sweep_q_f64",
+                 "p_sweep": "k_sweep_p_mixed" if mx else "k_sweep_p_f64",
                  "q_qp": "k_qp", "p_qp": "k_qp"}[dom]
     Ib = (spec.I + 3) // 4
     K = spec.K
@@ -295,10 +312,17 @@ def run_ours(args, rank, world, local_rank):
             "frac": achieved / hbm, "peak_kind": peak_kind,
             "traffic": _traffic(kern_name, spec.name),
             "alg_bytes_per_launch": alg_bytes[dom], "launch_ms": passes[dom]}
-    if dom in flops:
+    T = K * (K + 1) // 2
+    if mx and dom in ("q_sweep", "p_sweep"):
+        terms = 2 if dom == "q_sweep" else 1          # [W1 | W2] x [PP ; PbPb]  or  C x QQ
+        roof["tensor_tflops"] = 2 * spec.I * spec.J * terms * T / (passes[dom] / 1e3) / 1e12
+        roof["note"] = ("mixed form: the Hessian contraction runs on tcgen05 (tensor_tflops, far below the "
+                        "pipe's peak); the sweep is bound by the FP32 producer's issue rate, not by HBM; "
+                        "frac is the HBM fraction of its packed-genotype stream")
+    elif dom in flops:
         roof["fp64_tflops"] = flops[dom] / (passes[dom] / 1e3) / 1e12
-    roof["note"] = ("FP64 plain form: the sweep is bound by the FP64 pipe, not HBM; frac is the HBM "
-                    "fraction of its packed-genotype stream")
+        roof["note"] = ("FP64 plain form: the sweep is bound by the FP64 pipe, not HBM; frac is the HBM "
+                        "fraction of its packed-genotype stream")
 
     # end-to-end through the C ABI with host buffers (pinned), H2D + D2H inside the timed region
     qh = torch.from_numpy(np.ascontiguousarray(x_em[: spec.I])).pin_memory()
@@ -339,7 +363,48 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         ttc = {"seconds": g0.elapsed_time(g1) / 1e3, "iterations": n_done.value, "converged": bool(conv.value),
                "final_ll": hist[n_done.value - 1].ll_new if n_done.value else None,
+               "final_ll_fp64": d_cu.loglik(oa.X),
                "from": "5 EM iterations (not timed)"}
+
+    # the plain FP64 form on the same cohort and start, for the chosen-vs-plain comparison
+    vs_plain = None
+    if mx and not args.no_plain:
+        with oa.CuAdmixData(d, g, flags=0) as hp:
+            hp.upload(oa.X, x_em)
+            hp.set_ll(ll_em)
+            sp_ = torch.cuda.ExternalStream(hp.stream())
+            ps = max(3, min(args.steps, 5))
+            for w in range(1, 3):
+                hp._chk(lib.admix_qn_iteration(hp.handle, w, C_byref(info)))
+            torch.cuda.synchronize()
+            h0 = torch.cuda.Event(enable_timing=True); h1 = torch.cuda.Event(enable_timing=True)
+            h0.record(sp_)
+            for w in range(3, 3 + ps):
+                hp._chk(lib.admix_qn_iteration(hp.handle, w, C_byref(info)))
+            h1.record(sp_)
+            torch.cuda.synchronize()
+            plain_ms = h0.elapsed_time(h1) / ps
+            vs_plain = {"plain_ms_per_step": plain_ms, "plain_value": world * work / (plain_ms / 1e3),
+                        "speedup_per_iteration": plain_ms / (ms_max / args.steps)}
+            too_long = ttc is not None and plain_ms * (ttc["iterations"] + 10) > 120e3
+            if too_long:
+                vs_plain["plain_ttc_skipped"] = (f"plain form at {plain_ms / 1e3:.1f} s per iteration would run for "
+                                                 f"minutes; per-iteration ratio reported instead")
+            if ttc is not None and not too_long:
+                hp.upload(oa.X, x_em)
+                hp.set_ll(ll_em)
+                hist_p = (N.IterInfo * 1000)()
+                n_p = C.c_int32(); conv_p = C.c_int32()
+                torch.cuda.synchronize()
+                h0.record(sp_)
+                hp._chk(lib.admix_run_qn(hp.handle, 1000, 1e-7, 0, hist_p, C.byref(n_p), C.byref(conv_p)))
+                h1.record(sp_)
+                torch.cuda.synchronize()
+                ll_plain = hp.loglik(oa.X)
+                vs_plain.update({"plain_ttc_seconds": h0.elapsed_time(h1) / 1e3, "plain_iterations": n_p.value,
+                                 "ttc_speedup": (h0.elapsed_time(h1) / 1e3) / ttc["seconds"],
+                                 "plain_final_ll_fp64": ll_plain,
+                                 "chosen_vs_plain_final_ll_rel": abs(ttc["final_ll_fp64"] - ll_plain) / abs(ll_plain)})
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -354,10 +419,12 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32+f64" if mx else "f64", "data": "synthetic",
         "config": {"workload": f"{spec.name}: admixture_qn iteration, I={spec.I} J={spec.J} K={spec.K}, "
-                               f"{spec.miss:.1%} missing, plain FP64 form",
-                   "I": spec.I, "J": spec.J, "K": spec.K, "Q": 3, "form": "plain-fp64",
+                               f"{spec.miss:.1%} missing, "
+                               + ("mixed form: tcgen05 BF16 Hessians, FP32 gradients and loglik cells, FP64 "
+                                  "reductions / QPs / QN" if mx else "plain FP64 form"),
+                   "I": spec.I, "J": spec.J, "K": spec.K, "Q": 3, "form": "mixed" if mx else "plain-fp64",
                    "l2": f"inputs larger than L2: {bytes_bed / 1e6:.0f} MB packed genotypes streamed per pass",
                    "per_rank": "independent cohort per rank (seed = rank)"},
         "e2e": {"value": world * work / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": xbytes,
@@ -367,6 +434,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof,
         "passes_ms": passes,
         "ttc": ttc,
+        "vs_plain": vs_plain,
         "setup_s": {"generate": t_gen, "create_upload": t_upload},
         "clocks": clk,
         "cpu_baseline": cpu,

@@ -69,6 +69,11 @@ typedef struct {
  * K in [1, ADMIX_MAX_K], Q in [1, ADMIX_MAX_Q]. */
 int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
                  uint32_t flags, admix_ctx **out);
+/* Same, with the genotype bytes already on the current device (the reference's g_cu, a
+ * CuMatrix{UInt8} of ceil(I/4) x J, cuda/structs.jl:36-37), columns src_pitch bytes apart
+ * (src_pitch >= ceil(I/4)).  The bytes are copied; the caller keeps ownership of d_bed. */
+int admix_create_device(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *d_bed, int64_t src_pitch,
+                        uint32_t flags, admix_ctx **out);
 int admix_destroy(admix_ctx *h);
 /* Last error message of h (or of the calling thread's last failed admix_create when h is NULL). */
 const char *admix_last_error(const admix_ctx *h);

@@ -10,13 +10,13 @@ from ._native import AdmixError, IterInfo, ADMIX_FLAG_MIXED, ADMIX_FLAG_MU_GERSH
 from .admixture import (AdmixData, CuAdmixData, X, X_NEXT, X_NEXT2, X_TMP, _cu_admixture_base,
                         admixture_qn, em_p, em_q, init_em, loglikelihood, run_admixture, update_p,
                         update_q)
-from .bed import BedFormatError, Genotypes, read_bed, write_bed
-from .synth import COHORTS, CohortSpec, genotypes, init_x, make_cohort, truth
+from .bed import BedFormatError, DeviceGenotypes, Genotypes, read_bed, write_bed
+from .synth import COHORTS, CohortSpec, genotypes, genotypes_device, init_x, make_cohort, truth
 
 __all__ = [
-    "AdmixData", "CuAdmixData", "AdmixError", "IterInfo", "Genotypes", "BedFormatError",
+    "AdmixData", "CuAdmixData", "AdmixError", "IterInfo", "Genotypes", "DeviceGenotypes", "BedFormatError",
     "X", "X_NEXT", "X_NEXT2", "X_TMP", "ADMIX_FLAG_MIXED", "ADMIX_FLAG_MU_GERSHGORIN",
     "_cu_admixture_base", "admixture_qn", "em_p", "em_q", "init_em", "loglikelihood",
     "run_admixture", "update_p", "update_q", "read_bed", "write_bed",
-    "COHORTS", "CohortSpec", "genotypes", "init_x", "make_cohort", "truth",
+    "COHORTS", "CohortSpec", "genotypes", "genotypes_device", "init_x", "make_cohort", "truth",
 ]

@@ -24,7 +24,7 @@ import time
 import numpy as np
 
 from . import _native as N
-from .bed import Genotypes, read_bed
+from .bed import DeviceGenotypes, Genotypes, read_bed
 from .synth import init_x
 
 X, X_NEXT, X_NEXT2, X_TMP = N.ADMIX_X, N.ADMIX_X_NEXT, N.ADMIX_X_NEXT2, N.ADMIX_X_TMP
@@ -80,7 +80,11 @@ class CuAdmixData:
             raise ValueError(f"genotypes are {g.I} x {g.J}, AdmixData is {d.I} x {d.J}")
         lib = N.admix_lib()
         h = C.c_void_p()
-        N.check(lib.admix_create(d.I, d.J, d.K, d.Q, N.u8ptr(g.data), flags, C.byref(h)), None)
+        if isinstance(g, DeviceGenotypes):
+            N.check(lib.admix_create_device(d.I, d.J, d.K, d.Q, C.c_void_p(g.data.data_ptr()), g.Ib, flags,
+                                            C.byref(h)), None)
+        else:
+            N.check(lib.admix_create(d.I, d.J, d.K, d.Q, N.u8ptr(g.data), flags, C.byref(h)), None)
         self._h = h
         self.I, self.J, self.K, self.Q = d.I, d.J, d.K, d.Q
         self.flags = flags

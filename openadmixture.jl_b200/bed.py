@@ -104,3 +104,19 @@ def write_bed(path: str | os.PathLike, g: Genotypes, write_sidecars: bool = True
             for j in range(g.J):
                 f.write(f"1 snp{j} 0 {j + 1} A C\n")
     return path
+
+
+@dataclass
+class DeviceGenotypes:
+    """Packed genotypes already in device memory (the reference's g_cu, cuda/structs.jl:36-37):
+    `data` is a CUDA tensor of uint8, shape (J, ceil(I/4)), one SNP column per row."""
+    data: object
+    I: int
+    J: int
+
+    @property
+    def Ib(self) -> int:
+        return (self.I + 3) // 4
+
+    def to_host(self) -> Genotypes:
+        return Genotypes(self.data.cpu().numpy(), self.I, self.J)

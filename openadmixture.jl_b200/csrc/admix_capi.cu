@@ -119,8 +119,10 @@ extern "C" {
 
 const char *admix_last_error(const admix_ctx *h) { return h ? h->err : g_err; }
 
-int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed, uint32_t flags,
-                 admix_ctx **out)
+/* Shared by admix_create (host genotypes) and admix_create_device (device genotypes at
+ * src_pitch bytes per column). */
+static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed, bool on_device,
+                         int64_t src_pitch, uint32_t flags, admix_ctx **out)
 {
     if (!out) return fail(nullptr, ADMIX_ERR_ARG, "out is NULL");
     *out = nullptr;
@@ -179,8 +181,8 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
     /* genotypes in HBM: columns at a 16-byte pitch, padding bytes and the padding bits of each
      * column's last byte set to the missing code 01 (never read by the reference's loops) */
     TRYC(cudaMemsetAsync(h->bed, 0x55, (size_t)h->pitch * J + 64, h->st));
-    TRYC(cudaMemcpy2DAsync(h->bed, (size_t)h->pitch, bed, (size_t)h->Ib, (size_t)h->Ib, (size_t)J,
-                           cudaMemcpyHostToDevice, h->st));
+    TRYC(cudaMemcpy2DAsync(h->bed, (size_t)h->pitch, bed, (size_t)src_pitch, (size_t)h->Ib, (size_t)J,
+                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->st));
     TRYC(launch_mask_tail(h->bed, I, J, h->pitch, h->sms, h->st));
     TRYC(cudaMemsetAsync(h->xbuf, 0, sizeof(double) * 4 * nx, h->st));
     TRYC(cudaMemsetAsync(h->U, 0, sizeof(double) * nx * Q, h->st));
@@ -197,6 +199,25 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
 #undef TRYC
     *out = h;
     return ADMIX_OK;
+}
+
+int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed, uint32_t flags,
+                 admix_ctx **out)
+{
+    return create_common(I, J, K, Q, bed, false, (I + 3) / 4, flags, out);
+}
+
+int admix_create_device(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *d_bed, int64_t src_pitch,
+                        uint32_t flags, admix_ctx **out)
+{
+    if (src_pitch < (I + 3) / 4) return fail(nullptr, ADMIX_ERR_ARG, "src_pitch %lld is below ceil(I/4) = %lld",
+                                             (long long)src_pitch, (long long)((I + 3) / 4));
+    cudaPointerAttributes at;
+    if (d_bed && (cudaPointerGetAttributes(&at, d_bed) != cudaSuccess || at.type != cudaMemoryTypeDevice)) {
+        cudaGetLastError();
+        return fail(nullptr, ADMIX_ERR_ARG, "d_bed is not device memory");
+    }
+    return create_common(I, J, K, Q, d_bed, true, src_pitch, flags, out);
 }
 
 int admix_destroy(admix_ctx *h)

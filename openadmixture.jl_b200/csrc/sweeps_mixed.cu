@@ -70,7 +70,8 @@ struct MQ {
     static constexpr uint32_t A_BYTES = 128 * MQ_JC * 2;        /* one BF16 weight tile: 8 KB */
     static constexpr uint32_t B_BYTES = N * MQ_JC * 2;          /* one BF16 pair-product tile */
     static constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr uint32_t PBUF = 2 * K * MQ_JC * 4;         /* p and 1-p of one chunk, FP32 */
+    static constexpr int PS = MQ_JC + 2;                        /* P row stride (floats): rows on distinct banks */
+    static constexpr uint32_t PBUF = 2 * K * PS * 4;            /* p and 1-p of one chunk, FP32 [k][jj] */
     static constexpr uint32_t GBUF = MQ_JC * 32;                /* genotype bytes of one chunk */
     static constexpr uint32_t OFF_P = 2 * STAGE_BYTES;          /* two P buffers */
     static constexpr uint32_t OFF_G = OFF_P + 2 * PBUF;         /* two G buffers, [pair][byte][2] */
@@ -104,9 +105,9 @@ __device__ __forceinline__ void qchunk_load(QChunk<K> &cr, const uint8_t *__rest
     }
 #pragma unroll
     for (int u = 0; u < MQ<K>::PREF_P; ++u) {
-        const int t = tid + u * MQ_THREADS;          /* t = jj * K + k over the chunk's K*JC values */
-        const int jj = t / K;
-        cr.pv[u] = (t < K * MQ_JC && jj < n) ? p[(size_t)K * jc + t] : 0.5;
+        const int t = tid + u * MQ_THREADS;          /* t = k * JC + jj: shared stores hit distinct banks */
+        const int k = t / MQ_JC, jj = t - k * MQ_JC;
+        cr.pv[u] = (t < K * MQ_JC && jj < n) ? p[(size_t)K * (jc + jj) + k] : 0.5;
     }
 }
 
@@ -122,9 +123,9 @@ __device__ __forceinline__ void qchunk_store(const QChunk<K> &cr, float *Pb, uin
     for (int u = 0; u < MQ<K>::PREF_P; ++u) {
         const int t = tid + u * MQ_THREADS;
         if (t < K * MQ_JC) {
-            const int jj = t / K, k = t - jj * K;
-            Pb[k * MQ_JC + jj] = (float)cr.pv[u];
-            Pb[K * MQ_JC + k * MQ_JC + jj] = (float)(1.0 - cr.pv[u]);
+            const int k = t / MQ_JC, jj = t - k * MQ_JC;
+            Pb[k * MQ<K>::PS + jj] = (float)cr.pv[u];
+            Pb[K * MQ<K>::PS + k * MQ<K>::PS + jj] = (float)(1.0 - cr.pv[u]);
         }
     }
 }
@@ -203,19 +204,19 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             if (nn < T) {
                 int ka, kb;
                 tri_pair(nn, ka, kb);
-                const float *src = Pb + term * K * MQ_JC;
+                const float *src = Pb + term * K * C::PS;
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int jj = kc * 8 + 2 * e;
-                    w[e] = pack_bf16x2(src[ka * MQ_JC + jj] * src[kb * MQ_JC + jj],
-                                       src[ka * MQ_JC + jj + 1] * src[kb * MQ_JC + jj + 1]);
+                    w[e] = pack_bf16x2(src[ka * C::PS + jj] * src[kb * C::PS + jj],
+                                       src[ka * C::PS + jj + 1] * src[kb * C::PS + jj + 1]);
                 }
             }
             *(uint4 *)(Bt + term * C::B_BYTES + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
         }
         /* producer: this thread's individual, the chunk's 32 SNPs as 16 pairs */
-        const float2 *P2 = (const float2 *)Pb;                  /* [k][pair] */
-        const float2 *Pb2 = (const float2 *)(Pb + K * MQ_JC);
+        const float2 *P2 = (const float2 *)Pb;                  /* [k][pair], row stride PS / 2 */
+        const float2 *Pb2 = (const float2 *)(Pb + K * C::PS);
         const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);  /* [pair][byte]: both SNPs */
         float2 ga[K];
 #pragma unroll
@@ -233,8 +234,8 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 float2 pv[K], pbv[K];
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    pv[k] = P2[k * (MQ_JC / 2) + m];
-                    pbv[k] = Pb2[k * (MQ_JC / 2) + m];
+                    pv[k] = P2[k * (C::PS / 2) + m];
+                    pbv[k] = Pb2[k * (C::PS / 2) + m];
                     qp = __ffma2_rn(qq[k], pv[k], qp);
                     om = __ffma2_rn(qq[k], pbv[k], om);
                 }
@@ -332,7 +333,8 @@ struct MP {
     static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* one BF16 weight tile: 16 KB */
     static constexpr uint32_t B_BYTES = N * MP_IC * 2;
     static constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
-    static constexpr uint32_t QBUF = K * MP_IC * 4;             /* q of one chunk, FP32 [k][i] */
+    static constexpr int QS = MP_IC + 2;                        /* q row stride (floats) */
+    static constexpr uint32_t QBUF = K * QS * 4;                /* q of one chunk, FP32 [k][i] */
     static constexpr uint32_t OFF_Q = 2 * STAGE_BYTES;
     static constexpr uint32_t OFF_TAB = OFF_Q + 2 * QBUF;
     static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024;
@@ -387,9 +389,9 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     auto qload = [&](int64_t ic) {
 #pragma unroll
         for (int u = 0; u < C::PREF_Q; ++u) {
-            const int t = tid + u * MP_THREADS;              /* t = ii * K + k */
-            const int ii = t / K;
-            qr[u] = (t < K * MP_IC && ic + ii < ib) ? q[(size_t)K * ic + t] : 1.0 / K;
+            const int t = tid + u * MP_THREADS;              /* t = k * IC + ii */
+            const int k = t / MP_IC, ii = t - k * MP_IC;
+            qr[u] = (t < K * MP_IC && ic + ii < ib) ? q[(size_t)K * (ic + ii) + k] : 1.0 / K;
         }
     };
     auto qstore = [&](float *Qb) {
@@ -397,8 +399,8 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         for (int u = 0; u < C::PREF_Q; ++u) {
             const int t = tid + u * MP_THREADS;
             if (t < K * MP_IC) {
-                const int ii = t / K, k = t - ii * K;
-                Qb[k * MP_IC + ii] = (float)qr[u];
+                const int k = t / MP_IC, ii = t - k * MP_IC;
+                Qb[k * C::QS + ii] = (float)qr[u];
             }
         }
     };
@@ -452,8 +454,8 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int ii = kc * 8 + 2 * e;
-                    w[e] = pack_bf16x2(Qb[ka * MP_IC + ii] * Qb[kb * MP_IC + ii],
-                                       Qb[ka * MP_IC + ii + 1] * Qb[kb * MP_IC + ii + 1]);
+                    w[e] = pack_bf16x2(Qb[ka * C::QS + ii] * Qb[kb * C::QS + ii],
+                                       Qb[ka * C::QS + ii + 1] * Qb[kb * C::QS + ii + 1]);
                 }
             }
             *(uint4 *)(Bt + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -473,7 +475,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 float2 qv[K];
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
-                    qv[k] = Q2[k * (MP_IC / 2) + m];
+                    qv[k] = Q2[k * (C::QS / 2) + m];
                     qp = __ffma2_rn(qv[k], pd[k], qp);
                     om = __ffma2_rn(qv[k], pbd[k], om);
                 }
@@ -583,9 +585,9 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
     auto load = [&](int64_t ic) {
 #pragma unroll
         for (int u = 0; u < PREF; ++u) {
-            const int t = tid + u * 128;                 /* t = ii * K + k */
-            const int ii = t / K;
-            qr[u] = (t < K * ML_IC && ic + ii < ib) ? (float)q[(size_t)K * ic + t] : 1.0f / K;
+            const int t = tid + u * 128;                 /* t = k * IC + ii */
+            const int k = t / ML_IC, ii = t - k * ML_IC;
+            qr[u] = (t < K * ML_IC && ic + ii < ib) ? (float)q[(size_t)K * (ic + ii) + k] : 1.0f / K;
         }
         gnext = col_load64(bed, pitch, j, valid, ic);
     };
@@ -594,7 +596,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
         for (int u = 0; u < PREF; ++u) {
             const int t = tid + u * 128;
             if (t < K * ML_IC) {
-                const int ii = t / K, k = t - ii * K;
+                const int k = t / ML_IC, ii = t - k * ML_IC;
                 ((float *)Qs[s][k])[ii] = qr[u];
             }
         }

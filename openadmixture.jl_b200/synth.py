@@ -12,7 +12,7 @@ from dataclasses import dataclass, replace
 import numpy as np
 
 from . import _native as N
-from .bed import Genotypes
+from .bed import DeviceGenotypes, Genotypes
 
 
 @dataclass(frozen=True)
@@ -69,6 +69,22 @@ def genotypes(spec: CohortSpec, q: np.ndarray, p: np.ndarray) -> Genotypes:
     if rc != 0:
         raise ValueError(f"syn_bed_host failed for {spec}")
     return Genotypes(data, spec.I, spec.J)
+
+
+def genotypes_device(spec: CohortSpec, q: np.ndarray, p: np.ndarray) -> DeviceGenotypes:
+    """The same genotype bytes as genotypes(), drawn on the current CUDA device (for cohorts too
+    large to draw on the host quickly, e.g. 25 GB of packed genotypes)."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dq = torch.from_numpy(np.ascontiguousarray(q)).to(dev)
+    dp = torch.from_numpy(np.ascontiguousarray(p)).to(dev)
+    bed = torch.empty((spec.J, (spec.I + 3) // 4), dtype=torch.uint8, device=dev)
+    rc = N.synth_lib().syn_bed_device(spec.I, spec.J, spec.K, spec.seed, spec.miss, dq.data_ptr(), dp.data_ptr(),
+                                      bed.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"syn_bed_device failed for {spec}")
+    torch.cuda.synchronize()
+    return DeviceGenotypes(bed, spec.I, spec.J)
 
 
 def make_cohort(spec: CohortSpec) -> tuple[Genotypes, np.ndarray, np.ndarray]:

@@ -44,6 +44,9 @@ def test_create_rejects_bad_arguments_without_touching_a_gpu(oa):
     assert lib.admix_create(4, 4, 3, 3, None, 0, C.byref(h)) == N.ADMIX_ERR_ARG
     assert lib.admix_create(4, 4, 3, 3, N.u8ptr(bed), 0x100, C.byref(h)) == N.ADMIX_ERR_ARG
     assert lib.admix_loglik_dev(None, 4, 4, 3, None, None, None, None, 0, None) == N.ADMIX_ERR_ARG
+    # device variant: a source pitch below ceil(I/4) is rejected before any device call
+    assert lib.admix_create_device(40, 4, 3, 3, None, 9, 0, C.byref(h)) == N.ADMIX_ERR_ARG
+    assert b"src_pitch" in lib.admix_last_error(None)
 
 
 def test_engine_requires_gpu_path(oa):

@@ -281,3 +281,20 @@ def test_padding_bits_of_the_input_are_ignored(oa, flags):
     assert vals[0][0] == vals[1][0]
     assert np.array_equal(vals[0][1], vals[1][1]) and np.array_equal(vals[0][2], vals[1][2])
     assert np.array_equal(vals[0][3], vals[1][3]) and np.array_equal(vals[0][4], vals[1][4])
+
+
+def test_device_generated_cohort_and_device_create(oa):
+    """The device generator draws the host generator's bytes, and a handle created from device
+    genotypes (admix_create_device) computes what the host-created one does."""
+    spec = oa.COHORTS["c1"].scaled(I=1003, J=2111, K=4, seed=12)
+    q, p = oa.truth(spec)
+    gh = oa.genotypes(spec, q, p)
+    gd = oa.genotypes_device(spec, q, p)
+    assert np.array_equal(gd.to_host().data, gh.data)
+    lls = []
+    for g in (gh, gd):
+        d, h = _handle(oa, g, 4, seed=3)
+        lls.append((h.loglik(oa.X), h.decode_counts()))
+        h.close()
+    assert lls[0][0] == lls[1][0]
+    assert np.array_equal(lls[0][1][0], lls[1][1][0]) and np.array_equal(lls[0][1][1], lls[1][1][1])
