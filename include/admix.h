@@ -182,6 +182,42 @@ int admix_loglik_dev_noalloc(const uint8_t *d_bed, int64_t I, int64_t J, int32_t
                              const double *d_q, const double *d_p, double *d_out, void *stream);
 const char *admix_noalloc_last_error(void);
 
+/* --- learned warm start (no counterpart in the reference; hooks into run_admixture's
+ *     init_q / init_p, driver.jl:52-53,161-166,183-188) ---------------------------------- */
+
+/* Sketch of each individual: dosages of the S SNPs listed in d_snps (int8, 3 = missing, I x S),
+ * their allele frequencies d_freq (S), and R <= 32 projections of the frequency-standardised
+ * dosages onto fixed +-1 directions drawn from `seed` (I x R).  Asynchronous on `stream`. */
+int admix_sketch(const uint8_t *d_bed, int64_t pitch, int64_t I, const int32_t *d_snps, int32_t S,
+                 int32_t R, uint64_t seed, float *d_freq, int8_t *d_dos, float *d_proj, void *stream);
+
+/* MLP encoder (S + R) -> H -> H -> K: ReLU, ReLU, softmax.  Row-major FP32 device arrays:
+ * w1 (S+R) x H, w2 H x H, w3 H x K, biases of length H, H, K. */
+typedef struct {
+    int32_t S, R, H, K;
+    const float *w1, *b1, *w2, *b2, *w3, *b3;
+} admix_mlp;
+typedef struct {
+    float *w1, *b1, *w2, *b2, *w3, *b3;
+} admix_mlp_grads;
+
+/* Forward pass of n individuals: hidden activations h1, h2 (n x H), logits and probs (n x K). */
+int admix_mlp_forward(const admix_mlp *net, int64_t n, const int8_t *dos, const float *center, const float *proj,
+                      float *h1, float *h2, float *logits, float *probs, void *stream);
+/* Backward pass of the mean cross-entropy against soft targets (n x K): gradients into grad,
+ * scratch dlogits (n x K), dh2, dh1 (n x H); the summed loss is added into *loss. */
+int admix_mlp_backward(const admix_mlp *net, const admix_mlp_grads *grad, int64_t n, const int8_t *dos,
+                       const float *center, const float *proj, const float *h1, const float *h2, const float *logits,
+                       const float *target, float *probs, float *dlogits, float *dh2, float *dh1, float *loss,
+                       void *stream);
+/* One Adam step (step number t >= 1) on n parameters. */
+int admix_mlp_adam(float *w, const float *g, float *m, float *v, int64_t n, float lr, float beta1, float beta2,
+                   float eps, int32_t t, void *stream);
+/* Starting P from a predicted Q (K x I): p_kj = sum_i nm q_ki g_ij / (2 sum_i nm q_ki), clamped to
+ * [1e-5, 1 - 1e-5]; output K x J. */
+int admix_warm_p(const uint8_t *d_bed, int64_t pitch, int64_t I, int64_t J, int32_t K, const double *d_q,
+                 double *d_p, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,6 +12,7 @@ from .admixture import (AdmixData, CuAdmixData, X, X_NEXT, X_NEXT2, X_TMP, _cu_a
                         update_q)
 from .bed import BedFormatError, DeviceGenotypes, Genotypes, read_bed, write_bed
 from .synth import COHORTS, CohortSpec, genotypes, genotypes_device, init_x, make_cohort, truth
+from . import warmstart
 
 __all__ = [
     "AdmixData", "CuAdmixData", "AdmixError", "IterInfo", "Genotypes", "DeviceGenotypes", "BedFormatError",
@@ -19,4 +20,5 @@ __all__ = [
     "_cu_admixture_base", "admixture_qn", "em_p", "em_q", "init_em", "loglikelihood",
     "run_admixture", "update_p", "update_q", "read_bed", "write_bed",
     "COHORTS", "CohortSpec", "genotypes", "genotypes_device", "init_x", "make_cohort", "truth",
+    "warmstart",
 ]

@@ -48,6 +48,17 @@ class IterInfo(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class MLPNet(C.Structure):
+    _fields_ = [("S", C.c_int32), ("R", C.c_int32), ("H", C.c_int32), ("K", C.c_int32),
+                ("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
+                ("w3", C.c_void_p), ("b3", C.c_void_p)]
+
+
+class MLPGrads(C.Structure):
+    _fields_ = [("w1", C.c_void_p), ("b1", C.c_void_p), ("w2", C.c_void_p), ("b2", C.c_void_p),
+                ("w3", C.c_void_p), ("b3", C.c_void_p)]
+
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -82,6 +93,13 @@ ADMIX_SIGNATURES = {
     "admix_loglik_dev_workspace": (C.c_size_t, [C.c_int64, C.c_int64, C.c_int32]),
     "admix_loglik_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P, C.c_size_t, _P]),
     "admix_loglik_dev_noalloc": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P, _P]),
+    "admix_sketch": (C.c_int, [_P, C.c_int64, C.c_int64, _P, C.c_int32, C.c_int32, C.c_uint64, _P, _P, _P, _P]),
+    "admix_mlp_forward": (C.c_int, [C.POINTER(MLPNet), C.c_int64, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "admix_mlp_backward": (C.c_int, [C.POINTER(MLPNet), C.POINTER(MLPGrads), C.c_int64, _P, _P, _P, _P, _P, _P,
+                                     _P, _P, _P, _P, _P, _P, _P]),
+    "admix_mlp_adam": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float,
+                                 C.c_int32, _P]),
+    "admix_warm_p": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P]),
     "admix_noalloc_last_error": (C.c_char_p, []),
 }
 

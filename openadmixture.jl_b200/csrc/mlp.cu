@@ -1,0 +1,351 @@
+/*
+ * mlp.cu -- the learned warm start: genotype sketch, a small MLP encoder (forward, backward,
+ * Adam) and the closed-form P step that turns a predicted Q into a starting P.
+ *
+ * This part has no counterpart in the reference.  Its hook is run_admixture's init_q / init_p
+ * (driver.jl:52-53,161-166,183-188): the predicted Q and the derived P replace the random start
+ * and the EM priming.
+ *
+ * Features of individual i: the dosages of S fixed sketch SNPs (int8; 3 = missing) and R
+ * projections of the frequency-standardised dosages onto fixed +-1 directions,
+ *   proj_ir = S^-1/2 sum_s (d_is - 2 f_s) / sqrt(2 f_s (1 - f_s)) * sign_rs     (missing -> 0).
+ * Network: x = [d - 2f | proj] (S + R) -> ReLU(W1 x + b1) (H) -> ReLU(W2 . + b2) (H) ->
+ * softmax(W3 . + b3) (K).  Loss: cross-entropy against soft targets (aligned converged Q).
+ * All matrices are row-major FP32 (W1: (S+R) x H, W2: H x H, W3: H x K).
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include "../../include/admix.h"
+#include "common.cuh"
+#include "synth.h"
+
+namespace {
+
+__device__ __forceinline__ int code_of(const uint8_t *bed, int64_t pitch, int64_t i, int64_t j)
+{
+    return (bed[(size_t)j * pitch + (i >> 2)] >> ((i & 3) << 1)) & 3;
+}
+
+/* 2-bit code -> dosage: 00 -> 0, 10 -> 1, 11 -> 2, 01 (missing) -> 3 */
+__device__ __forceinline__ int8_t dosage_of(int c) { return c == 1 ? (int8_t)3 : (int8_t)(c == 0 ? 0 : c - 1); }
+
+/* allele frequency of each sketch SNP: one block per SNP */
+__global__ void k_sketch_freq(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I,
+                              const int32_t *__restrict__ snps, float *__restrict__ freq)
+{
+    __shared__ double red[8];
+    const int64_t j = snps[blockIdx.x];
+    double a = 0.0, n = 0.0;
+    for (int64_t i = threadIdx.x; i < I; i += blockDim.x) {
+        const int c = code_of(bed, pitch, i, j);
+        if (c != 1) { a += (c == 0) ? 0.0 : (double)(c - 1); n += 2.0; }
+    }
+    const double sa = block_sum(a, red);
+    const double sn = block_sum(n, red);
+    if (threadIdx.x == 0) freq[blockIdx.x] = sn > 0.0 ? (float)(sa / sn) : 0.5f;
+}
+
+/* dosage sketch (I x S int8) and the R standardised projections (I x R) */
+__global__ void k_sketch(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, const int32_t *__restrict__ snps,
+                         int S, const float *__restrict__ freq, int R, uint64_t seed, int8_t *__restrict__ dos,
+                         float *__restrict__ proj)
+{
+    extern __shared__ float sh[];                     /* [R] partial projections per warp */
+    const int64_t i = blockIdx.x;
+    float acc[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) acc[r] = 0.f;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+        const int c = code_of(bed, pitch, i, snps[s]);
+        const int8_t d = dosage_of(c);
+        dos[(size_t)i * S + s] = d;
+        if (d != 3) {
+            const float f = freq[s];
+            const float z = ((float)d - 2.f * f) * rsqrtf(fmaxf(2.f * f * (1.f - f), 1e-6f));
+            const uint64_t h = syn_hash3(seed, (uint64_t)s, 0);
+#pragma unroll
+            for (int r = 0; r < 32; ++r)
+                if (r < R) acc[r] += ((h >> r) & 1u) ? z : -z;
+        }
+    }
+    const float scale = rsqrtf((float)S);
+    for (int r = 0; r < R; ++r) {
+        float v = acc[r];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) sh[(threadIdx.x >> 5) * R + r] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < R) {
+        float v = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[w * R + threadIdx.x];
+        proj[(size_t)i * R + threadIdx.x] = v * scale;
+    }
+}
+
+} // namespace
+
+extern "C" int admix_sketch(const uint8_t *d_bed, int64_t pitch, int64_t I, const int32_t *d_snps, int32_t S,
+                            int32_t R, uint64_t seed, float *d_freq, int8_t *d_dos, float *d_proj, void *stream)
+{
+    if (!d_bed || !d_snps || !d_freq || !d_dos || !d_proj || I < 1 || S < 1 || R < 0 || R > 32 || pitch < (I + 3) / 4)
+        return ADMIX_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_sketch_freq<<<S, 256, 0, st>>>(d_bed, pitch, I, d_snps, d_freq);
+    k_sketch<<<(unsigned)I, 256, sizeof(float) * 8 * (R > 0 ? R : 1), st>>>(d_bed, pitch, I, d_snps, S, d_freq, R,
+                                                                            seed, d_dos, d_proj);
+    return cudaGetLastError() == cudaSuccess ? ADMIX_OK : ADMIX_ERR_CUDA;
+}
+
+namespace {
+
+/* ---- operand loaders: element (r, c) of a logical row-major matrix ---- */
+struct LoadF {                     /* dense FP32 with arbitrary strides (transposes are strides) */
+    const float *p; int64_t sr, sc;
+    __device__ float operator()(int64_t r, int64_t c) const { return p[r * sr + c * sc]; }
+};
+struct LoadX {                     /* network input: [dosage - 2f (0 if missing) | projections] */
+    const int8_t *dos; const float *center; const float *proj; int S, R;
+    __device__ float operator()(int64_t m, int64_t k) const
+    {
+        if (k < S) {
+            const int8_t d = dos[m * S + k];
+            return d == 3 ? 0.f : (float)d - center[k];
+        }
+        return proj[m * R + (k - S)];
+    }
+};
+struct LoadXT {                    /* the input transposed: (k, m) */
+    LoadX x;
+    __device__ float operator()(int64_t k, int64_t m) const { return x(m, k); }
+};
+
+constexpr int GB_M = 64, GB_N = 64, GB_K = 16;
+
+/* C[m, n] = alpha * sum_k A(m, k) B(k, n) (+ bias[n]); relu if act; times [mask(m, n) > 0] if mask.
+ * 256 threads, 64 x 64 tile, 4 x 4 outputs per thread, FP32 accumulation. */
+template <class LA, class LB>
+__global__ void __launch_bounds__(256)
+k_gemm(LA A, LB B, int64_t M, int64_t N, int64_t Kd, float alpha, const float *__restrict__ bias, int act,
+       const float *__restrict__ mask, float *__restrict__ C, int64_t ldc)
+{
+    __shared__ float As[GB_K][GB_M + 4];
+    __shared__ float Bs[GB_K][GB_N + 4];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int64_t m0 = (int64_t)blockIdx.y * GB_M, n0 = (int64_t)blockIdx.x * GB_N;
+    float acc[4][4] = {};
+    for (int64_t k0 = 0; k0 < Kd; k0 += GB_K) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = tid + u * 256;              /* 1024 elements of each 64 x 16 tile */
+            const int am = e >> 4, ak = e & 15;
+            const int64_t gm = m0 + am, gk = k0 + ak;
+            As[ak][am] = (gm < M && gk < Kd) ? A(gm, gk) : 0.f;
+            const int bk = e >> 6, bn = e & 63;
+            const int64_t gk2 = k0 + bk, gn = n0 + bn;
+            Bs[bk][bn] = (gk2 < Kd && gn < N) ? B(gk2, gn) : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GB_K; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) { a[r] = As[kk][ty * 4 + r]; b[r] = Bs[kk][tx * 4 + r]; }
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int64_t m = m0 + ty * 4 + r;
+        if (m >= M) continue;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int64_t n = n0 + tx * 4 + c;
+            if (n >= N) continue;
+            float v = alpha * acc[r][c] + (bias ? bias[n] : 0.f);
+            if (act) v = fmaxf(v, 0.f);
+            if (mask && !(mask[m * ldc + n] > 0.f)) v = 0.f;
+            C[m * ldc + n] = v;
+        }
+    }
+}
+
+template <class LA, class LB>
+cudaError_t gemm(LA A, LB B, int64_t M, int64_t N, int64_t Kd, float alpha, const float *bias, int act,
+                 const float *mask, float *C, int64_t ldc, cudaStream_t st)
+{
+    dim3 grid((unsigned)((N + GB_N - 1) / GB_N), (unsigned)((M + GB_M - 1) / GB_M));
+    k_gemm<LA, LB><<<grid, 256, 0, st>>>(A, B, M, N, Kd, alpha, bias, act, mask, C, ldc);
+    return cudaGetLastError();
+}
+
+/* row softmax of logits (n x K) into probs; with targets: dlogits = (probs - target) / n and the
+ * summed cross-entropy added (atomically) into *loss */
+__global__ void k_softmax_ce(const float *__restrict__ logits, int64_t n, int K, float *__restrict__ probs,
+                             const float *__restrict__ target, float *__restrict__ dlogits, float *__restrict__ loss)
+{
+    const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    const float *z = logits + m * K;
+    float mx = z[0];
+    for (int k = 1; k < K; ++k) mx = fmaxf(mx, z[k]);
+    float s = 0.f;
+    for (int k = 0; k < K; ++k) s += expf(z[k] - mx);
+    const float ls = logf(s);
+    float l = 0.f;
+    for (int k = 0; k < K; ++k) {
+        const float pk = expf(z[k] - mx - ls);
+        probs[m * K + k] = pk;
+        if (target) {
+            dlogits[m * K + k] = (pk - target[m * K + k]) / (float)n;
+            l -= target[m * K + k] * (z[k] - mx - ls);
+        }
+    }
+    if (target && loss) atomicAdd(loss, l);
+}
+
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m1,
+                       float *__restrict__ m2, int64_t n, float lr, float b1, float b2, float eps, float c1, float c2)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const float gt = g[t];
+        const float a = b1 * m1[t] + (1.f - b1) * gt, b = b2 * m2[t] + (1.f - b2) * gt * gt;
+        m1[t] = a; m2[t] = b;
+        w[t] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+    }
+}
+
+} // namespace
+
+namespace {
+
+__global__ void k_colsum_atomic(const float *__restrict__ dY, int64_t M, int64_t N, float *__restrict__ db)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int64_t rows = (M + gridDim.y - 1) / gridDim.y;
+    const int64_t m0 = (int64_t)blockIdx.y * rows, m1 = min(M, m0 + rows);
+    float s = 0.f;
+    for (int64_t m = m0; m < m1; ++m) s += dY[m * N + n];
+    atomicAdd(db + n, s);
+}
+
+cudaError_t colsum(const float *dY, int64_t M, int64_t N, float *db, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(db, 0, sizeof(float) * N, st);
+    if (e != cudaSuccess) return e;
+    const unsigned gy = (unsigned)std::min<int64_t>(64, std::max<int64_t>(1, M / 256));
+    k_colsum_atomic<<<dim3((unsigned)((N + 127) / 128), gy), 128, 0, st>>>(dY, M, N, db);
+    return cudaGetLastError();
+}
+
+/* closed-form P step from Q: p_kj = sum_i nm q_ki g_ij / (2 sum_i nm q_ki), clamped to
+ * [1e-5, 1-1e-5] like project_p! (projections.jl:69-74).  Thread = SNP, q staged 64 at a time. */
+template <int K>
+__global__ void __launch_bounds__(128)
+k_warm_p(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, int64_t J, const double *__restrict__ q,
+         double *__restrict__ p)
+{
+    __shared__ float qs[64 * K];
+    const int64_t j = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    float num[K], den[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) { num[k] = 0.f; den[k] = 0.f; }
+    for (int64_t i0 = 0; i0 < I; i0 += 64) {
+        const int n = (int)min((int64_t)64, I - i0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < n * K; t += 128) qs[t] = (float)q[(size_t)K * i0 + t];
+        __syncthreads();
+        if (j < J) {
+            for (int ii = 0; ii < n; ++ii) {
+                const int64_t i = i0 + ii;
+                const int c = (bed[(size_t)j * pitch + (i >> 2)] >> ((i & 3) << 1)) & 3;
+                if (c == 1) continue;
+                const float g = c == 0 ? 0.f : (float)(c - 1);
+#pragma unroll
+                for (int k = 0; k < K; ++k) { num[k] = fmaf(qs[ii * K + k], g, num[k]); den[k] += 2.f * qs[ii * K + k]; }
+            }
+        }
+    }
+    if (j < J)
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double v = den[k] > 0.f ? (double)num[k] / (double)den[k] : 0.5;
+            p[(size_t)K * j + k] = fmin(fmax(v, 1e-5), 1.0 - 1e-5);
+        }
+}
+
+} // namespace
+
+extern "C" {
+
+int admix_mlp_forward(const admix_mlp *net, int64_t n, const int8_t *dos, const float *center, const float *proj,
+                      float *h1, float *h2, float *logits, float *probs, void *stream)
+{
+    if (!net || n < 1 || !dos || !center || !proj || !h1 || !h2 || !logits || !probs) return ADMIX_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t D = net->S + net->R, H = net->H, K = net->K;
+    cudaError_t e = gemm(LoadX{dos, center, proj, net->S, net->R}, LoadF{net->w1, H, 1}, n, H, D, 1.f, net->b1, 1,
+                         nullptr, h1, H, st);
+    if (e == cudaSuccess) e = gemm(LoadF{h1, H, 1}, LoadF{net->w2, H, 1}, n, H, H, 1.f, net->b2, 1, nullptr, h2, H, st);
+    if (e == cudaSuccess) e = gemm(LoadF{h2, H, 1}, LoadF{net->w3, K, 1}, n, K, H, 1.f, net->b3, 0, nullptr, logits, K, st);
+    if (e == cudaSuccess) {
+        k_softmax_ce<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(logits, n, (int)K, probs, nullptr, nullptr, nullptr);
+        e = cudaGetLastError();
+    }
+    return e == cudaSuccess ? ADMIX_OK : ADMIX_ERR_CUDA;
+}
+
+int admix_mlp_backward(const admix_mlp *net, const admix_mlp_grads *grad, int64_t n, const int8_t *dos,
+                       const float *center, const float *proj, const float *h1, const float *h2, const float *logits,
+                       const float *target, float *probs, float *dlogits, float *dh2, float *dh1, float *loss,
+                       void *stream)
+{
+    if (!net || !grad || n < 1 || !target || !dlogits || !dh2 || !dh1) return ADMIX_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t D = net->S + net->R, H = net->H, K = net->K;
+    k_softmax_ce<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(logits, n, (int)K, probs, target, dlogits, loss);
+    cudaError_t e = cudaGetLastError();
+    /* layer 3 */
+    if (e == cudaSuccess) e = gemm(LoadF{h2, 1, H}, LoadF{dlogits, K, 1}, H, K, n, 1.f, nullptr, 0, nullptr, grad->w3, K, st);
+    if (e == cudaSuccess) e = colsum(dlogits, n, K, grad->b3, st);
+    if (e == cudaSuccess) e = gemm(LoadF{dlogits, K, 1}, LoadF{net->w3, 1, K}, n, H, K, 1.f, nullptr, 0, h2, dh2, H, st);
+    /* layer 2 */
+    if (e == cudaSuccess) e = gemm(LoadF{h1, 1, H}, LoadF{dh2, H, 1}, H, H, n, 1.f, nullptr, 0, nullptr, grad->w2, H, st);
+    if (e == cudaSuccess) e = colsum(dh2, n, H, grad->b2, st);
+    if (e == cudaSuccess) e = gemm(LoadF{dh2, H, 1}, LoadF{net->w2, 1, H}, n, H, H, 1.f, nullptr, 0, h1, dh1, H, st);
+    /* layer 1 */
+    if (e == cudaSuccess)
+        e = gemm(LoadXT{LoadX{dos, center, proj, net->S, net->R}}, LoadF{dh1, H, 1}, D, H, n, 1.f, nullptr, 0, nullptr,
+                 grad->w1, H, st);
+    if (e == cudaSuccess) e = colsum(dh1, n, H, grad->b1, st);
+    return e == cudaSuccess ? ADMIX_OK : ADMIX_ERR_CUDA;
+}
+
+int admix_mlp_adam(float *w, const float *g, float *m, float *v, int64_t n, float lr, float beta1, float beta2,
+                   float eps, int32_t t, void *stream)
+{
+    if (!w || !g || !m || !v || n < 1 || t < 1) return ADMIX_ERR_ARG;
+    const float c1 = 1.f - powf(beta1, (float)t), c2 = 1.f - powf(beta2, (float)t);
+    const unsigned grid = (unsigned)std::min<int64_t>(4096, (n + 255) / 256);
+    k_adam<<<grid, 256, 0, (cudaStream_t)stream>>>(w, g, m, v, n, lr, beta1, beta2, eps, c1, c2);
+    return cudaGetLastError() == cudaSuccess ? ADMIX_OK : ADMIX_ERR_CUDA;
+}
+
+int admix_warm_p(const uint8_t *d_bed, int64_t pitch, int64_t I, int64_t J, int32_t K, const double *d_q,
+                 double *d_p, void *stream)
+{
+    if (!d_bed || !d_q || !d_p || I < 1 || J < 1 || K < 1 || K > ADMIX_MAX_K || pitch < (I + 3) / 4)
+        return ADMIX_ERR_ARG;
+    cudaError_t e = cudaErrorInvalidValue;
+    ADMIX_DISPATCH_K(K, (k_warm_p<KK><<<(unsigned)((J + 127) / 128), 128, 0, (cudaStream_t)stream>>>(d_bed, pitch, I, J,
+                                                                                                  d_q, d_p),
+                         e = cudaGetLastError()));
+    return e == cudaSuccess ? ADMIX_OK : ADMIX_ERR_CUDA;
+}
+
+} /* extern "C" */

@@ -105,9 +105,9 @@ __device__ __forceinline__ void qchunk_load(QChunk<K> &cr, const uint8_t *__rest
     }
 #pragma unroll
     for (int u = 0; u < MQ<K>::PREF_P; ++u) {
-        const int t = tid + u * MQ_THREADS;          /* t = k * JC + jj: shared stores hit distinct banks */
-        const int k = t / MQ_JC, jj = t - k * MQ_JC;
-        cr.pv[u] = (t < K * MQ_JC && jj < n) ? p[(size_t)K * (jc + jj) + k] : 0.5;
+        const int t = tid + u * MQ_THREADS;          /* t = jj * K + k: coalesced loads; the padded */
+        const int jj = t / K;                        /* row stride keeps the stores <= 2-way conflicted */
+        cr.pv[u] = (t < K * MQ_JC && jj < n) ? p[(size_t)K * jc + t] : 0.5;
     }
 }
 
@@ -123,7 +123,7 @@ __device__ __forceinline__ void qchunk_store(const QChunk<K> &cr, float *Pb, uin
     for (int u = 0; u < MQ<K>::PREF_P; ++u) {
         const int t = tid + u * MQ_THREADS;
         if (t < K * MQ_JC) {
-            const int k = t / MQ_JC, jj = t - k * MQ_JC;
+            const int jj = t / K, k = t - jj * K;
             Pb[k * MQ<K>::PS + jj] = (float)cr.pv[u];
             Pb[K * MQ<K>::PS + k * MQ<K>::PS + jj] = (float)(1.0 - cr.pv[u]);
         }
@@ -389,9 +389,9 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     auto qload = [&](int64_t ic) {
 #pragma unroll
         for (int u = 0; u < C::PREF_Q; ++u) {
-            const int t = tid + u * MP_THREADS;              /* t = k * IC + ii */
-            const int k = t / MP_IC, ii = t - k * MP_IC;
-            qr[u] = (t < K * MP_IC && ic + ii < ib) ? q[(size_t)K * (ic + ii) + k] : 1.0 / K;
+            const int t = tid + u * MP_THREADS;              /* t = ii * K + k: coalesced */
+            const int ii = t / K;
+            qr[u] = (t < K * MP_IC && ic + ii < ib) ? q[(size_t)K * ic + t] : 1.0 / K;
         }
     };
     auto qstore = [&](float *Qb) {
@@ -399,7 +399,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         for (int u = 0; u < C::PREF_Q; ++u) {
             const int t = tid + u * MP_THREADS;
             if (t < K * MP_IC) {
-                const int k = t / MP_IC, ii = t - k * MP_IC;
+                const int ii = t / K, k = t - ii * K;
                 Qb[k * C::QS + ii] = (float)qr[u];
             }
         }

@@ -28,6 +28,8 @@ class CohortSpec:
     beta_a: float = 0.5
     miss: float = 0.01
     seed: int = 0
+    p_seed: int = -1               # seed of P; -1: the cohort seed.  Cohorts sharing a p_seed share
+                                   # their ancestral allele frequencies SNP by SNP (one "world").
 
     def scaled(self, I: int | None = None, J: int | None = None, K: int | None = None, **kw) -> "CohortSpec":
         return replace(self, I=I or self.I, J=J or self.J, K=K or self.K, **kw)
@@ -57,6 +59,12 @@ def truth(spec: CohortSpec) -> tuple[np.ndarray, np.ndarray]:
                                  spec.p_lo, spec.p_hi, spec.beta_a, spec.alpha, N.dptr(q), N.dptr(p))
     if rc != 0:
         raise ValueError(f"syn_truth failed for {spec}")
+    if spec.p_seed >= 0 and spec.p_seed != spec.seed:
+        q2 = np.empty((1, spec.K))
+        rc = N.synth_lib().syn_truth(1, spec.J, spec.K, spec.p_seed, 0 if spec.p_dist == "uniform" else 1,
+                                     spec.p_lo, spec.p_hi, spec.beta_a, spec.alpha, N.dptr(q2), N.dptr(p))
+        if rc != 0:
+            raise ValueError(f"syn_truth failed for {spec}")
     return q, p
 
 
