@@ -327,24 +327,40 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
                   admix_rtol: float = 1e-7, admix_n_em_iters: int = 5, T=np.float64, Q: int = 3,
                   use_gpu: bool = True, verbose: bool = False, progress_bar: bool = False,
                   fix_q: bool = False, fix_p: bool = False, init_q=None, init_p=None,
-                  quiet: bool = False, flags: int = 0):
+                  quiet: bool = False, flags: int = 0, warm_start=None):
     """run_admixture(filename, K; ...) (driver.jl:35-75) -> (d, clusters, aims).
 
-    ``filename`` is a .bed path or an in-memory Genotypes.  ``rng`` is an integer seed of this
-    engine's generator (the reference's Julia RNG streams are not reproduced).  SKFR
-    (sparsity) is not part of the likelihood engine and raises."""
+    ``filename`` is a .bed path, an in-memory Genotypes or a DeviceGenotypes.  ``rng`` is an
+    integer seed of this engine's generator (the reference's Julia RNG streams are not
+    reproduced).  SKFR (sparsity) is not part of the likelihood engine and raises.
+
+    init_q (K x I) / init_p (K x J): as in the reference, EM priming runs unless both are given
+    (driver.jl:180); a given one overwrites the primed value.  warm_start ("learned", a model
+    path or a WarmStartMLP) starts from the learned encoder's Q and the closed-form P instead
+    of the random start, with no EM; where no model applies it falls back to the random start +
+    EM.  Explicit init_q / init_p take precedence over the warm start."""
     if sparsity is not None:
         raise NotImplementedError("sparsity (SKFR AIM pre-selection) is outside the likelihood engine")
     if T not in (np.float64, float, "Float64"):
         raise NotImplementedError("only T = Float64 is on the device path")
     if not use_gpu:
         raise NotImplementedError("use_gpu=False is the reference's CPU path; this engine runs on the GPU")
-    g = filename if isinstance(filename, Genotypes) else read_bed(filename)
+    g = filename if isinstance(filename, (Genotypes, DeviceGenotypes)) else read_bed(filename)
     if not quiet:
         print(f"Loaded {g.I} samples and {g.J} SNPs")
     d = AdmixData(g.I, g.J, K, Q, rng=rng)
     d_cu, g_cu = _cu_admixture_base(d, g, g.I, g.J, flags=flags)
     try:
+        if warm_start is not None and (init_q is None or init_p is None):
+            from . import warmstart
+            start = warmstart.learned_start(g, K, None if warm_start == "learned" else warm_start)
+            if start is not None:
+                if not quiet:
+                    print("Starting from the learned warm start")
+                init_q = start[0].T if init_q is None else init_q
+                init_p = start[1].T if init_p is None else init_p
+            elif not quiet:
+                print(f"No warm-start model applies to K={K}, J={g.J}; random start + EM")
         if init_q is None or init_p is None:
             init_em(d, g, admix_n_em_iters, d_cu=d_cu, g_cu=g_cu, quiet=quiet)
         if init_q is not None:

@@ -35,6 +35,9 @@ class CohortSpec:
         return replace(self, I=I or self.I, J=J or self.J, K=K or self.K, **kw)
 
 
+# p_seed of the synthetic "world" (shared ancestral allele frequencies) of the warm-start models
+WARMSTART_WORLD = 777
+
 COHORTS = {
     # plain method, CPU-runnable
     "c1": CohortSpec("c1", 1_000, 10_000, 3, alpha=0.5, miss=0.01),
@@ -45,8 +48,9 @@ COHORTS = {
                      beta_a=0.5, miss=0.01),
     # batching form
     "c4": CohortSpec("c4", 20_000, 50_000, 6, alpha=0.3, miss=0.01),
-    # learned warm-start form (packed genotypes 25 GB)
-    "c5": CohortSpec("c5", 200_000, 500_000, 8, alpha=0.2, miss=0.01),
+    # learned warm-start form (packed genotypes 25 GB); drawn from the ancestral frequencies the
+    # shipped warm-start model was trained on (its training cohorts: I=20k, J=100k, seeds 1000-1049)
+    "c5": CohortSpec("c5", 200_000, 500_000, 8, alpha=0.2, miss=0.01, p_seed=WARMSTART_WORLD),
 }
 
 

@@ -56,6 +56,8 @@ def main():
 
     if args.model:
         model = ws.WarmStartMLP.load(args.model)
+        if model.snps is None:
+            model.snps = snps
     else:
         data, t_solve = [], time.perf_counter()
         for c in range(args.cohorts):
@@ -71,7 +73,7 @@ def main():
             log(f"cohort {c}: plain solve {r['iterations']} iterations, {r['seconds']:.1f} s, ll {r['ll']:.6e}")
             del g
         report["solve_seconds"] = time.perf_counter() - t_solve
-        model = ws.WarmStartMLP(len(snps), 32, args.K, seed=0)
+        model = ws.WarmStartMLP(len(snps), 32, args.K, seed=0, snps=snps)
         t_train = time.perf_counter()
         hist = ws.train(model, data, epochs=args.epochs, log=log)
         report["train_seconds"] = time.perf_counter() - t_train
@@ -98,7 +100,7 @@ def main():
     rand = ws.run_to_target(g, spec.K, flags=oa.ADMIX_FLAG_MIXED, rng=1, target=target, max_iter=args.max_iter)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    start = ws.predict_start(model, g, snps)
+    start = ws.predict_start(model, g)
     t_pred = time.perf_counter() - t0
     learned = ws.run_to_target(g, spec.K, flags=oa.ADMIX_FLAG_MIXED, rng=1, start=start, target=target,
                                max_iter=args.max_iter)

@@ -18,10 +18,11 @@ import numpy as np
 
 from . import _native as N
 from .bed import DeviceGenotypes, Genotypes
+from .synth import WARMSTART_WORLD
 
 MODEL_DIR = Path(__file__).resolve().parent / "models"
 # ancestral-frequency seed (CohortSpec.p_seed) of the cohorts the shipped models were trained on
-WORLD_SEED = 777
+WORLD_SEED = WARMSTART_WORLD
 
 
 def _torch():
@@ -78,9 +79,13 @@ class WarmStartMLP:
 
     NAMES = ("w1", "b1", "w2", "b2", "w3", "b3")
 
-    def __init__(self, S: int, R: int, K: int, H: int = 256, seed: int = 0, params: dict | None = None):
+    def __init__(self, S: int, R: int, K: int, H: int = 256, seed: int = 0, params: dict | None = None,
+                 snps: np.ndarray | None = None):
         torch = _torch()
         self.S, self.R, self.K, self.H = S, R, K, H
+        self.snps = None if snps is None else np.ascontiguousarray(snps, dtype=np.int32)
+        if self.snps is not None and len(self.snps) != S:
+            raise ValueError(f"{len(self.snps)} sketch SNPs for an input of S={S}")
         dev = torch.device("cuda", torch.cuda.current_device())
         if params is None:
             rng = np.random.default_rng(seed)
@@ -100,14 +105,16 @@ class WarmStartMLP:
 
     def save(self, path) -> None:
         """FP16 weights on disk (the deployed precision); the sketch definition alongside."""
-        np.savez_compressed(path, S=self.S, R=self.R, K=self.K, H=self.H,
+        extra = {} if self.snps is None else {"snps": np.ascontiguousarray(self.snps, dtype=np.int32)}
+        np.savez_compressed(path, S=self.S, R=self.R, K=self.K, H=self.H, **extra,
                             **{k: v.detach().cpu().numpy().astype(np.float16) for k, v in self.p.items()})
 
     @classmethod
     def load(cls, path) -> "WarmStartMLP":
         z = np.load(path)
         params = {k: z[k].astype(np.float32) for k in cls.NAMES}
-        return cls(int(z["S"]), int(z["R"]), int(z["K"]), int(z["H"]), params=params)
+        return cls(int(z["S"]), int(z["R"]), int(z["K"]), int(z["H"]), params=params,
+                   snps=z["snps"] if "snps" in z.files else None)
 
     def forward(self, sk: Sketch, batch: int = 65536):
         """Class probabilities (n x K) of every individual of the sketch, as a device tensor."""
@@ -213,9 +220,14 @@ def warm_p(g, q: np.ndarray) -> np.ndarray:
     return dp.cpu().numpy()
 
 
-def predict_start(model: WarmStartMLP, g, snps: np.ndarray, R: int = 32, seed: int = 7):
-    """(q, p) starting point for run_admixture's init_q / init_p: Q from the encoder (rows
-    floored at the projection's pseudocount 1e-5 and renormalised), P from the closed-form step."""
+def predict_start(model: WarmStartMLP, g, snps: np.ndarray | None = None, R: int = 32, seed: int = 7):
+    """(q, p) starting point for run_admixture's init_q / init_p: Q (I, K) from the encoder (rows
+    floored at the projection's pseudocount 1e-5 and renormalised), P (J, K) from the closed-form
+    step.  snps defaults to the sketch stored with the model."""
+    if snps is None:
+        snps = model.snps
+    if snps is None:
+        raise ValueError("the model carries no sketch SNP list; pass snps")
     sk = sketch(g, snps, R, seed)
     q = model.forward(sk).cpu().numpy().astype(np.float64)
     q = np.maximum(q, 1e-5)
@@ -225,6 +237,25 @@ def predict_start(model: WarmStartMLP, g, snps: np.ndarray, R: int = 32, seed: i
 
 def default_model_path(K: int) -> Path:
     return MODEL_DIR / f"warmstart_k{K}.npz"
+
+
+def load_default(K: int) -> WarmStartMLP | None:
+    """The shipped model for K clusters, or None if there is none."""
+    path = default_model_path(K)
+    return WarmStartMLP.load(path) if path.exists() else None
+
+
+def learned_start(g, K: int, model=None):
+    """(q, p) from the learned encoder, or None when no model applies (none for K, or the cohort
+    has fewer SNPs than the sketch reaches): the caller then falls back to the random start + EM.
+    `model` is a WarmStartMLP, a path to one, or None for the shipped model of K."""
+    if model is None:
+        model = load_default(K)
+    elif not isinstance(model, WarmStartMLP):
+        model = WarmStartMLP.load(model)
+    if model is None or model.K != K or model.snps is None or int(model.snps.max()) >= g.J:
+        return None
+    return predict_start(model, g)
 
 
 def run_to_target(g, K: int, *, flags: int = 0, start=None, em: int = 5, rtol: float = 1e-7, target=None,

@@ -186,11 +186,27 @@ def test_committed_model_gain(oa, ws):
     spec = _world(oa, "held-out", 20_000, 100_000, 8, 4242, ws.WORLD_SEED)
     q, p = oa.truth(spec)
     g = oa.genotypes_device(spec, q, p)
-    snps = ws.sketch_snps(100_000, S=model.S)
+    assert np.array_equal(model.snps, ws.sketch_snps(100_000, S=model.S))
     plain = ws.run_to_target(g, 8, rng=1)
     target = plain["ll"] - 1e-6 * abs(plain["ll"])
     rand = ws.run_to_target(g, 8, flags=oa.ADMIX_FLAG_MIXED, rng=1, target=target)
-    learned = ws.run_to_target(g, 8, flags=oa.ADMIX_FLAG_MIXED, rng=1, start=ws.predict_start(model, g, snps),
+    learned = ws.run_to_target(g, 8, flags=oa.ADMIX_FLAG_MIXED, rng=1, start=ws.predict_start(model, g),
                                target=target)
     assert learned["iterations_to_target"] is not None
     assert learned["iterations_to_target"] < rand["iterations_to_target"] + 5, (learned, rand)
+
+
+def test_run_admixture_warm_start_plumbing(oa, ws, tmp_path):
+    """run_admixture(warm_start=...) starts from the encoder's Q and the closed-form P with no EM;
+    with no model for K it falls back to the random start + EM and matches the plain run."""
+    g, _, _ = _cohort(oa, 1500, 2000, 3, 21)
+    m = _random_model(ws, 256, 32, 3, 64, seed=3)
+    m.snps = ws.sketch_snps(2000, S=256, seed=2)
+    m.save(tmp_path / "m3.npz")
+    d, _, _ = oa.run_admixture(g, 3, rng=4, warm_start=tmp_path / "m3.npz", quiet=True, admix_n_iter=200)
+    assert np.allclose(d.q.sum(0), 1.0) and np.all(d.p >= 1e-5 - 1e-15)
+    assert np.isfinite(d.ll_new)
+    # fallback (no shipped K=3 model): identical to the plain call
+    d0, _, _ = oa.run_admixture(g, 3, rng=4, quiet=True, admix_n_iter=200)
+    d1, _, _ = oa.run_admixture(g, 3, rng=4, warm_start="learned", quiet=True, admix_n_iter=200)
+    assert np.array_equal(d0.x, d1.x) and d0.ll_new == d1.ll_new
