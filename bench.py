@@ -486,6 +486,149 @@ def C_byref(x):
     return ctypes.byref(x)
 
 
+BATCH_RESTARTS, BATCH_KS = 64, tuple(range(2, 13))
+
+
+def run_batch(args, rank, world, local_rank):
+    """The batching configuration: one batch of 64 random restarts at K=6 plus a K sweep
+    K=2..12 over one cohort (I=20000, J=50000), advanced together -- one graph launch per batch
+    iteration, work split chosen by the autotuner.  A step is one batch iteration (every member
+    one admixture_qn! iteration); value = sum over members of I*J*K^2 per second.  Beside it:
+    the same members' solo iterations one after another (the reference's one-run-per-call
+    usage), and time to converge of the whole batch from the random starts + 5 EM."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import openadmixture_b200 as oa
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    spec = oa.COHORTS[args.config].scaled(seed=rank)
+    qt, pt = oa.truth(spec)
+    g = oa.genotypes_device(spec, qt, pt)
+    Ks = [spec.K] * BATCH_RESTARTS + list(BATCH_KS)
+    seeds = list(range(BATCH_RESTARTS)) + [0] * len(BATCH_KS)
+    flags = oa.ADMIX_FLAG_MIXED if args.form == "mixed" else 0
+    work = sum(spec.I * spec.J * K * K for K in Ks)
+    b = oa.AdmixBatch(g, Ks, flags=flags, seeds=seeds)
+    t0 = time.perf_counter()
+    divisor, probe_ms = b.autotune()
+    t_tune = time.perf_counter() - t0
+    b.init_em(5)
+    b.run_qn(args.warmup, 0.0)                         # rtol 0: no member leaves
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    rec = b.run_qn(args.steps, 0.0)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t = torch.tensor([rec["ms_device"]], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = world * work * args.steps / (ms / 1e3)
+
+    # end to end through the public API: every member's q, p from pinned host memory, one batch
+    # iteration, every member's q, p back (all calls synchronous; wall clock)
+    hx = [torch.from_numpy(np.ascontiguousarray(b.x(m))).pin_memory() for m in range(len(Ks))]
+    ho = [torch.empty_like(x).pin_memory() for x in hx]
+    e2e_steps = max(2, args.steps // 3)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for m, mem in enumerate(b.members):
+            mem.upload(oa.X, hx[m].numpy())
+        b.run_qn(1, 0.0)
+        for m, mem in enumerate(b.members):
+            mem.download(oa.X, ho[m].numpy())
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - w0) * 1e3 / e2e_steps
+    xbytes = sum(8 * K * (spec.I + spec.J) for K in Ks)
+
+    # solo iterations of each distinct K, one problem at a time
+    solo_ms = {}
+    for K in sorted(set(Ks)):
+        d = oa.AdmixData(spec.I, spec.J, K, 3, rng=0)
+        with oa.CuAdmixData(d, g, flags=flags) as h:
+            oa.init_em(d, g, 2, d_cu=h, quiet=True)
+            h.set_ll(d.ll_new)
+            from openadmixture_b200 import _native as N
+            info = N.IterInfo()
+            h._chk(N.admix_lib().admix_qn_iteration(h.handle, 1, C_byref(info)))
+            st = torch.cuda.ExternalStream(h.stream())
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True); a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(st)
+            for it in range(2, 5):
+                h._chk(N.admix_lib().admix_qn_iteration(h.handle, it, C_byref(info)))
+            a1.record(st)
+            torch.cuda.synchronize()
+            solo_ms[K] = a0.elapsed_time(a1) / 3
+    seq_ms = sum(solo_ms[K] for K in Ks)
+
+    # time to converge of the whole batch from the random starts + 5 EM
+    ttc = None
+    if not args.no_ttc:
+        for m, mem in enumerate(b.members):
+            mem.upload(oa.X, oa.init_x(spec.I, spec.J, Ks[m], seeds[m]))
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        b.init_em(5)
+        r = b.run_qn(1000, 1e-7)
+        torch.cuda.synchronize()
+        lls = np.array([mem.loglik(oa.X) for mem in b.members])
+        best = int(np.argmax(lls[:BATCH_RESTARTS]))
+        ttc = {"seconds": time.perf_counter() - w0, "members": len(Ks), "all_converged": bool(r["converged"].all()),
+               "iterations_max": int(r["iterations"].max()), "iterations_mean": float(r["iterations"].mean()),
+               "qn_device_ms": r["ms_device"], "best_restart": best, "best_restart_ll_fp64": float(lls[best]),
+               "k_sweep_ll_fp64": {int(K): float(lls[BATCH_RESTARTS + t]) for t, K in enumerate(BATCH_KS)}}
+    n_kern = sum(mem.iteration_kernels() for mem in b.members)
+    b.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(oa, spec)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    hbm, _, peak_kind = _peaks()
+    Ib = (spec.I + 3) // 4
+    alg = len(Ks) * 6 * Ib * spec.J                  # 6 genotype passes per member iteration
+    achieved = alg / (ms / args.steps / 1e3) / 1e9
+    line = {
+        "metric": "genotype*K^2/s per batch iteration (64 restarts at K=6 + K sweep 2..12, one launch), 1 B200",
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16+f32+f64" if flags else "f64", "data": "synthetic",
+        "config": {"workload": f"{spec.name}: batch of {len(Ks)} problems on I={spec.I} J={spec.J}: "
+                               f"{BATCH_RESTARTS} restarts at K={spec.K} and K={BATCH_KS[0]}..{BATCH_KS[-1]}",
+                   "I": spec.I, "J": spec.J, "members": len(Ks), "form": args.form,
+                   "l2": f"inputs larger than L2: {Ib * spec.J / 1e6:.0f} MB packed genotypes, "
+                         f"{len(Ks)} members' iterates",
+                   "autotune": {"divisor": divisor, "probe_ms": probe_ms, "seconds": t_tune}},
+        "e2e": {"value": world * work / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": xbytes,
+                "d2h_bytes_per_step": xbytes, "ms_per_step": e2e_ms,
+                "path": "admix_set_x per member + admix_batch_run_qn(1) + admix_get_x per member"},
+        "gpu_launches": n_kern * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "batch iteration (all members)", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+                     "alg_bytes_per_launch": alg,
+                     "note": "packed-genotype bytes the members' passes stream per batch iteration"},
+        "vs_sequential": {"solo_ms_per_iteration": solo_ms, "sequential_ms_per_step": seq_ms,
+                          "speedup_per_iteration": seq_ms / (ms / args.steps)},
+        "ttc": ttc,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = _args()
     rank = int(os.environ.get("RANK", "0"))
@@ -495,6 +638,8 @@ def main():
         return run_reference(args, rank, world)
     if args.pass_only:
         return run_pass_only(args)
+    if args.config == "c4":
+        return run_batch(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -218,6 +218,41 @@ int admix_mlp_adam(float *w, const float *g, float *m, float *v, int64_t n, floa
 int admix_warm_p(const uint8_t *d_bed, int64_t pitch, int64_t I, int64_t J, int32_t K, const double *d_q,
                  double *d_p, void *stream);
 
+/* --- batching: random restarts and K sweeps over one cohort ----------------------------
+ * The reference runs one problem per run_admixture call (driver.jl:35-75); a user who wants
+ * several restarts or several K calls it once per seed / K.  A batch holds n member problems
+ * (member m has K = Ks[m]; repeat a K for restarts) over ONE device copy of the genotypes.
+ * Each member is an ordinary handle (admix_batch_member) for set_x / get_x / loglik / ...;
+ * the batch calls below advance all members together: one batch iteration is one CUDA graph
+ * launch whose independent branches are the members' captured admixture_qn! iterations, so the
+ * members' kernels run concurrently.  Members that converge drop out of later launches. */
+typedef struct admix_batch admix_batch;
+
+int admix_batch_create(int64_t I, int64_t J, const uint8_t *bed, int32_t n, const int32_t *Ks, int32_t Q,
+                       uint32_t flags, admix_batch **out);
+/* as admix_batch_create, genotypes already on the current device at src_pitch bytes per column */
+int admix_batch_create_device(int64_t I, int64_t J, const uint8_t *d_bed, int64_t src_pitch, int32_t n,
+                              const int32_t *Ks, int32_t Q, uint32_t flags, admix_batch **out);
+int admix_batch_destroy(admix_batch *b);
+const char *admix_batch_last_error(const admix_batch *b);
+int admix_batch_size(const admix_batch *b, int32_t *n);
+/* borrowed handle of member m (owned by the batch; do not destroy it) */
+int admix_batch_member(admix_batch *b, int32_t m, admix_ctx **h);
+/* init_em! (algorithms_outer.jl:12-45) on every member, concurrently; ll_hist: n x iters or NULL */
+int admix_batch_init_em(admix_batch *b, int32_t iters, double *ll_hist);
+/* Work split of the members' passes: every member's sweep and log-likelihood plans are sized
+ * as if it had the GPU's SM count divided by `divisor` to itself (1 = the single-problem plans). */
+int admix_batch_set_split(admix_batch *b, int32_t divisor);
+/* Autotuner: times one concurrent launch of every member's Q sweep, P sweep and log-likelihood
+ * pass (read-only on the iterates) for divisor = 1, 2, 4, ... up to 4n, keeps the fastest and
+ * applies it.  Outputs the chosen divisor and its milliseconds (either may be NULL). */
+int admix_batch_autotune(admix_batch *b, int32_t *divisor, double *ms);
+/* admixture_qn! on every member until it converges (reldiff < rtol) or n_iter iterations:
+ * per member (arrays of length n, any may be NULL) the iterations run, whether it converged and
+ * its last iteration record; ms_device = summed device time of the batch launches. */
+int admix_batch_run_qn(admix_batch *b, int32_t n_iter, double rtol, int32_t *n_done, int32_t *converged,
+                       admix_iterinfo *last, double *ms_device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,7 @@ from .admixture import (AdmixData, CuAdmixData, X, X_NEXT, X_NEXT2, X_TMP, _cu_a
 from .bed import BedFormatError, DeviceGenotypes, Genotypes, read_bed, write_bed
 from .synth import COHORTS, CohortSpec, genotypes, genotypes_device, init_x, make_cohort, truth
 from . import warmstart
+from .batch import AdmixBatch, BatchMember, k_sweep, run_restarts
 
 __all__ = [
     "AdmixData", "CuAdmixData", "AdmixError", "IterInfo", "Genotypes", "DeviceGenotypes", "BedFormatError",
@@ -20,5 +21,5 @@ __all__ = [
     "_cu_admixture_base", "admixture_qn", "em_p", "em_q", "init_em", "loglikelihood",
     "run_admixture", "update_p", "update_q", "read_bed", "write_bed",
     "COHORTS", "CohortSpec", "genotypes", "genotypes_device", "init_x", "make_cohort", "truth",
-    "warmstart",
+    "warmstart", "AdmixBatch", "BatchMember", "k_sweep", "run_restarts",
 ]

@@ -101,6 +101,18 @@ ADMIX_SIGNATURES = {
                                  C.c_int32, _P]),
     "admix_warm_p": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int32, _P, _P, _P]),
     "admix_noalloc_last_error": (C.c_char_p, []),
+    "admix_batch_create": (C.c_int, [C.c_int64, C.c_int64, _U8, C.c_int32, _I32, C.c_int32, C.c_uint32,
+                                     C.POINTER(_P)]),
+    "admix_batch_create_device": (C.c_int, [C.c_int64, C.c_int64, _P, C.c_int64, C.c_int32, _I32, C.c_int32,
+                                            C.c_uint32, C.POINTER(_P)]),
+    "admix_batch_destroy": (C.c_int, [_P]),
+    "admix_batch_last_error": (C.c_char_p, [_P]),
+    "admix_batch_size": (C.c_int, [_P, _I32]),
+    "admix_batch_member": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
+    "admix_batch_init_em": (C.c_int, [_P, C.c_int32, _D]),
+    "admix_batch_set_split": (C.c_int, [_P, C.c_int32]),
+    "admix_batch_autotune": (C.c_int, [_P, _I32, _D]),
+    "admix_batch_run_qn": (C.c_int, [_P, C.c_int32, C.c_double, _I32, _I32, C.POINTER(IterInfo), _D]),
 }
 
 SYNTH_SIGNATURES = {

@@ -27,6 +27,7 @@ struct admix_ctx {
     int dev = 0, sms = 148;
     cudaStream_t st = nullptr;
     uint8_t *bed = nullptr;
+    bool owns_bed = true;            /* false for batch members: the batch owns the genotypes */
     double *xbuf = nullptr;          /* 4 * K(I+J): x, x_next, x_next2, x_tmp */
     double *x[4] = {nullptr, nullptr, nullptr, nullptr};
     double *parts_q = nullptr, *parts_p = nullptr;
@@ -42,6 +43,7 @@ struct admix_ctx {
     QNPlan qnp;
     size_t bytes = 0;
     cudaGraphExec_t iter_graph = nullptr;
+    cudaGraph_t iter_graph_def = nullptr;   /* the captured iteration (a batch embeds it) */
     char err[512] = {0};
 };
 
@@ -106,7 +108,9 @@ static void release(admix_ctx *h)
 {
     if (!h) return;
     if (h->iter_graph) cudaGraphExecDestroy(h->iter_graph);
-    void *dps[] = {h->bed, h->xbuf, h->parts_q, h->parts_p, h->U, h->V, h->vt, h->status_q,
+    if (h->iter_graph_def) cudaGraphDestroy(h->iter_graph_def);
+    if (h->bed && h->owns_bed) cudaFree(h->bed);
+    void *dps[] = {h->xbuf, h->parts_q, h->parts_p, h->U, h->V, h->vt, h->status_q,
                    h->status_p, h->ll_partial, h->qn_partial, h->sc, h->counts};
     for (void *p : dps)
         if (p) cudaFree(p);
@@ -121,8 +125,23 @@ const char *admix_last_error(const admix_ctx *h) { return h ? h->err : g_err; }
 
 /* Shared by admix_create (host genotypes) and admix_create_device (device genotypes at
  * src_pitch bytes per column). */
+/* Copy packed genotypes (Ib bytes per column at src_pitch) into dst at a 16-byte column pitch,
+ * padding bytes and the padding bits of each column's last byte set to the missing code 01
+ * (never read by the reference's loops). */
+static cudaError_t upload_genotypes(uint8_t *dst, int64_t pitch, const uint8_t *src, int64_t src_pitch, int64_t I,
+                                    int64_t J, bool on_device, int sms, cudaStream_t st)
+{
+    const int64_t Ib = (I + 3) / 4;
+    cudaError_t e = cudaMemsetAsync(dst, 0x55, (size_t)pitch * J + 64, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(dst, (size_t)pitch, src, (size_t)src_pitch, (size_t)Ib, (size_t)J,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_mask_tail(dst, I, J, pitch, sms, st);
+    return e;
+}
+
 static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed, bool on_device,
-                         int64_t src_pitch, uint32_t flags, admix_ctx **out)
+                         int64_t src_pitch, uint32_t flags, admix_ctx **out, uint8_t *shared_bed = nullptr)
 {
     if (!out) return fail(nullptr, ADMIX_ERR_ARG, "out is NULL");
     *out = nullptr;
@@ -161,7 +180,12 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     h->llm = plan_loglik_mixed(I, J, h->sms);
     h->qnp = plan_qn(nx, h->sms);
 
-    TRY(dalloc(h, &h->bed, (size_t)h->pitch * J + 64));
+    if (shared_bed) {
+        h->bed = shared_bed;
+        h->owns_bed = false;
+    } else {
+        TRY(dalloc(h, &h->bed, (size_t)h->pitch * J + 64));
+    }
     TRY(dalloc(h, &h->xbuf, (size_t)4 * nx));
     for (int w = 0; w < 4; ++w) h->x[w] = h->xbuf + (size_t)w * nx;
     TRY(dalloc(h, &h->parts_q, (size_t)std::max(h->sq.S, (flags & ADMIX_FLAG_MIXED) ? h->sqm.S : 1) * I * E));
@@ -178,12 +202,7 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     TRYC(cudaMallocHost((void **)&h->sc_host, sizeof(DevScalars)));
     TRYC(cudaMallocHost((void **)&h->iter_host, sizeof(int32_t)));
 
-    /* genotypes in HBM: columns at a 16-byte pitch, padding bytes and the padding bits of each
-     * column's last byte set to the missing code 01 (never read by the reference's loops) */
-    TRYC(cudaMemsetAsync(h->bed, 0x55, (size_t)h->pitch * J + 64, h->st));
-    TRYC(cudaMemcpy2DAsync(h->bed, (size_t)h->pitch, bed, (size_t)src_pitch, (size_t)h->Ib, (size_t)J,
-                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->st));
-    TRYC(launch_mask_tail(h->bed, I, J, h->pitch, h->sms, h->st));
+    if (!shared_bed) TRYC(upload_genotypes(h->bed, h->pitch, bed, src_pitch, I, J, on_device, h->sms, h->st));
     TRYC(cudaMemsetAsync(h->xbuf, 0, sizeof(double) * 4 * nx, h->st));
     TRYC(cudaMemsetAsync(h->U, 0, sizeof(double) * nx * Q, h->st));
     TRYC(cudaMemsetAsync(h->V, 0, sizeof(double) * nx * Q, h->st));
@@ -401,10 +420,9 @@ int admix_em_p(admix_ctx *h)
     return ADMIX_OK;
 }
 
-int admix_init_em(admix_ctx *h, int32_t iters, double *ll_hist)
+/* init_em! stream-ordered on the handle's stream (no synchronisation) */
+static int enq_init_em(admix_ctx *h, int32_t iters, double *ll_hist)
 {
-    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
-    if (iters < 0) return fail(h, ADMIX_ERR_ARG, "iters must be >= 0");
     for (int it = 0; it < iters; ++it) {
         CK(h, enq_em(h));
         CK(h, cudaMemcpyAsync(Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), sizeof(double) * h->K * h->J, cudaMemcpyDeviceToDevice, h->st));
@@ -413,6 +431,15 @@ int admix_init_em(admix_ctx *h, int32_t iters, double *ll_hist)
         if (ll_hist) CK(h, cudaMemcpyAsync(ll_hist + it, &h->sc->ll_tmp, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     }
     CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new));
+    return ADMIX_OK;
+}
+
+int admix_init_em(admix_ctx *h, int32_t iters, double *ll_hist)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (iters < 0) return fail(h, ADMIX_ERR_ARG, "iters must be >= 0");
+    int rc = enq_init_em(h, iters, ll_hist);
+    if (rc != ADMIX_OK) return rc;
     CK(h, cudaStreamSynchronize(h->st));
     return ADMIX_OK;
 }
@@ -488,11 +515,12 @@ static int ensure_graph(admix_ctx *h)
         return fail(h, ADMIX_ERR_CUDA, "iteration capture failed: %s / %s", cudaGetErrorString(e), cudaGetErrorString(e2));
     }
     e = cudaGraphInstantiate(&h->iter_graph, g, 0);
-    cudaGraphDestroy(g);
     if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
         h->iter_graph = nullptr;
         return fail(h, ADMIX_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
     }
+    h->iter_graph_def = g;
     return ADMIX_OK;
 }
 
@@ -648,6 +676,382 @@ int admix_loglik_dev(const uint8_t *d_bed, int64_t I, int64_t J, int32_t K, cons
                     sizeof(double) * (size_t)pl.gx * pl.gy);
     cudaError_t e = launch_loglik_f64(K, d_bed, I, J, (I + 3) / 4, d_q, d_p, pl, (double *)d_work, d_out, (cudaStream_t)stream);
     if (e != cudaSuccess) return fail(nullptr, ADMIX_ERR_CUDA, "loglik launch failed: %s", cudaGetErrorString(e));
+    return ADMIX_OK;
+}
+
+} /* extern "C" */
+
+/* ===================================================================== batches
+ * Restarts and K sweeps over one cohort: n member handles over one device copy of the
+ * genotypes.  A batch iteration is one graph launch: per active member a branch
+ * [iteration number H2D] -> [the member's captured iteration graph] -> [scalars D2H]; branches
+ * are independent, so the members' kernels run concurrently and fill the GPU even when one
+ * member alone would not. */
+
+struct admix_batch {
+    int64_t I = 0, J = 0, pitch = 0;
+    uint32_t flags = 0;
+    int sms = 148, divisor = 1;
+    cudaStream_t st = nullptr;
+    uint8_t *bed = nullptr;
+    std::vector<admix_ctx *> m;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int> exec_members;
+    char err[512] = {0};
+};
+
+static int bfail(admix_batch *b, int code, const char *fmt, ...)
+{
+    char *dst = b ? b->err : g_err;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(dst, 512, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define BCK(b, call)                                                                           \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return bfail((b), ADMIX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+static void batch_release(admix_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    for (admix_ctx *h : b->m) {
+        if (!h) continue;
+        if (h->st) cudaStreamSynchronize(h->st);
+        release(h);
+        delete h;
+    }
+    if (b->bed) cudaFree(b->bed);
+    if (b->st) cudaStreamDestroy(b->st);
+}
+
+/* Plans of one member as if it had sms_eff SMs to itself.  The partial-sum buffers were sized
+ * for the full SM count, and every plan's slice count only shrinks with fewer SMs. */
+static void set_plans(admix_ctx *h, int sms_eff)
+{
+    h->llp = plan_loglik(h->I, h->J, sms_eff);
+    h->sq = plan_sweep_q(h->K, h->I, h->J, sms_eff);
+    h->sp = plan_sweep_p(h->K, h->I, h->J, sms_eff);
+    h->sqm = plan_sweep_q_mixed(h->K, h->I, h->J, sms_eff);
+    h->spm = plan_sweep_p_mixed(h->K, h->I, h->J, sms_eff);
+    h->llm = plan_loglik_mixed(h->I, h->J, sms_eff);
+    if (h->iter_graph) { cudaGraphExecDestroy(h->iter_graph); h->iter_graph = nullptr; }
+    if (h->iter_graph_def) { cudaGraphDestroy(h->iter_graph_def); h->iter_graph_def = nullptr; }
+}
+
+static void batch_invalidate(admix_batch *b)
+{
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    b->exec_members.clear();
+}
+
+static int batch_sync_members(admix_batch *b)
+{
+    for (admix_ctx *h : b->m) BCK(b, cudaStreamSynchronize(h->st));
+    return ADMIX_OK;
+}
+
+/* one graph: per listed member an independent branch built by `branch` */
+template <class F>
+static int batch_compose(admix_batch *b, const std::vector<int> &members, F branch, cudaGraphExec_t *exec)
+{
+    cudaGraph_t g = nullptr;
+    BCK(b, cudaGraphCreate(&g, 0));
+    for (int mi : members) {
+        int rc = branch(g, b->m[mi]);
+        if (rc != ADMIX_OK) { cudaGraphDestroy(g); return rc; }
+    }
+    cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { *exec = nullptr; return bfail(b, ADMIX_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(e)); }
+    return ADMIX_OK;
+}
+
+static int batch_iteration_graph(admix_batch *b, const std::vector<int> &active)
+{
+    if (b->exec && active == b->exec_members) return ADMIX_OK;
+    batch_invalidate(b);
+    auto branch = [b](cudaGraph_t g, admix_ctx *h) -> int {
+        if (ensure_graph(h) != ADMIX_OK) return bfail(b, ADMIX_ERR_CUDA, "member capture: %s", h->err);
+        cudaGraphNode_t n0, n1, n2;
+        BCK(b, cudaGraphAddMemcpyNode1D(&n0, g, nullptr, 0, &h->sc->iter, h->iter_host, sizeof(int32_t),
+                                        cudaMemcpyHostToDevice));
+        BCK(b, cudaGraphAddChildGraphNode(&n1, g, &n0, 1, h->iter_graph_def));
+        BCK(b, cudaGraphAddMemcpyNode1D(&n2, g, &n1, 1, h->sc_host, h->sc, sizeof(DevScalars),
+                                        cudaMemcpyDeviceToHost));
+        return ADMIX_OK;
+    };
+    int rc = batch_compose(b, active, branch, &b->exec);
+    if (rc == ADMIX_OK) b->exec_members = active;
+    return rc;
+}
+
+/* Member passes captured as one graph per member: Q sweep, P sweep and the iteration's
+ * log-likelihood form, all on X (they write only partial sums and a scratch scalar). */
+static int capture_probe(admix_batch *b, admix_ctx *h, cudaGraph_t *out)
+{
+    *out = nullptr;
+    BCK(b, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int S;
+    cudaError_t e = enq_sweep_q(h, ADMIX_X, ADMIX_X, &S);
+    if (e == cudaSuccess) e = enq_sweep_p(h, ADMIX_X, ADMIX_X, &S);
+    if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X, &h->sc->ll_tmp, true);
+    cudaError_t e2 = cudaStreamEndCapture(h->st, out);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (*out) cudaGraphDestroy(*out);
+        *out = nullptr;
+        return bfail(b, ADMIX_ERR_CUDA, "probe capture: %s / %s", cudaGetErrorString(e), cudaGetErrorString(e2));
+    }
+    return ADMIX_OK;
+}
+
+static int time_probe(admix_batch *b, double *ms)
+{
+    std::vector<int> all(b->m.size());
+    for (size_t t = 0; t < all.size(); ++t) all[t] = (int)t;
+    cudaGraphExec_t ex = nullptr;
+    auto branch = [b](cudaGraph_t g, admix_ctx *h) -> int {
+        cudaGraph_t pg = nullptr;
+        int rc = capture_probe(b, h, &pg);
+        if (rc != ADMIX_OK) return rc;
+        cudaGraphNode_t n;
+        cudaError_t e = cudaGraphAddChildGraphNode(&n, g, nullptr, 0, pg);
+        cudaGraphDestroy(pg);
+        if (e != cudaSuccess) return bfail(b, ADMIX_ERR_CUDA, "probe node: %s", cudaGetErrorString(e));
+        return ADMIX_OK;
+    };
+    int rc = batch_compose(b, all, branch, &ex);
+    if (rc != ADMIX_OK) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ex, b->st);                 /* warm-up */
+    if (e == cudaSuccess) e = cudaEventRecord(e0, b->st);
+    for (int r = 0; r < 2 && e == cudaSuccess; ++r) e = cudaGraphLaunch(ex, b->st);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, b->st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float f = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaGraphExecDestroy(ex);
+    if (e != cudaSuccess) return bfail(b, ADMIX_ERR_CUDA, "probe timing: %s", cudaGetErrorString(e));
+    *ms = f / 2.0;
+    return ADMIX_OK;
+}
+
+extern "C" {
+
+static int batch_create_common(int64_t I, int64_t J, const uint8_t *bed, bool on_device, int64_t src_pitch,
+                               int32_t n, const int32_t *Ks, int32_t Q, uint32_t flags, admix_batch **out)
+{
+    if (!out) return bfail(nullptr, ADMIX_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (n < 1 || !Ks) return bfail(nullptr, ADMIX_ERR_ARG, "a batch needs n >= 1 members and their K (n=%d)", n);
+    if (I < 1 || J < 1) return bfail(nullptr, ADMIX_ERR_ARG, "I and J must be >= 1");
+    if (!bed) return bfail(nullptr, ADMIX_ERR_ARG, "bed is NULL");
+    if (src_pitch < (I + 3) / 4) return bfail(nullptr, ADMIX_ERR_ARG, "src_pitch %lld is below ceil(I/4) = %lld",
+                                              (long long)src_pitch, (long long)((I + 3) / 4));
+    for (int t = 0; t < n; ++t)
+        if (Ks[t] < 1 || Ks[t] > ADMIX_MAX_K)
+            return bfail(nullptr, ADMIX_ERR_UNSUPPORTED, "member %d: K=%d outside [1, %d]", t, Ks[t], ADMIX_MAX_K);
+    if (Q < 1 || Q > ADMIX_MAX_Q) return bfail(nullptr, ADMIX_ERR_UNSUPPORTED, "Q=%d outside [1, %d]", Q, ADMIX_MAX_Q);
+    if (flags & ~(ADMIX_FLAG_MU_GERSHGORIN | ADMIX_FLAG_MIXED)) return bfail(nullptr, ADMIX_ERR_ARG, "unknown flags 0x%x", flags);
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev == 0) return bfail(nullptr, ADMIX_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(ce));
+
+    admix_batch *b = new admix_batch();
+    b->I = I; b->J = J; b->flags = flags;
+    b->pitch = ((I + 3) / 4 + 15) / 16 * 16;
+    b->m.assign((size_t)n, nullptr);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        e = cudaMalloc((void **)&b->bed, (size_t)b->pitch * J + 64);
+        if (e != cudaSuccess) {
+            b->bed = nullptr;
+            bfail(nullptr, ADMIX_ERR_NOMEM, "cudaMalloc of %lld genotype bytes failed", (long long)(b->pitch * J + 64));
+            batch_release(b); delete b;
+            return ADMIX_ERR_NOMEM;
+        }
+    }
+    if (e == cudaSuccess) e = upload_genotypes(b->bed, b->pitch, bed, src_pitch, I, J, on_device, b->sms, b->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+    if (e != cudaSuccess) {
+        bfail(nullptr, ADMIX_ERR_CUDA, "batch genotypes: %s", cudaGetErrorString(e));
+        batch_release(b); delete b;
+        return ADMIX_ERR_CUDA;
+    }
+    for (int t = 0; t < n; ++t) {
+        int rc = create_common(I, J, Ks[t], Q, bed, on_device, src_pitch, flags, &b->m[t], b->bed);
+        if (rc != ADMIX_OK) {
+            char msg[512];
+            snprintf(msg, sizeof(msg), "member %d: %s", t, g_err);
+            batch_release(b); delete b;
+            bfail(nullptr, rc, "%s", msg);
+            return rc;
+        }
+    }
+    *out = b;
+    return ADMIX_OK;
+}
+
+int admix_batch_create(int64_t I, int64_t J, const uint8_t *bed, int32_t n, const int32_t *Ks, int32_t Q,
+                       uint32_t flags, admix_batch **out)
+{
+    return batch_create_common(I, J, bed, false, (I + 3) / 4, n, Ks, Q, flags, out);
+}
+
+int admix_batch_create_device(int64_t I, int64_t J, const uint8_t *d_bed, int64_t src_pitch, int32_t n,
+                              const int32_t *Ks, int32_t Q, uint32_t flags, admix_batch **out)
+{
+    cudaPointerAttributes at;
+    if (d_bed && (cudaPointerGetAttributes(&at, d_bed) != cudaSuccess || at.type != cudaMemoryTypeDevice)) {
+        cudaGetLastError();
+        return bfail(nullptr, ADMIX_ERR_ARG, "d_bed is not device memory");
+    }
+    return batch_create_common(I, J, d_bed, true, src_pitch, n, Ks, Q, flags, out);
+}
+
+int admix_batch_destroy(admix_batch *b)
+{
+    if (!b) return ADMIX_OK;
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_release(b);
+    delete b;
+    return ADMIX_OK;
+}
+
+const char *admix_batch_last_error(const admix_batch *b) { return b ? b->err : g_err; }
+
+int admix_batch_size(const admix_batch *b, int32_t *n)
+{
+    if (!b || !n) return bfail(nullptr, ADMIX_ERR_ARG, "NULL argument");
+    *n = (int32_t)b->m.size();
+    return ADMIX_OK;
+}
+
+int admix_batch_member(admix_batch *b, int32_t m, admix_ctx **h)
+{
+    if (!b || !h) return bfail(b, ADMIX_ERR_ARG, "NULL argument");
+    if (m < 0 || m >= (int32_t)b->m.size()) return bfail(b, ADMIX_ERR_ARG, "member %d outside [0, %d)", m, (int)b->m.size());
+    *h = b->m[m];
+    return ADMIX_OK;
+}
+
+int admix_batch_init_em(admix_batch *b, int32_t iters, double *ll_hist)
+{
+    if (!b) return bfail(nullptr, ADMIX_ERR_ARG, "batch is NULL");
+    if (iters < 0) return bfail(b, ADMIX_ERR_ARG, "iters must be >= 0");
+    for (size_t t = 0; t < b->m.size(); ++t) {          /* member streams run concurrently */
+        int rc = enq_init_em(b->m[t], iters, ll_hist ? ll_hist + t * (size_t)iters : nullptr);
+        if (rc != ADMIX_OK) return bfail(b, rc, "member %d: %s", (int)t, b->m[t]->err);
+    }
+    return batch_sync_members(b);
+}
+
+int admix_batch_set_split(admix_batch *b, int32_t divisor)
+{
+    if (!b) return bfail(nullptr, ADMIX_ERR_ARG, "batch is NULL");
+    if (divisor < 1) return bfail(b, ADMIX_ERR_ARG, "divisor must be >= 1 (got %d)", divisor);
+    int rc = batch_sync_members(b);
+    if (rc != ADMIX_OK) return rc;
+    batch_invalidate(b);
+    const int sms_eff = std::max(1, b->sms / divisor);
+    for (admix_ctx *h : b->m) set_plans(h, sms_eff);
+    b->divisor = divisor;
+    return ADMIX_OK;
+}
+
+int admix_batch_autotune(admix_batch *b, int32_t *divisor, double *ms)
+{
+    if (!b) return bfail(nullptr, ADMIX_ERR_ARG, "batch is NULL");
+    int rc = batch_sync_members(b);
+    if (rc != ADMIX_OK) return rc;
+    const int limit = std::max(1, 4 * (int)b->m.size());
+    int best_d = 1;
+    double best = 1e300;
+    for (int d = 1; d <= limit && d <= b->sms; d *= 2) {
+        rc = admix_batch_set_split(b, d);
+        if (rc != ADMIX_OK) return rc;
+        double t = 0.0;
+        rc = time_probe(b, &t);
+        if (rc != ADMIX_OK) return rc;
+        if (t < best) { best = t; best_d = d; }
+    }
+    rc = admix_batch_set_split(b, best_d);
+    if (rc != ADMIX_OK) return rc;
+    if (divisor) *divisor = best_d;
+    if (ms) *ms = best;
+    return ADMIX_OK;
+}
+
+int admix_batch_run_qn(admix_batch *b, int32_t n_iter, double rtol, int32_t *n_done, int32_t *converged,
+                       admix_iterinfo *last, double *ms_device)
+{
+    if (!b) return bfail(nullptr, ADMIX_ERR_ARG, "batch is NULL");
+    if (n_iter < 0) return bfail(b, ADMIX_ERR_ARG, "n_iter must be >= 0");
+    const int n = (int)b->m.size();
+    int rc = batch_sync_members(b);
+    if (rc != ADMIX_OK) return rc;
+    /* a member without a log-likelihood gets its FP64 value first (algorithms_outer.jl:76-83) */
+    for (admix_ctx *h : b->m) {
+        BCK(b, cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+        BCK(b, cudaStreamSynchronize(h->st));
+        if (isnan(h->sc_host->ll_new)) BCK(b, enq_loglik(h, ADMIX_X, &h->sc->ll_new));
+    }
+    rc = batch_sync_members(b);
+    if (rc != ADMIX_OK) return rc;
+    std::vector<int> active(n), done(n, 0), conv(n, 0);
+    for (int t = 0; t < n; ++t) active[t] = t;
+    std::vector<admix_iterinfo> rec((size_t)n);
+    memset(rec.data(), 0, sizeof(admix_iterinfo) * n);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BCK(b, cudaEventCreate(&e0));
+    cudaError_t e = cudaEventCreate(&e1);
+    double total = 0.0;
+    for (int it = 1; it <= n_iter && !active.empty() && e == cudaSuccess; ++it) {
+        rc = batch_iteration_graph(b, active);
+        if (rc != ADMIX_OK) break;
+        for (int t : active) *b->m[t]->iter_host = it;
+        e = cudaEventRecord(e0, b->st);
+        if (e == cudaSuccess) e = cudaGraphLaunch(b->exec, b->st);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, b->st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float f = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+        total += f;
+        std::vector<int> still;
+        for (int t : active) {
+            const DevScalars &s = *b->m[t]->sc_host;
+            admix_iterinfo &r = rec[t];
+            r.ll_prev = s.ll_prev; r.ll_basic = s.ll_basic; r.ll_qn = s.ll_qn; r.ll_new = s.ll_new;
+            r.reldiff = s.reldiff; r.iter = it; r.accepted_qn = s.accepted; r.qp_fail_q = s.fail_q;
+            r.qp_fail_p = s.fail_p;
+            done[t] = it;
+            if (s.reldiff < rtol) conv[t] = 1;
+            else still.push_back(t);
+        }
+        active.swap(still);
+    }
+    cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (rc != ADMIX_OK) return rc;
+    if (e != cudaSuccess) return bfail(b, ADMIX_ERR_CUDA, "batch iteration: %s", cudaGetErrorString(e));
+    for (int t = 0; t < n; ++t) {
+        if (n_done) n_done[t] = done[t];
+        if (converged) converged[t] = conv[t];
+        if (last) last[t] = rec[t];
+    }
+    if (ms_device) *ms_device = total;
     return ADMIX_OK;
 }
 

@@ -115,3 +115,22 @@ def test_decode_matches_golden(oa):
     gg, nm = g.decode()
     assert np.array_equal((nm == 0).sum(1), z["miss_ind"])
     assert np.array_equal((nm == 0).sum(0), z["miss_snp"])
+
+
+def test_batch_create_rejects_bad_arguments_without_touching_a_gpu(oa):
+    from openadmixture_b200 import _native as N
+    lib = N.admix_lib()
+    b = C.c_void_p()
+    bed = np.zeros((4, 1), np.uint8)
+    ks = (C.c_int32 * 3)(3, 17, 4)
+    assert lib.admix_batch_create(4, 4, N.u8ptr(bed), 0, ks, 3, 0, C.byref(b)) == N.ADMIX_ERR_ARG
+    assert b"n >= 1" in lib.admix_batch_last_error(None)
+    assert lib.admix_batch_create(4, 4, N.u8ptr(bed), 3, ks, 3, 0, C.byref(b)) == N.ADMIX_ERR_UNSUPPORTED
+    assert b"member 1: K=17" in lib.admix_batch_last_error(None)
+    ok = (C.c_int32 * 2)(3, 4)
+    assert lib.admix_batch_create(4, 4, N.u8ptr(bed), 2, ok, 9, 0, C.byref(b)) == N.ADMIX_ERR_UNSUPPORTED
+    assert lib.admix_batch_create(4, 4, N.u8ptr(bed), 2, ok, 3, 0x100, C.byref(b)) == N.ADMIX_ERR_ARG
+    assert lib.admix_batch_create(4, 4, None, 2, ok, 3, 0, C.byref(b)) == N.ADMIX_ERR_ARG
+    assert lib.admix_batch_create_device(40, 4, None, 9, 2, ok, 3, 0, C.byref(b)) == N.ADMIX_ERR_ARG
+    assert lib.admix_batch_run_qn(None, 5, 1e-7, None, None, None, None) == N.ADMIX_ERR_ARG
+    assert lib.admix_batch_destroy(None) == N.ADMIX_OK
