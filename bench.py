@@ -49,6 +49,8 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ttc", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 form beside the chosen one")
+    ap.add_argument("--I", type=int, default=None, help="override the configuration's I (--pass-only runs)")
+    ap.add_argument("--J", type=int, default=None, help="override the configuration's J (--pass-only runs)")
     ap.add_argument("--pass-only", default=None,
                     choices=["loglik", "q_sweep", "p_sweep", "q_qp", "p_qp", "em"],
                     help="set up the cohort and launch one pass warmup+steps times (for profilers)")
@@ -62,7 +64,7 @@ def run_pass_only(args):
     import openadmixture_b200 as oa
     from openadmixture_b200 import _native as N
     torch.cuda.set_device(0)
-    spec = oa.COHORTS[args.config]
+    spec = oa.COHORTS[args.config].scaled(I=args.I, J=args.J)
     if spec.I * spec.J > 2_000_000_000:
         qt, pt = oa.truth(spec)
         g = oa.genotypes_device(spec, qt, pt)
@@ -76,7 +78,8 @@ def run_pass_only(args):
         if pid in (N.ADMIX_PASS_QQP, N.ADMIX_PASS_PQP):   # give the QPs real sweep outputs
             d_cu.time_pass(N.ADMIX_PASS_QSWEEP if pid == N.ADMIX_PASS_QQP else N.ADMIX_PASS_PSWEEP, 1)
         ms = d_cu.time_pass(pid, max(1, args.steps))
-    print(json.dumps({"pass": args.pass_only, "config": spec.name, "ms_per_launch": ms}), flush=True)
+    print(json.dumps({"pass": args.pass_only, "config": spec.name, "I": spec.I, "J": spec.J, "K": spec.K,
+                      "form": args.form, "ms_per_launch": ms}), flush=True)
     return 0
 
 

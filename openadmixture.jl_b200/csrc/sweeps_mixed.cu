@@ -56,242 +56,380 @@ __device__ __forceinline__ uint4 interleave8(uint2 a, uint2 b)
                       __byte_perm(a.y, b.y, 0x5140), __byte_perm(a.y, b.y, 0x7362));
 }
 
-/* ===================================================================== Q side */
+/* ===================================================================== Q side
+ *
+ * Per 32-SNP chunk, two tensor-core products:
+ *   qp / om    D[128 x 64] = Qtile * [p ; 1-p]^T in TF32 split form (hi*hi + lo*hi + hi*lo, about
+ *              2^-21 relative): the K-term dot products of every (individual, SNP) cell;
+ *   Hessian    D[128 x N] += [w1 | w2] * [PP ; PbarPbar]^T in BF16 (FP32 accumulation);
+ * and on the CUDA cores, per cell: the code lookup, one reciprocal, z1, z2, w1, w2 and the FP32
+ * gradient sum_j (z1 - z2) p_k + z2 (= sum_j z1 p_k + z2 (1 - p_k)), added into FP64 per chunk.
+ *
+ * Everything that depends on P alone -- the BF16 pair-product tiles, the TF32 hi / lo split of
+ * [p ; 1-p] and p in FP32 -- is built once per sweep by k_q_pack, one "package" per chunk laid
+ * out exactly as the sweep's shared memory wants it, and fetched by each CTA with one bulk
+ * asynchronous copy (three package buffers in flight).  The qp MMA of chunk c+1 runs while the
+ * CUDA cores work on chunk c. */
 
-constexpr int MQ_JC = 32;          /* SNPs per chunk = 2 MMA K-steps */
+constexpr int MQ_JC = 32;          /* SNPs per chunk = 2 BF16 MMA K-steps */
 constexpr int MQ_THREADS = 128;    /* one thread per individual = accumulator row */
+constexpr int MQ_NPKG = 3;         /* package buffers */
 
 template <int K>
 struct MQ {
     static constexpr int T = K * (K + 1) / 2;
-    static constexpr int N = ((T + 15) / 16) * 16;              /* MMA N (multiple of 16 for M = 128) */
-    static constexpr uint32_t NCOLS = tmem_cols_for(N);
+    static constexpr int N = ((T + 15) / 16) * 16;              /* Hessian MMA N (multiple of 16 for M = 128) */
+    static constexpr int KP = ((K + 7) / 8) * 8;                /* TF32 K extent of the qp MMAs */
+    static constexpr int QPN = 2 * MQ_JC;                       /* qp MMA N: the chunk's p rows, then 1-p rows */
+    static constexpr uint32_t COL_H = 64;                       /* TMEM column of the Hessian accumulator */
+    static constexpr uint32_t NCOLS = tmem_cols_for(COL_H + N);
     static constexpr int E = T + K;                             /* partial entries per individual */
     static constexpr uint32_t A_BYTES = 128 * MQ_JC * 2;        /* one BF16 weight tile: 8 KB */
     static constexpr uint32_t B_BYTES = N * MQ_JC * 2;          /* one BF16 pair-product tile */
-    static constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-    static constexpr int PS = MQ_JC + 2;                        /* P row stride (floats): rows on distinct banks */
-    static constexpr uint32_t PBUF = 2 * K * PS * 4;            /* p and 1-p of one chunk, FP32 [k][jj] */
+    static constexpr uint32_t QA_BYTES = 128 * 2 * KP * 4;      /* TF32 Q tile [hi | lo] */
+    static constexpr uint32_t QB_BYTES = QPN * 2 * KP * 4;      /* TF32 [p ; 1-p] chunk [hi | lo] */
+    static constexpr int PS = MQ_JC + 4;                        /* FP32 p row stride (floats, 16-byte rows) */
+    /* package of one chunk: [PP tile | PbarPbar tile | TF32 [p ; 1-p] | FP32 p [k][jj]] */
+    static constexpr uint32_t PK_QB = 2 * B_BYTES;
+    static constexpr uint32_t PK_PF = PK_QB + QB_BYTES;
+    static constexpr uint32_t PKG = PK_PF + K * PS * 4;
     static constexpr uint32_t GBUF = MQ_JC * 32;                /* genotype bytes of one chunk */
-    static constexpr uint32_t OFF_P = 2 * STAGE_BYTES;          /* two P buffers */
-    static constexpr uint32_t OFF_G = OFF_P + 2 * PBUF;         /* two G buffers, [pair][byte][2] */
+    static constexpr uint32_t OFF_A = 0;                        /* W1 tile, then W2 tile */
+    static constexpr uint32_t OFF_PKG = 2 * A_BYTES;
+    static constexpr uint32_t OFF_QA = OFF_PKG + MQ_NPKG * PKG;
+    static constexpr uint32_t OFF_G = OFF_QA + QA_BYTES;        /* two G buffers, [pair][byte][2] */
     static constexpr uint32_t OFF_TAB = OFF_G + 2 * GBUF;       /* float4 [16][8] code table */
     static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024; /* + alignment slack */
-    /* A core matrices 128 B apart along M, 2048 B along K; B 128 B along N, 16 N bytes along K */
+    /* core matrices (8 rows x 16 B): BF16 A 128 B apart along M, 2048 B along K; BF16 B 128 B
+     * along N, 16 N bytes along K; TF32 Q tile 128 B along M, 2048 B along K; TF32 [p ; 1-p]
+     * 128 B along N, 1024 B along K */
     static constexpr uint32_t A_LBO = 2048, A_SBO = 128;
     static constexpr uint32_t B_LBO = 16 * N, B_SBO = 128;
-    static constexpr int PREF_P = (K * MQ_JC + MQ_THREADS - 1) / MQ_THREADS;
+    static constexpr uint32_t QA_LBO = 2048, QB_LBO = 1024, Q_SBO = 128;
+    static_assert(PKG % 16 == 0 && OFF_QA % 16 == 0, "bulk copies and descriptors need 16-byte alignment");
 };
 
-/* One chunk's inputs in registers (loaded a chunk ahead): threads 0..63 hold 8 bytes of each of
- * the SNP pair's two columns (pair t >> 2, bytes 8 (t & 3) .. +7 of the CTA's 32); every thread
- * holds up to PREF_P allele frequencies. */
-template <int K>
-struct QChunk {
-    uint2 ga, gb;
-    double pv[MQ<K>::PREF_P];
-};
+/* byte offset of element (row r, 4-byte column f) in a K-major no-swizzle tile */
+__device__ __forceinline__ uint32_t kmaj_off(int r, int f, uint32_t lbo)
+{
+    return (uint32_t)(f >> 2) * lbo + (uint32_t)(r >> 3) * 128u + (uint32_t)(r & 7) * 16u + (uint32_t)(f & 3) * 4u;
+}
 
+/* One package per 32-SNP chunk of the whole SNP range (block = chunk).  SNPs beyond J get
+ * p = 0.5; their genotypes read as missing, so they contribute nothing. */
 template <int K>
-__device__ __forceinline__ void qchunk_load(QChunk<K> &cr, const uint8_t *__restrict__ bed, int64_t pitch,
-                                            const double *__restrict__ p, int64_t i0, int64_t jc, int n, int tid)
+__global__ void __launch_bounds__(128)
+k_q_pack(const double *__restrict__ p, int64_t J, uint8_t *__restrict__ pkg)
+{
+    using C = MQ<K>;
+    constexpr int T = C::T, N = C::N;
+    __shared__ __align__(16) float pf[2 * K * C::PS];          /* p, then 1-p: [term][k][jj] */
+    __shared__ __align__(16) uint8_t buf[C::PKG];
+    const int tid = threadIdx.x;
+    const int64_t jc = (int64_t)blockIdx.x * MQ_JC;
+    for (uint32_t t = tid; t < C::PKG / 16; t += 128) ((uint4 *)buf)[t] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    for (int t = tid; t < K * MQ_JC; t += 128) {
+        const int jj = t / K, k = t - jj * K;
+        const double pd = (jc + jj < J) ? p[(size_t)K * jc + t] : 0.5;
+        const float a = (float)pd, b = (float)(1.0 - pd);
+        pf[k * C::PS + jj] = a;
+        pf[K * C::PS + k * C::PS + jj] = b;
+        ((float *)(buf + C::PK_PF))[k * C::PS + jj] = a;
+        float h, l;
+        tf32_split(a, h, l);
+        *(float *)(buf + C::PK_QB + kmaj_off(jj, k, C::QB_LBO)) = h;
+        *(float *)(buf + C::PK_QB + kmaj_off(jj, C::KP + k, C::QB_LBO)) = l;
+        tf32_split(b, h, l);
+        *(float *)(buf + C::PK_QB + kmaj_off(MQ_JC + jj, k, C::QB_LBO)) = h;
+        *(float *)(buf + C::PK_QB + kmaj_off(MQ_JC + jj, C::KP + k, C::QB_LBO)) = l;
+    }
+    __syncthreads();
+    /* pair-product tiles: task (term, kc, nn) writes pair nn's 8 SNPs of k-chunk kc at kc*16N + 16nn */
+    for (int t = tid; t < 2 * 4 * N; t += 128) {
+        const int term = t / (4 * N), rem = t - term * 4 * N;
+        const int kc = rem / N, nn = rem - kc * N;
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+        if (nn < T) {
+            int ka, kb;
+            tri_pair(nn, ka, kb);
+            const float *src = pf + term * K * C::PS + kc * 8;
+            const float4 a0 = *(const float4 *)(src + ka * C::PS), a1 = *(const float4 *)(src + ka * C::PS + 4);
+            const float4 b0 = *(const float4 *)(src + kb * C::PS), b1 = *(const float4 *)(src + kb * C::PS + 4);
+            w[0] = pack_bf16x2(a0.x * b0.x, a0.y * b0.y);
+            w[1] = pack_bf16x2(a0.z * b0.z, a0.w * b0.w);
+            w[2] = pack_bf16x2(a1.x * b1.x, a1.y * b1.y);
+            w[3] = pack_bf16x2(a1.z * b1.z, a1.w * b1.w);
+        }
+        *(uint4 *)(buf + term * C::B_BYTES + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    __syncthreads();
+    uint4 *dst = (uint4 *)(pkg + (size_t)blockIdx.x * C::PKG);
+    for (uint32_t t = tid; t < C::PKG / 16; t += 128) dst[t] = ((const uint4 *)buf)[t];
+}
+
+/* genotype bytes of one chunk in registers (loaded a chunk ahead): threads 0..63 hold 8 bytes
+ * of each of the SNP pair's two columns (pair t >> 2, bytes 8 (t & 3) .. +7 of the CTA's 32) */
+__device__ __forceinline__ void qgeno_load(uint2 &ga, uint2 &gb, const uint8_t *__restrict__ bed, int64_t pitch,
+                                           int64_t i0, int64_t jc, int n, int tid)
 {
     if (tid < 64) {
         const int m = tid >> 2, qb = tid & 3;
         const size_t off = (size_t)(i0 / 4) + 8 * qb;
         const uint2 miss = make_uint2(0x55555555u, 0x55555555u);
-        cr.ga = (2 * m < n) ? __ldg((const uint2 *)(bed + (size_t)(jc + 2 * m) * pitch + off)) : miss;
-        cr.gb = (2 * m + 1 < n) ? __ldg((const uint2 *)(bed + (size_t)(jc + 2 * m + 1) * pitch + off)) : miss;
-    }
-#pragma unroll
-    for (int u = 0; u < MQ<K>::PREF_P; ++u) {
-        const int t = tid + u * MQ_THREADS;          /* t = jj * K + k: coalesced loads; the padded */
-        const int jj = t / K;                        /* row stride keeps the stores <= 2-way conflicted */
-        cr.pv[u] = (t < K * MQ_JC && jj < n) ? p[(size_t)K * jc + t] : 0.5;
+        ga = (2 * m < n) ? __ldg((const uint2 *)(bed + (size_t)(jc + 2 * m) * pitch + off)) : miss;
+        gb = (2 * m + 1 < n) ? __ldg((const uint2 *)(bed + (size_t)(jc + 2 * m + 1) * pitch + off)) : miss;
     }
 }
 
-/* registers -> shared: p / 1-p as FP32 [k][jj]; genotypes as [pair m][byte b][2] */
-template <int K>
-__device__ __forceinline__ void qchunk_store(const QChunk<K> &cr, float *Pb, uint8_t *Gb, int tid)
+/* registers -> shared as [pair m][byte b][2] */
+__device__ __forceinline__ void qgeno_store(uint2 ga, uint2 gb, uint8_t *Gb, int tid)
 {
     if (tid < 64) {
         const int m = tid >> 2, qb = tid & 3;
-        *(uint4 *)(Gb + (m * 32 + 8 * qb) * 2) = interleave8(cr.ga, cr.gb);
+        *(uint4 *)(Gb + (m * 32 + 8 * qb) * 2) = interleave8(ga, gb);
     }
+}
+
+/* qp / om of the package's chunk into TMEM columns 0..63: 3 * KP/8 TF32 MMAs (one thread) */
+template <int K>
+__device__ __forceinline__ void issue_qp(uint32_t tmem, const uint8_t *sm, const uint8_t *pk)
+{
+    using C = MQ<K>;
+    const uint32_t a = smem_u32(sm + C::OFF_QA), b = smem_u32(pk + C::PK_QB);
+    constexpr uint32_t id = idesc_tf32_f32(128, C::QPN);
+    constexpr uint32_t alo = (C::KP / 4) * C::QA_LBO, blo = (C::KP / 4) * C::QB_LBO;
 #pragma unroll
-    for (int u = 0; u < MQ<K>::PREF_P; ++u) {
-        const int t = tid + u * MQ_THREADS;
-        if (t < K * MQ_JC) {
-            const int jj = t / K, k = t - jj * K;
-            Pb[k * MQ<K>::PS + jj] = (float)cr.pv[u];
-            Pb[K * MQ<K>::PS + k * MQ<K>::PS + jj] = (float)(1.0 - cr.pv[u]);
-        }
+    for (int s = 0; s < C::KP / 8; ++s) {
+        const uint32_t ao = a + s * 2 * C::QA_LBO, bo = b + s * 2 * C::QB_LBO;
+        const uint64_t ahi = umma_desc_kmajor(ao, C::QA_LBO, C::Q_SBO);
+        const uint64_t alw = umma_desc_kmajor(ao + alo, C::QA_LBO, C::Q_SBO);
+        const uint64_t bhi = umma_desc_kmajor(bo, C::QB_LBO, C::Q_SBO);
+        const uint64_t blw = umma_desc_kmajor(bo + blo, C::QB_LBO, C::Q_SBO);
+        tc_mma_tf32(tmem, ahi, bhi, id, s > 0 ? 1u : 0u);
+        tc_mma_tf32(tmem, alw, bhi, id, 1u);
+        tc_mma_tf32(tmem, ahi, blw, id, 1u);
     }
 }
 
 template <int K>
 __global__ void __launch_bounds__(MQ_THREADS)
 k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
-                const double *__restrict__ q, const double *__restrict__ p, int64_t jslice,
+                const double *__restrict__ q, const uint8_t *__restrict__ pkg, int64_t jslice,
                 double *__restrict__ out, int *__restrict__ err)
 {
     using C = MQ<K>;
     constexpr int T = C::T, N = C::N, E = C::E;
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    __shared__ uint64_t mbar[2];
+    __shared__ uint64_t mbar[2 + MQ_NPKG];              /* Hessian MMA, qp MMA, package copies */
     __shared__ uint32_t tmem_holder;
+    uint64_t *bar_h = &mbar[0], *bar_q = &mbar[1], *bar_p = &mbar[2];
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const int64_t i0 = (int64_t)blockIdx.x * 128;
     const int64_t i = i0 + tid;
     const bool valid = i < I;
-    const int64_t j0 = (int64_t)blockIdx.y * jslice;
+    const int64_t j0 = (int64_t)blockIdx.y * jslice;    /* jslice is a multiple of MQ_JC */
     const int64_t j1 = min(J, j0 + jslice);
     const int nchunk = (int)((j1 - j0 + MQ_JC - 1) / MQ_JC);
+    const uint8_t *pk0 = pkg + (size_t)(j0 / MQ_JC) * C::PKG;
     const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
+    uint8_t *At = sm + C::OFF_A;
 
     if (warp == 0) tmem_alloc_warp(&tmem_holder, C::NCOLS);
     if (tid == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
+        for (int b = 0; b < 2 + MQ_NPKG; ++b) mbar_init(&mbar[b], 1);
         mbar_fence_init();
     }
     code_table_init((float4 *)(sm + C::OFF_TAB), tid, MQ_THREADS);
-    QChunk<K> cr;
-    if (nchunk > 0) {
-        qchunk_load<K>(cr, bed, pitch, p, i0, j0, (int)min((int64_t)MQ_JC, j1 - j0), tid);
-        qchunk_store<K>(cr, (float *)(sm + C::OFF_P), sm + C::OFF_G, tid);
+    {   /* this thread's row of the TF32 Q tile: columns 0..K-1 hi, KP..KP+K-1 lo, the rest zero */
+        float hv[C::KP], lv[C::KP];
+#pragma unroll
+        for (int k = 0; k < C::KP; ++k) {
+            hv[k] = 0.f; lv[k] = 0.f;
+            if (k < K) tf32_split(valid ? (float)q[(size_t)K * i + k] : 1.0f / K, hv[k], lv[k]);
+        }
+#pragma unroll
+        for (int f = 0; f < C::KP; f += 4) {
+            *(float4 *)(sm + C::OFF_QA + kmaj_off(tid, f, C::QA_LBO)) = make_float4(hv[f], hv[f + 1], hv[f + 2], hv[f + 3]);
+            *(float4 *)(sm + C::OFF_QA + kmaj_off(tid, C::KP + f, C::QA_LBO)) = make_float4(lv[f], lv[f + 1], lv[f + 2], lv[f + 3]);
+        }
     }
-    if (nchunk > 1) qchunk_load<K>(cr, bed, pitch, p, i0, j0 + MQ_JC, (int)min((int64_t)MQ_JC, j1 - j0 - MQ_JC), tid);
+    uint2 ga = make_uint2(0u, 0u), gb = make_uint2(0u, 0u);
+    if (nchunk > 0) {
+        qgeno_load(ga, gb, bed, pitch, i0, j0, (int)min((int64_t)MQ_JC, j1 - j0), tid);
+        qgeno_store(ga, gb, sm + C::OFF_G, tid);
+    }
+    if (nchunk > 1) qgeno_load(ga, gb, bed, pitch, i0, j0 + MQ_JC, (int)min((int64_t)MQ_JC, j1 - j0 - MQ_JC), tid);
+    fence_async_smem();
     tc_fence_before_sync();
-    __syncthreads();
+    __syncthreads();                                    /* barriers initialised, Q tile staged */
     tc_fence_after_sync();
     const uint32_t tmem = tmem_holder;
-
-    float2 qq[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const float v = valid ? (float)q[(size_t)K * i + k] : 1.0f / K;
-        qq[k] = make_float2(v, v);
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    bool ok = true;
+    int p_issued = 0, p_waited = 0;                     /* package copies (thread 0's view) */
+    if (tid == 0) {
+        for (int c = 0; c < min(nchunk, 2); ++c) {
+            mbar_arrive_expect_tx(&bar_p[c], C::PKG);
+            bulk_g2s(sm + C::OFF_PKG + c * C::PKG, pk0 + (size_t)c * C::PKG, C::PKG, &bar_p[c]);
+            ++p_issued;
+        }
+        if (nchunk > 0) {
+            if (mbar_wait_bounded(&bar_p[0], 0u, MX_WAIT_LIMIT)) {
+                ++p_waited;
+                issue_qp<K>(tmem, sm, sm + C::OFF_PKG);
+                tc_commit(bar_q);
+            } else {
+                ok = false;
+                atomicOr(err, 1);
+            }
+        }
     }
+    ok = __syncthreads_and(ok);
+    int q_issued = (ok && nchunk > 0) ? 1 : 0, q_done = 0, h_issued = 0, h_done = 0;
+
     double gd[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) gd[k] = 0.0;
     const int sh = valid ? (int)(i & 3) * 2 : 0;
     const uint32_t gmask = valid ? 0xFFFFu : 0u;        /* rows beyond I read code pair 01|01 */
     constexpr uint32_t idesc = idesc_bf16_f32(128, N);
-    bool ok = true;
 
     for (int c = 0; c < nchunk; ++c) {
-        const int s = c & 1;
-        uint8_t *At = sm + s * C::STAGE_BYTES;                 /* W1 tile, then W2 tile */
-        uint8_t *Bt = At + 2 * C::A_BYTES;                      /* PP tile, then PbarPbar tile */
-        const float *Pb = (const float *)(sm + C::OFF_P + s * C::PBUF);
-        const uint8_t *Gb = sm + C::OFF_G + s * C::GBUF;
-        if (c >= 2 && ok) {                                     /* MMAs of chunk c-2 read this stage */
-            if (!mbar_wait_bounded(&mbar[s], (uint32_t)(((c - 2) >> 1) & 1), MX_WAIT_LIMIT)) {
-                ok = false;
-                if (tid == 0) atomicOr(err, 1);
+        const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
+        const float *Pf = (const float *)(pk + C::PK_PF);
+        const uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF;
+        /* 1. qp and 1 - qp of this thread's individual and the chunk's 32 SNPs */
+        uint32_t rq[32], ro[32];
+        if (ok && q_done < q_issued) {
+            if (mbar_wait_bounded(bar_q, (uint32_t)(q_done & 1), MX_WAIT_LIMIT)) ++q_done;
+            else { ok = false; atomicOr(err, 1); }
+        }
+        tc_fence_after_sync();
+        tmem_ld32_nowait(tmem + lane_base, rq);
+        tmem_ld32_nowait(tmem + lane_base + 32u, ro);
+        tmem_wait_ld();
+        /* 2. the Hessian MMAs of chunk c-1 are done: the weight tile and package c-1 are free */
+        if (ok && h_done < h_issued) {
+            if (mbar_wait_bounded(bar_h, (uint32_t)(h_done & 1), MX_WAIT_LIMIT)) ++h_done;
+            else { ok = false; atomicOr(err, 1); }
+        }
+        /* 3. genotypes of chunk c+1 to shared memory, chunk c+2 to registers */
+        if (c + 1 < nchunk) {
+            qgeno_store(ga, gb, sm + C::OFF_G + ((c + 1) & 1) * C::GBUF, tid);
+            if (c + 2 < nchunk) {
+                const int64_t jn = j0 + (int64_t)(c + 2) * MQ_JC;
+                qgeno_load(ga, gb, bed, pitch, i0, jn, (int)min((int64_t)MQ_JC, j1 - jn), tid);
             }
         }
-        /* B tiles: task (term, kc, nn) writes pair nn's 8 SNPs of k-chunk kc at kc*16N + 16nn */
-        for (int t = tid; t < 2 * 4 * N; t += MQ_THREADS) {
-            const int term = t / (4 * N), rem = t - term * 4 * N;
-            const int kc = rem / N, nn = rem - kc * N;
-            uint32_t w[4] = {0u, 0u, 0u, 0u};
-            if (nn < T) {
-                int ka, kb;
-                tri_pair(nn, ka, kb);
-                const float *src = Pb + term * K * C::PS;
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int jj = kc * 8 + 2 * e;
-                    w[e] = pack_bf16x2(src[ka * C::PS + jj] * src[kb * C::PS + jj],
-                                       src[ka * C::PS + jj + 1] * src[kb * C::PS + jj + 1]);
+        fence_async_smem();
+        tc_fence_before_sync();
+        ok = __syncthreads_and(ok);
+        /* 4. qp MMA of chunk c+1 (its package landed), copy of package c+2 */
+        if (ok && c + 1 < nchunk) {
+            if (tid == 0) {
+                tc_fence_after_sync();
+                const int cn = c + 1;
+                if (mbar_wait_bounded(&bar_p[cn % MQ_NPKG], (uint32_t)((cn / MQ_NPKG) & 1), MX_WAIT_LIMIT)) {
+                    ++p_waited;
+                    issue_qp<K>(tmem, sm, sm + C::OFF_PKG + (cn % MQ_NPKG) * C::PKG);
+                    tc_commit(bar_q);
+                } else {
+                    ok = false;
+                    atomicOr(err, 1);
+                }
+                if (ok && c + 2 < nchunk) {
+                    const int cm = c + 2;
+                    fence_async_smem();
+                    mbar_arrive_expect_tx(&bar_p[cm % MQ_NPKG], C::PKG);
+                    bulk_g2s(sm + C::OFF_PKG + (cm % MQ_NPKG) * C::PKG, pk0 + (size_t)cm * C::PKG, C::PKG,
+                             &bar_p[cm % MQ_NPKG]);
+                    ++p_issued;
                 }
             }
-            *(uint4 *)(Bt + term * C::B_BYTES + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
+            ++q_issued;
         }
-        /* producer: this thread's individual, the chunk's 32 SNPs as 16 pairs */
-        const float2 *P2 = (const float2 *)Pb;                  /* [k][pair], row stride PS / 2 */
-        const float2 *Pb2 = (const float2 *)(Pb + K * C::PS);
+        /* 5. producer: the chunk's 32 SNPs as 16 pairs, 4 pairs per BF16 k-chunk */
         const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);  /* [pair][byte]: both SNPs */
-        float2 ga[K];
+        float2 gk[K], zs = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int k = 0; k < K; ++k) ga[k] = make_float2(0.f, 0.f);
+        for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int kc = 0; kc < 4; ++kc) {
             uint32_t w1p[4], w2p[4];
+            float2 dz[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const int m = kc * 4 + e;                       /* SNPs 2m, 2m+1 of the chunk */
                 const uint32_t gw = ((uint32_t)G2[m * 32] & gmask) | (~gmask & 0x5555u);
                 const uint32_t tb = gw >> sh;
                 const float4 a = tab[8 * ((tb & 3u) | ((tb >> 6) & 12u))];
-                float2 qp = make_float2(0.f, 0.f), om = make_float2(0.f, 0.f);
-                float2 pv[K], pbv[K];
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    pv[k] = P2[k * (C::PS / 2) + m];
-                    pbv[k] = Pb2[k * (C::PS / 2) + m];
-                    qp = __ffma2_rn(qq[k], pv[k], qp);
-                    om = __ffma2_rn(qq[k], pbv[k], om);
-                }
+                const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
+                const float2 om = make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1]));
                 const float2 pr = __fmul2_rn(qp, om);
                 const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
                 const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);   /* 1/qp, 1/(1-qp) */
                 const float2 z1 = __fmul2_rn(make_float2(a.x, a.y), r1);
                 const float2 z2 = __fmul2_rn(make_float2(a.z, a.w), r2);
                 const float2 w1 = __fmul2_rn(z1, r1), w2 = __fmul2_rn(z2, r2);
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    ga[k] = __ffma2_rn(z1, pv[k], ga[k]);
-                    ga[k] = __ffma2_rn(z2, pbv[k], ga[k]);
-                }
+                dz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);
+                zs = __fadd2_rn(zs, z2);
                 w1p[e] = pack_bf16x2(w1.x, w1.y);
                 w2p[e] = pack_bf16x2(w2.x, w2.y);
             }
             /* A tiles: row tid, k-chunk kc at kc*2048 + 16 tid */
             *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(w1p[0], w1p[1], w1p[2], w1p[3]);
             *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(w2p[0], w2p[1], w2p[2], w2p[3]);
-        }
+            /* gradient: sum (z1 - z2) p_k over the k-chunk's 8 SNPs (broadcast 16-byte loads) */
 #pragma unroll
-        for (int k = 0; k < K; ++k) gd[k] += (double)ga[k].x + (double)ga[k].y;
-        if (c + 1 < nchunk) {
-            qchunk_store<K>(cr, (float *)(sm + C::OFF_P + (s ^ 1) * C::PBUF), sm + C::OFF_G + (s ^ 1) * C::GBUF, tid);
-            if (c + 2 < nchunk) {
-                const int64_t jn = j0 + (int64_t)(c + 2) * MQ_JC;
-                qchunk_load<K>(cr, bed, pitch, p, i0, jn, (int)min((int64_t)MQ_JC, j1 - jn), tid);
+            for (int k = 0; k < K; ++k) {
+                const float4 p0 = *(const float4 *)(Pf + k * C::PS + kc * 8);
+                const float4 p1 = *(const float4 *)(Pf + k * C::PS + kc * 8 + 4);
+                gk[k] = __ffma2_rn(dz[0], make_float2(p0.x, p0.y), gk[k]);
+                gk[k] = __ffma2_rn(dz[1], make_float2(p0.z, p0.w), gk[k]);
+                gk[k] = __ffma2_rn(dz[2], make_float2(p1.x, p1.y), gk[k]);
+                gk[k] = __ffma2_rn(dz[3], make_float2(p1.z, p1.w), gk[k]);
             }
         }
+        const double zsum = (double)zs.x + (double)zs.y;
+#pragma unroll
+        for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y + zsum;
+        /* 6. Hessian MMAs of chunk c: the weight tile and the package's pair-product tiles */
         fence_async_smem();
-        __syncthreads();
-        if (tid == 0 && ok) {
-            tc_fence_after_sync();
-            const uint32_t abase = smem_u32(At), bbase = smem_u32(Bt);
+        tc_fence_before_sync();
+        ok = __syncthreads_and(ok);
+        if (ok) {
+            if (tid == 0) {
+                tc_fence_after_sync();
+                const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
 #pragma unroll
-            for (int term = 0; term < 2; ++term) {
+                for (int term = 0; term < 2; ++term) {
 #pragma unroll
-                for (int ks = 0; ks < 2; ++ks) {
-                    const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
-                    const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
-                    tc_mma_bf16(tmem, ad, bd, idesc, (c > 0 || term > 0 || ks > 0) ? 1u : 0u);
+                    for (int ks = 0; ks < 2; ++ks) {
+                        const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
+                        const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
+                        tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c > 0 || term > 0 || ks > 0) ? 1u : 0u);
+                    }
                 }
+                tc_commit(bar_h);
             }
-            tc_commit(&mbar[s]);
+            ++h_issued;
         }
     }
-    /* wait for the last MMAs of both stages (bounded even after a failed wait, so the TMEM is
-     * not released under an MMA still in flight) */
-    for (int c = max(0, nchunk - 2); c < nchunk; ++c) {
-        const int s = c & 1;
-        if (!mbar_wait_bounded(&mbar[s], (uint32_t)((c >> 1) & 1), ok ? MX_WAIT_LIMIT : 1024u)) {
-            ok = false;
-            if (tid == 0) atomicOr(err, 1);
-        }
+    /* drain: every MMA batch and package copy still in flight is waited for (bounded, and
+     * briefly after a failure) before the TMEM is released and the CTA exits */
+    const uint32_t lim = ok ? MX_WAIT_LIMIT : 1024u;
+    if (h_done < h_issued) {
+        if (mbar_wait_bounded(bar_h, (uint32_t)(h_done & 1), lim)) ++h_done;
+        else { ok = false; atomicOr(err, 1); }
     }
+    if (q_done < q_issued && mbar_wait_bounded(bar_q, (uint32_t)(q_done & 1), ok ? MX_WAIT_LIMIT : 1024u)) ++q_done;
+    if (tid == 0)
+        for (int cw = p_waited; cw < p_issued; ++cw)
+            mbar_wait_bounded(&bar_p[cw % MQ_NPKG], (uint32_t)((cw / MQ_NPKG) & 1), 1024u);
+    ok = __syncthreads_and(ok && h_done == h_issued);
     tc_fence_after_sync();
     double *o = out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E;
     if (valid) {
@@ -303,7 +441,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
 #pragma unroll 1
         for (int c0 = 0; c0 < N; c0 += 16) {
             float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            tmem_ld16(tmem + lane_base + C::COL_H + (uint32_t)c0, v);
             if (valid) {
 #pragma unroll
                 for (int e = 0; e < 16; ++e)
@@ -668,11 +806,21 @@ cudaError_t prepare_mixed_t()
 
 template <int K>
 cudaError_t launch_q_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                             const double *p, const SweepPlan &pl, double *out, int *err, cudaStream_t st)
+                             const double *p, const SweepPlan &pl, double *out, int *err, uint8_t *pkg,
+                             cudaStream_t st)
 {
+    k_q_pack<K><<<(unsigned)((J + MQ_JC - 1) / MQ_JC), 128, 0, st>>>(p, J, pkg);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_q_mixed<K><<<grid, MQ_THREADS, MQ<K>::SMEM, st>>>(bed, I, J, pitch, q, p, pl.slice, out, err);
+    k_sweep_q_mixed<K><<<grid, MQ_THREADS, MQ<K>::SMEM, st>>>(bed, I, J, pitch, q, pkg, pl.slice, out, err);
     return cudaGetLastError();
+}
+
+template <int K>
+size_t q_pkg_bytes_t(int64_t J)
+{
+    return (size_t)((J + MQ_JC - 1) / MQ_JC) * MQ<K>::PKG;
 }
 
 template <int K>
@@ -738,11 +886,19 @@ SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms)
 }
 
 cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                                 const double *p, const SweepPlan &pl, double *out, int *err, cudaStream_t st)
+                                 const double *p, const SweepPlan &pl, double *out, int *err, uint8_t *pkg,
+                                 cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_q_mixed_t<KK>(bed, I, J, pitch, q, p, pl, out, err, st));
+    ADMIX_DISPATCH_K(K, e = launch_q_mixed_t<KK>(bed, I, J, pitch, q, p, pl, out, err, pkg, st));
     return e;
+}
+
+size_t sweep_q_mixed_pkg_bytes(int K, int64_t J)
+{
+    size_t b = 0;
+    ADMIX_DISPATCH_K(K, b = q_pkg_bytes_t<KK>(J));
+    return b;
 }
 
 cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
