@@ -33,7 +33,7 @@ struct admix_ctx {
     double *parts_q = nullptr, *parts_p = nullptr;
     double *U = nullptr, *V = nullptr, *vt = nullptr;
     int32_t *status_q = nullptr, *status_p = nullptr;
-    uint8_t *qpkg = nullptr;         /* mixed Q sweep: per-chunk P packages */
+    uint8_t *pkg = nullptr;          /* mixed sweeps: per-chunk packages of the fixed block */
     double *ll_partial = nullptr, *qn_partial = nullptr;
     DevScalars *sc = nullptr;
     DevScalars *sc_host = nullptr;   /* pinned mirror */
@@ -111,7 +111,7 @@ static void release(admix_ctx *h)
     if (h->iter_graph) cudaGraphExecDestroy(h->iter_graph);
     if (h->iter_graph_def) cudaGraphDestroy(h->iter_graph_def);
     if (h->bed && h->owns_bed) cudaFree(h->bed);
-    void *dps[] = {h->qpkg, h->xbuf, h->parts_q, h->parts_p, h->U, h->V, h->vt, h->status_q,
+    void *dps[] = {h->pkg, h->xbuf, h->parts_q, h->parts_p, h->U, h->V, h->vt, h->status_q,
                    h->status_p, h->ll_partial, h->qn_partial, h->sc, h->counts};
     for (void *p : dps)
         if (p) cudaFree(p);
@@ -195,7 +195,8 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     TRY(dalloc(h, &h->V, (size_t)nx * Q));
     TRY(dalloc(h, &h->vt, (size_t)K * K));
     TRY(dalloc(h, &h->status_q, (size_t)I));
-    if (flags & ADMIX_FLAG_MIXED) TRY(dalloc(h, &h->qpkg, sweep_q_mixed_pkg_bytes(K, J)));
+    if (flags & ADMIX_FLAG_MIXED)
+        TRY(dalloc(h, &h->pkg, std::max(sweep_q_mixed_pkg_bytes(K, J), sweep_p_mixed_pkg_bytes(K, I))));
     TRY(dalloc(h, &h->status_p, (size_t)J));
     TRY(dalloc(h, &h->ll_partial, std::max((size_t)h->llp.gx * h->llp.gy, (size_t)h->llm.gx * h->llm.S)));
     TRY(dalloc(h, &h->qn_partial, (size_t)h->qnp.blocks * (Q * Q + Q)));
@@ -313,7 +314,7 @@ static cudaError_t enq_sweep_q(admix_ctx *h, int wq, int wp, int *S)
     if (h->flags & ADMIX_FLAG_MIXED) {
         *S = h->sqm.S;
         return launch_sweep_q_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sqm, h->parts_q,
-                                    &h->sc->tc_err, h->qpkg, h->st);
+                                    &h->sc->tc_err, h->pkg, h->st);
     }
     *S = h->sq.S;
     return launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
@@ -325,7 +326,7 @@ static cudaError_t enq_sweep_p(admix_ctx *h, int wq, int wp, int *S)
     if (h->flags & ADMIX_FLAG_MIXED) {
         *S = h->spm.S;
         return launch_sweep_p_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->spm, h->parts_p,
-                                    &h->sc->tc_err, h->st);
+                                    &h->sc->tc_err, h->pkg, h->st);
     }
     *S = h->sp.S;
     return launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);

@@ -168,29 +168,6 @@ k_q_pack(const double *__restrict__ p, int64_t J, uint8_t *__restrict__ pkg)
     for (uint32_t t = tid; t < C::PKG / 16; t += 128) dst[t] = ((const uint4 *)buf)[t];
 }
 
-/* genotype bytes of one chunk in registers (loaded a chunk ahead): threads 0..63 hold 8 bytes
- * of each of the SNP pair's two columns (pair t >> 2, bytes 8 (t & 3) .. +7 of the CTA's 32) */
-__device__ __forceinline__ void qgeno_load(uint2 &ga, uint2 &gb, const uint8_t *__restrict__ bed, int64_t pitch,
-                                           int64_t i0, int64_t jc, int n, int tid)
-{
-    if (tid < 64) {
-        const int m = tid >> 2, qb = tid & 3;
-        const size_t off = (size_t)(i0 / 4) + 8 * qb;
-        const uint2 miss = make_uint2(0x55555555u, 0x55555555u);
-        ga = (2 * m < n) ? __ldg((const uint2 *)(bed + (size_t)(jc + 2 * m) * pitch + off)) : miss;
-        gb = (2 * m + 1 < n) ? __ldg((const uint2 *)(bed + (size_t)(jc + 2 * m + 1) * pitch + off)) : miss;
-    }
-}
-
-/* registers -> shared as [pair m][byte b][2] */
-__device__ __forceinline__ void qgeno_store(uint2 ga, uint2 gb, uint8_t *Gb, int tid)
-{
-    if (tid < 64) {
-        const int m = tid >> 2, qb = tid & 3;
-        *(uint4 *)(Gb + (m * 32 + 8 * qb) * 2) = interleave8(ga, gb);
-    }
-}
-
 /* qp / om of the package's chunk into TMEM columns 0..63: 3 * KP/8 TF32 MMAs (one thread) */
 template <int K>
 __device__ __forceinline__ void issue_qp(uint32_t tmem, const uint8_t *sm, const uint8_t *pk)
@@ -212,8 +189,14 @@ __device__ __forceinline__ void issue_qp(uint32_t tmem, const uint8_t *sm, const
     }
 }
 
+/* Warp roles: warps 0-3 are producers (thread = accumulator row), warp 4 is the controller
+ * (bulk copies, genotype staging, MMA issue).  No CTA-wide barrier inside the chunk loop: the
+ * roles hand off through mbarriers.  Every wait is bounded; after a failed wait a thread sets
+ * the shared abort flag and both roles run to the end without waiting. */
+constexpr int MQ_CTA = MQ_THREADS + 32;
+
 template <int K>
-__global__ void __launch_bounds__(MQ_THREADS)
+__global__ void __launch_bounds__(MQ_CTA, (K <= 10 ? 3 : (K <= 12 ? 2 : 1)))
 k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                 const double *__restrict__ q, const uint8_t *__restrict__ pkg, int64_t jslice,
                 double *__restrict__ out, int *__restrict__ err)
@@ -222,28 +205,38 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     constexpr int T = C::T, N = C::N, E = C::E;
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    __shared__ uint64_t mbar[2 + MQ_NPKG];              /* Hessian MMA, qp MMA, package copies */
+    /* qp ready, qp consumed (4 warps), A tile written (4 warps), Hessian done, G staged [2], package [3] */
+    __shared__ uint64_t mbar[6 + MQ_NPKG];
     __shared__ uint32_t tmem_holder;
-    uint64_t *bar_h = &mbar[0], *bar_q = &mbar[1], *bar_p = &mbar[2];
+    __shared__ volatile int abort_flag;
+    uint64_t *bar_qp = &mbar[0], *bar_qfree = &mbar[1], *bar_afull = &mbar[2], *bar_h = &mbar[3];
+    uint64_t *bar_g = &mbar[4], *bar_p = &mbar[6];
 
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp < 4;
     const int64_t i0 = (int64_t)blockIdx.x * 128;
     const int64_t i = i0 + tid;
-    const bool valid = i < I;
+    const bool valid = producer && i < I;
     const int64_t j0 = (int64_t)blockIdx.y * jslice;    /* jslice is a multiple of MQ_JC */
     const int64_t j1 = min(J, j0 + jslice);
     const int nchunk = (int)((j1 - j0 + MQ_JC - 1) / MQ_JC);
     const uint8_t *pk0 = pkg + (size_t)(j0 / MQ_JC) * C::PKG;
-    const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
     uint8_t *At = sm + C::OFF_A;
 
-    if (warp == 0) tmem_alloc_warp(&tmem_holder, C::NCOLS);
+    if (warp == 4) tmem_alloc_warp(&tmem_holder, C::NCOLS);
     if (tid == 0) {
-        for (int b = 0; b < 2 + MQ_NPKG; ++b) mbar_init(&mbar[b], 1);
+        mbar_init(bar_qp, 1);
+        mbar_init(bar_qfree, 4);
+        mbar_init(bar_afull, 4);
+        mbar_init(bar_h, 1);
+        mbar_init(&bar_g[0], 1);
+        mbar_init(&bar_g[1], 1);
+        for (int b = 0; b < MQ_NPKG; ++b) mbar_init(&bar_p[b], 1);
+        abort_flag = 0;
         mbar_fence_init();
     }
-    code_table_init((float4 *)(sm + C::OFF_TAB), tid, MQ_THREADS);
-    {   /* this thread's row of the TF32 Q tile: columns 0..K-1 hi, KP..KP+K-1 lo, the rest zero */
+    code_table_init((float4 *)(sm + C::OFF_TAB), tid, MQ_CTA);
+    if (producer) {   /* this thread's row of the TF32 Q tile: columns 0..K-1 hi, KP..KP+K-1 lo */
         float hv[C::KP], lv[C::KP];
 #pragma unroll
         for (int k = 0; k < C::KP; ++k) {
@@ -256,20 +249,400 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             *(float4 *)(sm + C::OFF_QA + kmaj_off(tid, C::KP + f, C::QA_LBO)) = make_float4(lv[f], lv[f + 1], lv[f + 2], lv[f + 3]);
         }
     }
-    uint2 ga = make_uint2(0u, 0u), gb = make_uint2(0u, 0u);
-    if (nchunk > 0) {
-        qgeno_load(ga, gb, bed, pitch, i0, j0, (int)min((int64_t)MQ_JC, j1 - j0), tid);
-        qgeno_store(ga, gb, sm + C::OFF_G, tid);
-    }
-    if (nchunk > 1) qgeno_load(ga, gb, bed, pitch, i0, j0 + MQ_JC, (int)min((int64_t)MQ_JC, j1 - j0 - MQ_JC), tid);
     fence_async_smem();
     tc_fence_before_sync();
-    __syncthreads();                                    /* barriers initialised, Q tile staged */
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tmem = tmem_holder;
+    bool ok = true;
+    auto wait = [&](uint64_t *b, uint32_t parity) -> bool {
+        if (!ok) return false;
+        for (uint32_t n = 0; n < MX_WAIT_LIMIT; ++n) {
+            if (mbar_try_wait(b, parity)) return true;
+            if ((n & 255u) == 255u && abort_flag) break;
+        }
+        ok = false;
+        abort_flag = 1;
+        atomicOr(err, 1);
+        return false;
+    };
+
+    if (!producer) {
+        /* ---------------------------------------------------------------- controller warp */
+        const bool leader = lane == 0;
+        /* genotypes of chunk c into G buffer c & 1: lane l loads SNP jc + l (32 bytes: the CTA's 128
+         * individuals); lanes 2m, 2m+1 exchange and write pair m interleaved as [byte][2] */
+        auto stage_g = [&](int c) {
+            const int64_t jc = j0 + (int64_t)c * MQ_JC;
+            uint4 a0 = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), a1 = a0;
+            if (jc + lane < j1) {
+                const uint4 *src = (const uint4 *)(bed + (size_t)(jc + lane) * pitch + (size_t)(i0 / 4));
+                a0 = __ldg(src);
+                a1 = __ldg(src + 1);
+            }
+            uint4 b0, b1;                                   /* the partner lane's bytes */
+            b0.x = __shfl_xor_sync(0xffffffffu, a0.x, 1); b0.y = __shfl_xor_sync(0xffffffffu, a0.y, 1);
+            b0.z = __shfl_xor_sync(0xffffffffu, a0.z, 1); b0.w = __shfl_xor_sync(0xffffffffu, a0.w, 1);
+            b1.x = __shfl_xor_sync(0xffffffffu, a1.x, 1); b1.y = __shfl_xor_sync(0xffffffffu, a1.y, 1);
+            b1.z = __shfl_xor_sync(0xffffffffu, a1.z, 1); b1.w = __shfl_xor_sync(0xffffffffu, a1.w, 1);
+            const bool even = (lane & 1) == 0;
+            /* even lane: bytes 0..15 of (own, partner); odd lane: bytes 16..31 of (partner, own) */
+            const uint4 s0 = even ? a0 : b1, s1 = even ? b0 : a1;   /* SNP 2m bytes, SNP 2m+1 bytes */
+            uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF + (lane >> 1) * 64 + (even ? 0 : 32);
+            *(uint4 *)(Gb) = interleave8(make_uint2(s0.x, s0.y), make_uint2(s1.x, s1.y));
+            *(uint4 *)(Gb + 16) = interleave8(make_uint2(s0.z, s0.w), make_uint2(s1.z, s1.w));
+            __syncwarp();
+            if (leader) mbar_arrive(&bar_g[c & 1]);
+        };
+        auto copy_pkg = [&](int c) {
+            if (leader) {
+                mbar_arrive_expect_tx(&bar_p[c % MQ_NPKG], C::PKG);
+                bulk_g2s(sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG, pk0 + (size_t)c * C::PKG, C::PKG,
+                         &bar_p[c % MQ_NPKG]);
+            }
+        };
+        for (int c = 0; c < min(nchunk, MQ_NPKG); ++c) copy_pkg(c);
+        if (nchunk > 0) stage_g(0);
+        if (nchunk > 1) stage_g(1);
+        if (nchunk > 0 && wait(&bar_p[0], 0u) && leader) {
+            tc_fence_after_sync();
+            issue_qp<K>(tmem, sm, sm + C::OFF_PKG);
+            tc_commit(bar_qp);
+        }
+        constexpr uint32_t idesc = idesc_bf16_f32(128, N);
+        for (int c = 0; c < nchunk && ok; ++c) {
+            /* qp of chunk c+1 once its package landed and the producers read qp of chunk c */
+            if (c + 1 < nchunk) {
+                const int cn = c + 1;
+                const bool landed = wait(&bar_p[cn % MQ_NPKG], (uint32_t)((cn / MQ_NPKG) & 1));
+                if (landed && wait(bar_qfree, (uint32_t)(c & 1)) && leader) {
+                    tc_fence_after_sync();
+                    issue_qp<K>(tmem, sm, sm + C::OFF_PKG + (cn % MQ_NPKG) * C::PKG);
+                    tc_commit(bar_qp);
+                }
+            }
+            /* Hessian of chunk c once the producers wrote its weight tile */
+            if (wait(bar_afull, (uint32_t)(c & 1))) {
+                if (leader) {
+                    tc_fence_after_sync();
+                    const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
+                    const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
+#pragma unroll
+                    for (int term = 0; term < 2; ++term) {
+#pragma unroll
+                        for (int ks = 0; ks < 2; ++ks) {
+                            const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
+                            const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
+                            tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c > 0 || term > 0 || ks > 0) ? 1u : 0u);
+                        }
+                    }
+                    tc_commit(bar_h);
+                }
+                /* the producers are done with G buffer c & 1: stage chunk c+2 into it */
+                if (c + 2 < nchunk) stage_g(c + 2);
+            }
+            /* package c is free once the Hessian of chunk c is done: fetch chunk c+3 into it */
+            if (c + MQ_NPKG < nchunk && wait(bar_h, (uint32_t)(c & 1))) {
+                fence_async_smem();
+                copy_pkg(c + MQ_NPKG);
+            }
+        }
+    } else {
+        /* ---------------------------------------------------------------- producer warps */
+        const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
+        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        const int sh = valid ? (int)(i & 3) * 2 : 0;
+        const uint32_t gmask = valid ? 0xFFFFu : 0u;    /* rows beyond I read code pair 01|01 */
+        double gd[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) gd[k] = 0.0;
+        for (int c = 0; c < nchunk && ok; ++c) {
+            const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
+            const float *Pf = (const float *)(pk + C::PK_PF);
+            const uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF;
+            uint32_t rq[32], ro[32];
+            if (!wait(bar_qp, (uint32_t)(c & 1))) break;
+            tc_fence_after_sync();
+            tmem_ld32_nowait(tmem + lane_base, rq);
+            tmem_ld32_nowait(tmem + lane_base + 32u, ro);
+            tmem_wait_ld();
+            tc_fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_qfree);
+            if (!wait(&bar_p[c % MQ_NPKG], (uint32_t)((c / MQ_NPKG) & 1))) break;
+            if (!wait(&bar_g[c & 1], (uint32_t)((c >> 1) & 1))) break;
+            if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the weight tile is free */
+            const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);
+            float2 gk[K], zs = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int kc = 0; kc < 4; ++kc) {
+                uint32_t w1p[4], w2p[4];
+                float2 dz[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int m = kc * 4 + e;
+                    const uint32_t gw = ((uint32_t)G2[m * 32] & gmask) | (~gmask & 0x5555u);
+                    const uint32_t tb = gw >> sh;
+                    const float4 a = tab[8 * ((tb & 3u) | ((tb >> 6) & 12u))];
+                    const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
+                    const float2 om = make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1]));
+                    const float2 pr = __fmul2_rn(qp, om);
+                    const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
+                    const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
+                    const float2 z1 = __fmul2_rn(make_float2(a.x, a.y), r1);
+                    const float2 z2 = __fmul2_rn(make_float2(a.z, a.w), r2);
+                    const float2 w1 = __fmul2_rn(z1, r1), w2 = __fmul2_rn(z2, r2);
+                    dz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);
+                    zs = __fadd2_rn(zs, z2);
+                    w1p[e] = pack_bf16x2(w1.x, w1.y);
+                    w2p[e] = pack_bf16x2(w2.x, w2.y);
+                }
+                *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(w1p[0], w1p[1], w1p[2], w1p[3]);
+                *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(w2p[0], w2p[1], w2p[2], w2p[3]);
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const float4 p0 = *(const float4 *)(Pf + k * C::PS + kc * 8);
+                    const float4 p1 = *(const float4 *)(Pf + k * C::PS + kc * 8 + 4);
+                    gk[k] = __ffma2_rn(dz[0], make_float2(p0.x, p0.y), gk[k]);
+                    gk[k] = __ffma2_rn(dz[1], make_float2(p0.z, p0.w), gk[k]);
+                    gk[k] = __ffma2_rn(dz[2], make_float2(p1.x, p1.y), gk[k]);
+                    gk[k] = __ffma2_rn(dz[3], make_float2(p1.z, p1.w), gk[k]);
+                }
+            }
+            const double zsum = (double)zs.x + (double)zs.y;
+#pragma unroll
+            for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y + zsum;
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_afull);
+        }
+        if (nchunk > 0) wait(bar_h, (uint32_t)((nchunk - 1) & 1));   /* the last Hessian MMAs */
+        if (valid) {
+            double *o = out + ((size_t)blockIdx.y * I + i) * E;
+#pragma unroll
+            for (int k = 0; k < K; ++k) o[T + k] = gd[k];
+        }
+    }
+    /* every role is past its loop; after a failure, give MMAs and copies still in flight a
+     * bounded moment before the TMEM is read and released */
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == MQ_THREADS) {
+        mbar_wait_bounded(bar_h, 0u, 1024u);
+        mbar_wait_bounded(bar_h, 1u, 1024u);
+        mbar_wait_bounded(bar_qp, 0u, 1024u);
+        mbar_wait_bounded(bar_qp, 1u, 1024u);
+        for (int b = 0; b < MQ_NPKG; ++b) { mbar_wait_bounded(&bar_p[b], 0u, 1024u); mbar_wait_bounded(&bar_p[b], 1u, 1024u); }
+    }
+    __syncthreads();
+    tc_fence_after_sync();
+    if (producer) {
+        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        if (nchunk > 0) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + lane_base + C::COL_H + (uint32_t)c0, v);
+                if (valid) {
+                    double *o = out + ((size_t)blockIdx.y * I + i) * E;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        if (c0 + e < T) o[c0 + e] = ok ? (double)v[e] : __longlong_as_double(0x7ff8000000000000LL);
+                }
+            }
+        } else if (valid) {
+            double *o = out + ((size_t)blockIdx.y * I + i) * E;
+            for (int e = 0; e < T; ++e) o[e] = 0.0;
+        }
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 4) tmem_dealloc_warp(tmem, C::NCOLS);
+}
+
+/* ===================================================================== P side
+ *
+ * Mirror of the Q side with the roles of the axes swapped: rows = 128 SNPs, reduction over
+ * chunks of 32 individuals.  Per chunk:
+ *   qp, om     D[128 x 32] = Ptile * Qchunk^T and (1-P)tile * Qchunk^T, TF32 split form;
+ *   Hessian    D[128 x N] += C * QQ^T in BF16, C = nm (g/qp^2 + (2-g)/(1-qp)^2);
+ * and per cell on the CUDA cores the code (from the thread's own genotype word), one reciprocal
+ * and the FP32 gradient sum_i nm (g/qp - (2-g)/(1-qp)) q_k, added into FP64 per chunk.  The
+ * Q-derived tiles of each chunk (QQ in BF16, Q split into TF32 hi / lo, q in FP32) are built
+ * once per sweep by k_p_pack and fetched with one bulk copy per chunk. */
+
+constexpr int MP_IC = 32;          /* individuals per chunk = 2 BF16 MMA K-steps */
+constexpr int MP_THREADS = 128;    /* one thread per SNP = accumulator row */
+constexpr int MP_NPKG = 3;
+
+template <int K>
+struct MP {
+    static constexpr int T = K * (K + 1) / 2;
+    static constexpr int N = ((T + 15) / 16) * 16;
+    static constexpr int KP = ((K + 7) / 8) * 8;
+    static constexpr uint32_t COL_OM = 32, COL_H = 64;          /* TMEM: qp 0..31, om 32..63, Hessian */
+    static constexpr uint32_t NCOLS = tmem_cols_for(COL_H + N);
+    static constexpr int E = T + K;
+    static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* BF16 C tile: 8 KB */
+    static constexpr uint32_t B_BYTES = N * MP_IC * 2;          /* BF16 QQ tile */
+    static constexpr uint32_t PA_BYTES = 128 * 2 * KP * 4;      /* TF32 P tile [hi | lo] (and 1-P) */
+    static constexpr uint32_t QB_BYTES = MP_IC * 2 * KP * 4;    /* TF32 Q chunk [hi | lo] */
+    static constexpr int QS = MP_IC + 4;                        /* FP32 q row stride (floats) */
+    static constexpr uint32_t PK_QB = B_BYTES;
+    static constexpr uint32_t PK_QF = PK_QB + QB_BYTES;
+    static constexpr uint32_t PKG = PK_QF + K * QS * 4;
+    static constexpr uint32_t OFF_A = 0;
+    static constexpr uint32_t OFF_PKG = A_BYTES;
+    static constexpr uint32_t OFF_PA = OFF_PKG + MP_NPKG * PKG; /* P tile, then (1-P) tile */
+    static constexpr uint32_t OFF_TAB = OFF_PA + 2 * PA_BYTES;
+    static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024;
+    static constexpr uint32_t A_LBO = 2048, A_SBO = 128;
+    static constexpr uint32_t B_LBO = 16 * N, B_SBO = 128;
+    static constexpr uint32_t PA_LBO = 2048, QB_LBO = 512, T_SBO = 128;
+    static_assert(PKG % 16 == 0 && OFF_PA % 16 == 0, "bulk copies and descriptors need 16-byte alignment");
+};
+
+/* One package per 32-individual chunk of the whole individual range (block = chunk).
+ * Individuals beyond I get q = 1/K; their genotype codes read as missing. */
+template <int K>
+__global__ void __launch_bounds__(128)
+k_p_pack(const double *__restrict__ q, int64_t I, uint8_t *__restrict__ pkg)
+{
+    using C = MP<K>;
+    constexpr int T = C::T, N = C::N;
+    __shared__ __align__(16) uint8_t buf[C::PKG];
+    const int tid = threadIdx.x;
+    const int64_t ic = (int64_t)blockIdx.x * MP_IC;
+    float *qf = (float *)(buf + C::PK_QF);
+    for (uint32_t t = tid; t < C::PKG / 16; t += 128) ((uint4 *)buf)[t] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    for (int t = tid; t < K * MP_IC; t += 128) {
+        const int ii = t / K, k = t - ii * K;
+        const float a = (ic + ii < I) ? (float)q[(size_t)K * ic + t] : 1.0f / K;
+        qf[k * C::QS + ii] = a;
+        float h, l;
+        tf32_split(a, h, l);
+        *(float *)(buf + C::PK_QB + kmaj_off(ii, k, C::QB_LBO)) = h;
+        *(float *)(buf + C::PK_QB + kmaj_off(ii, C::KP + k, C::QB_LBO)) = l;
+    }
+    __syncthreads();
+    /* QQ tile: task (kc, nn) writes pair nn's 8 individuals of k-chunk kc at kc*16N + 16nn */
+    for (int t = tid; t < 4 * N; t += 128) {
+        const int kc = t / N, nn = t - kc * N;
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+        if (nn < T) {
+            int ka, kb;
+            tri_pair(nn, ka, kb);
+            const float *src = qf + kc * 8;
+            const float4 a0 = *(const float4 *)(src + ka * C::QS), a1 = *(const float4 *)(src + ka * C::QS + 4);
+            const float4 b0 = *(const float4 *)(src + kb * C::QS), b1 = *(const float4 *)(src + kb * C::QS + 4);
+            w[0] = pack_bf16x2(a0.x * b0.x, a0.y * b0.y);
+            w[1] = pack_bf16x2(a0.z * b0.z, a0.w * b0.w);
+            w[2] = pack_bf16x2(a1.x * b1.x, a1.y * b1.y);
+            w[3] = pack_bf16x2(a1.z * b1.z, a1.w * b1.w);
+        }
+        *(uint4 *)(buf + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    __syncthreads();
+    uint4 *dst = (uint4 *)(pkg + (size_t)blockIdx.x * C::PKG);
+    for (uint32_t t = tid; t < C::PKG / 16; t += 128) dst[t] = ((const uint4 *)buf)[t];
+}
+
+/* qp (TMEM columns 0..31) and om (32..63) of the package's chunk: 2 * 3 * KP/8 TF32 MMAs */
+template <int K>
+__device__ __forceinline__ void issue_qp_p(uint32_t tmem, const uint8_t *sm, const uint8_t *pk)
+{
+    using C = MP<K>;
+    const uint32_t a0 = smem_u32(sm + C::OFF_PA), b = smem_u32(pk + C::PK_QB);
+    constexpr uint32_t id = idesc_tf32_f32(128, MP_IC);
+    constexpr uint32_t alo = (C::KP / 4) * C::PA_LBO, blo = (C::KP / 4) * C::QB_LBO;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const uint32_t a = a0 + t * C::PA_BYTES, d = tmem + (t ? C::COL_OM : 0u);
+#pragma unroll
+        for (int s = 0; s < C::KP / 8; ++s) {
+            const uint32_t ao = a + s * 2 * C::PA_LBO, bo = b + s * 2 * C::QB_LBO;
+            const uint64_t ahi = umma_desc_kmajor(ao, C::PA_LBO, C::T_SBO);
+            const uint64_t alw = umma_desc_kmajor(ao + alo, C::PA_LBO, C::T_SBO);
+            const uint64_t bhi = umma_desc_kmajor(bo, C::QB_LBO, C::T_SBO);
+            const uint64_t blw = umma_desc_kmajor(bo + blo, C::QB_LBO, C::T_SBO);
+            tc_mma_tf32(d, ahi, bhi, id, s > 0 ? 1u : 0u);
+            tc_mma_tf32(d, alw, bhi, id, 1u);
+            tc_mma_tf32(d, ahi, blw, id, 1u);
+        }
+    }
+}
+
+/* 32 individuals' codes of SNP column j from individual ic (a multiple of 32) */
+__device__ __forceinline__ uint2 col_load32(const uint8_t *__restrict__ bed, int64_t pitch, int64_t j, bool valid,
+                                            int64_t ic)
+{
+    return valid ? __ldg((const uint2 *)(bed + (size_t)j * pitch + (size_t)(ic / 4)))
+                 : make_uint2(0x55555555u, 0x55555555u);
+}
+
+template <int K>
+__global__ void __launch_bounds__(MP_THREADS, (K <= 10 ? 4 : 2))
+k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
+                const uint8_t *__restrict__ pkg, const double *__restrict__ p, int64_t islice,
+                double *__restrict__ out, int *__restrict__ err)
+{
+    using C = MP<K>;
+    constexpr int T = C::T, N = C::N, E = C::E;
+    extern __shared__ __align__(1024) uint8_t smraw[];
+    uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    __shared__ uint64_t mbar[2 + MP_NPKG];              /* Hessian MMA, qp MMA, package copies */
+    __shared__ uint32_t tmem_holder;
+    uint64_t *bar_h = &mbar[0], *bar_q = &mbar[1], *bar_p = &mbar[2];
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int64_t j = (int64_t)blockIdx.x * 128 + tid;
+    const bool valid = j < J;
+    const int64_t ia = (int64_t)blockIdx.y * islice;    /* islice is a multiple of MP_IC */
+    const int64_t ib = min(I, ia + islice);
+    const int nchunk = (int)((ib - ia + MP_IC - 1) / MP_IC);
+    const uint8_t *pk0 = pkg + (size_t)(ia / MP_IC) * C::PKG;
+    const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
+    uint8_t *At = sm + C::OFF_A;
+
+    if (warp == 0) tmem_alloc_warp(&tmem_holder, C::NCOLS);
+    if (tid == 0) {
+        for (int b = 0; b < 2 + MP_NPKG; ++b) mbar_init(&mbar[b], 1);
+        mbar_fence_init();
+    }
+    code_table_init((float4 *)(sm + C::OFF_TAB), tid, MP_THREADS);
+    {   /* this thread's rows of the TF32 P and (1-P) tiles */
+        float hv[C::KP], lv[C::KP], hb[C::KP], lb[C::KP];
+#pragma unroll
+        for (int k = 0; k < C::KP; ++k) {
+            hv[k] = lv[k] = hb[k] = lb[k] = 0.f;
+            if (k < K) {
+                const double pv = valid ? p[(size_t)K * j + k] : 0.5;
+                tf32_split((float)pv, hv[k], lv[k]);
+                tf32_split((float)(1.0 - pv), hb[k], lb[k]);
+            }
+        }
+        uint8_t *pa = sm + C::OFF_PA, *pb = pa + C::PA_BYTES;
+#pragma unroll
+        for (int f = 0; f < C::KP; f += 4) {
+            *(float4 *)(pa + kmaj_off(tid, f, C::PA_LBO)) = make_float4(hv[f], hv[f + 1], hv[f + 2], hv[f + 3]);
+            *(float4 *)(pa + kmaj_off(tid, C::KP + f, C::PA_LBO)) = make_float4(lv[f], lv[f + 1], lv[f + 2], lv[f + 3]);
+            *(float4 *)(pb + kmaj_off(tid, f, C::PA_LBO)) = make_float4(hb[f], hb[f + 1], hb[f + 2], hb[f + 3]);
+            *(float4 *)(pb + kmaj_off(tid, C::KP + f, C::PA_LBO)) = make_float4(lb[f], lb[f + 1], lb[f + 2], lb[f + 3]);
+        }
+    }
+    uint2 gcur = make_uint2(0x55555555u, 0x55555555u), gnext = gcur;
+    if (nchunk > 0) gcur = col_load32(bed, pitch, j, valid, ia);
+    if (nchunk > 1) gnext = col_load32(bed, pitch, j, valid, ia + MP_IC);
+    fence_async_smem();
+    tc_fence_before_sync();
+    __syncthreads();
     tc_fence_after_sync();
     const uint32_t tmem = tmem_holder;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
     bool ok = true;
-    int p_issued = 0, p_waited = 0;                     /* package copies (thread 0's view) */
+    int p_issued = 0, p_waited = 0;
     if (tid == 0) {
         for (int c = 0; c < min(nchunk, 2); ++c) {
             mbar_arrive_expect_tx(&bar_p[c], C::PKG);
@@ -279,7 +652,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         if (nchunk > 0) {
             if (mbar_wait_bounded(&bar_p[0], 0u, MX_WAIT_LIMIT)) {
                 ++p_waited;
-                issue_qp<K>(tmem, sm, sm + C::OFF_PKG);
+                issue_qp_p<K>(tmem, sm, sm + C::OFF_PKG);
                 tc_commit(bar_q);
             } else {
                 ok = false;
@@ -293,15 +666,12 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     double gd[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) gd[k] = 0.0;
-    const int sh = valid ? (int)(i & 3) * 2 : 0;
-    const uint32_t gmask = valid ? 0xFFFFu : 0u;        /* rows beyond I read code pair 01|01 */
     constexpr uint32_t idesc = idesc_bf16_f32(128, N);
 
     for (int c = 0; c < nchunk; ++c) {
-        const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
-        const float *Pf = (const float *)(pk + C::PK_PF);
-        const uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF;
-        /* 1. qp and 1 - qp of this thread's individual and the chunk's 32 SNPs */
+        const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
+        const float *Qf = (const float *)(pk + C::PK_QF);
+        /* 1. qp and 1 - qp of this thread's SNP and the chunk's 32 individuals */
         uint32_t rq[32], ro[32];
         if (ok && q_done < q_issued) {
             if (mbar_wait_bounded(bar_q, (uint32_t)(q_done & 1), MX_WAIT_LIMIT)) ++q_done;
@@ -309,32 +679,23 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         }
         tc_fence_after_sync();
         tmem_ld32_nowait(tmem + lane_base, rq);
-        tmem_ld32_nowait(tmem + lane_base + 32u, ro);
+        tmem_ld32_nowait(tmem + lane_base + C::COL_OM, ro);
         tmem_wait_ld();
-        /* 2. the Hessian MMAs of chunk c-1 are done: the weight tile and package c-1 are free */
+        /* 2. the Hessian MMAs of chunk c-1 are done: the C tile and package c-1 are free */
         if (ok && h_done < h_issued) {
             if (mbar_wait_bounded(bar_h, (uint32_t)(h_done & 1), MX_WAIT_LIMIT)) ++h_done;
             else { ok = false; atomicOr(err, 1); }
         }
-        /* 3. genotypes of chunk c+1 to shared memory, chunk c+2 to registers */
-        if (c + 1 < nchunk) {
-            qgeno_store(ga, gb, sm + C::OFF_G + ((c + 1) & 1) * C::GBUF, tid);
-            if (c + 2 < nchunk) {
-                const int64_t jn = j0 + (int64_t)(c + 2) * MQ_JC;
-                qgeno_load(ga, gb, bed, pitch, i0, jn, (int)min((int64_t)MQ_JC, j1 - jn), tid);
-            }
-        }
-        fence_async_smem();
         tc_fence_before_sync();
         ok = __syncthreads_and(ok);
-        /* 4. qp MMA of chunk c+1 (its package landed), copy of package c+2 */
+        /* 3. qp / om MMAs of chunk c+1 (its package landed), copy of package c+2 */
         if (ok && c + 1 < nchunk) {
             if (tid == 0) {
                 tc_fence_after_sync();
                 const int cn = c + 1;
-                if (mbar_wait_bounded(&bar_p[cn % MQ_NPKG], (uint32_t)((cn / MQ_NPKG) & 1), MX_WAIT_LIMIT)) {
+                if (mbar_wait_bounded(&bar_p[cn % MP_NPKG], (uint32_t)((cn / MP_NPKG) & 1), MX_WAIT_LIMIT)) {
                     ++p_waited;
-                    issue_qp<K>(tmem, sm, sm + C::OFF_PKG + (cn % MQ_NPKG) * C::PKG);
+                    issue_qp_p<K>(tmem, sm, sm + C::OFF_PKG + (cn % MP_NPKG) * C::PKG);
                     tc_commit(bar_q);
                 } else {
                     ok = false;
@@ -343,60 +704,56 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 if (ok && c + 2 < nchunk) {
                     const int cm = c + 2;
                     fence_async_smem();
-                    mbar_arrive_expect_tx(&bar_p[cm % MQ_NPKG], C::PKG);
-                    bulk_g2s(sm + C::OFF_PKG + (cm % MQ_NPKG) * C::PKG, pk0 + (size_t)cm * C::PKG, C::PKG,
-                             &bar_p[cm % MQ_NPKG]);
+                    mbar_arrive_expect_tx(&bar_p[cm % MP_NPKG], C::PKG);
+                    bulk_g2s(sm + C::OFF_PKG + (cm % MP_NPKG) * C::PKG, pk0 + (size_t)cm * C::PKG, C::PKG,
+                             &bar_p[cm % MP_NPKG]);
                     ++p_issued;
                 }
             }
             ++q_issued;
         }
-        /* 5. producer: the chunk's 32 SNPs as 16 pairs, 4 pairs per BF16 k-chunk */
-        const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);  /* [pair][byte]: both SNPs */
-        float2 gk[K], zs = make_float2(0.f, 0.f);
+        /* 4. producer: 16 individual pairs, 4 per BF16 k-chunk */
+        float2 gk[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int kc = 0; kc < 4; ++kc) {
-            uint32_t w1p[4], w2p[4];
-            float2 dz[4];
+            uint32_t cp[4];
+            float2 zz[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                const int m = kc * 4 + e;                       /* SNPs 2m, 2m+1 of the chunk */
-                const uint32_t gw = ((uint32_t)G2[m * 32] & gmask) | (~gmask & 0x5555u);
-                const uint32_t tb = gw >> sh;
-                const float4 a = tab[8 * ((tb & 3u) | ((tb >> 6) & 12u))];
+                const int m = kc * 4 + e;                       /* individuals 2m, 2m+1 of the chunk */
+                const uint32_t w = (m < 8) ? gcur.x : gcur.y;
+                const float4 a = tab[8 * ((w >> (4 * (m & 7))) & 15u)];
                 const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
                 const float2 om = make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1]));
                 const float2 pr = __fmul2_rn(qp, om);
                 const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
-                const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);   /* 1/qp, 1/(1-qp) */
+                const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
                 const float2 z1 = __fmul2_rn(make_float2(a.x, a.y), r1);
                 const float2 z2 = __fmul2_rn(make_float2(a.z, a.w), r2);
-                const float2 w1 = __fmul2_rn(z1, r1), w2 = __fmul2_rn(z2, r2);
-                dz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);
-                zs = __fadd2_rn(zs, z2);
-                w1p[e] = pack_bf16x2(w1.x, w1.y);
-                w2p[e] = pack_bf16x2(w2.x, w2.y);
+                const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
+                zz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);              /* nm (g/qp - (2-g)/(1-qp)) */
+                cp[e] = pack_bf16x2(cw.x, cw.y);
             }
-            /* A tiles: row tid, k-chunk kc at kc*2048 + 16 tid */
-            *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(w1p[0], w1p[1], w1p[2], w1p[3]);
-            *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(w2p[0], w2p[1], w2p[2], w2p[3]);
-            /* gradient: sum (z1 - z2) p_k over the k-chunk's 8 SNPs (broadcast 16-byte loads) */
+            *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                const float4 p0 = *(const float4 *)(Pf + k * C::PS + kc * 8);
-                const float4 p1 = *(const float4 *)(Pf + k * C::PS + kc * 8 + 4);
-                gk[k] = __ffma2_rn(dz[0], make_float2(p0.x, p0.y), gk[k]);
-                gk[k] = __ffma2_rn(dz[1], make_float2(p0.z, p0.w), gk[k]);
-                gk[k] = __ffma2_rn(dz[2], make_float2(p1.x, p1.y), gk[k]);
-                gk[k] = __ffma2_rn(dz[3], make_float2(p1.z, p1.w), gk[k]);
+                const float4 q0 = *(const float4 *)(Qf + k * C::QS + kc * 8);
+                const float4 q1 = *(const float4 *)(Qf + k * C::QS + kc * 8 + 4);
+                gk[k] = __ffma2_rn(zz[0], make_float2(q0.x, q0.y), gk[k]);
+                gk[k] = __ffma2_rn(zz[1], make_float2(q0.z, q0.w), gk[k]);
+                gk[k] = __ffma2_rn(zz[2], make_float2(q1.x, q1.y), gk[k]);
+                gk[k] = __ffma2_rn(zz[3], make_float2(q1.z, q1.w), gk[k]);
             }
         }
-        const double zsum = (double)zs.x + (double)zs.y;
 #pragma unroll
-        for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y + zsum;
-        /* 6. Hessian MMAs of chunk c: the weight tile and the package's pair-product tiles */
+        for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y;
+        if (c + 1 < nchunk) {
+            gcur = gnext;
+            if (c + 2 < nchunk) gnext = col_load32(bed, pitch, j, valid, ia + (int64_t)(c + 2) * MP_IC);
+        }
+        /* 5. Hessian MMAs of chunk c */
         fence_async_smem();
         tc_fence_before_sync();
         ok = __syncthreads_and(ok);
@@ -405,21 +762,16 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 tc_fence_after_sync();
                 const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
 #pragma unroll
-                for (int term = 0; term < 2; ++term) {
-#pragma unroll
-                    for (int ks = 0; ks < 2; ++ks) {
-                        const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
-                        const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
-                        tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c > 0 || term > 0 || ks > 0) ? 1u : 0u);
-                    }
+                for (int ks = 0; ks < 2; ++ks) {
+                    const uint64_t ad = umma_desc_kmajor(abase + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
+                    const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
+                    tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
                 }
                 tc_commit(bar_h);
             }
             ++h_issued;
         }
     }
-    /* drain: every MMA batch and package copy still in flight is waited for (bounded, and
-     * briefly after a failure) before the TMEM is released and the CTA exits */
     const uint32_t lim = ok ? MX_WAIT_LIMIT : 1024u;
     if (h_done < h_issued) {
         if (mbar_wait_bounded(bar_h, (uint32_t)(h_done & 1), lim)) ++h_done;
@@ -428,16 +780,15 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     if (q_done < q_issued && mbar_wait_bounded(bar_q, (uint32_t)(q_done & 1), ok ? MX_WAIT_LIMIT : 1024u)) ++q_done;
     if (tid == 0)
         for (int cw = p_waited; cw < p_issued; ++cw)
-            mbar_wait_bounded(&bar_p[cw % MQ_NPKG], (uint32_t)((cw / MQ_NPKG) & 1), 1024u);
+            mbar_wait_bounded(&bar_p[cw % MP_NPKG], (uint32_t)((cw / MP_NPKG) & 1), 1024u);
     ok = __syncthreads_and(ok && h_done == h_issued);
     tc_fence_after_sync();
-    double *o = out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E;
+    double *o = out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E;
     if (valid) {
 #pragma unroll
         for (int k = 0; k < K; ++k) o[T + k] = gd[k];
     }
     if (nchunk > 0) {
-        /* Hessian: warp w reads TMEM lanes 32w .. 32w+31 (= this thread's row) */
 #pragma unroll 1
         for (int c0 = 0; c0 < N; c0 += 16) {
             float v[16];
@@ -456,31 +807,6 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     if (warp == 0) tmem_dealloc_warp(tmem, C::NCOLS);
 }
 
-/* ===================================================================== P side
- * Thread = SNP row; individuals in chunks of 64 (one 16-byte load of the thread's own column);
- * the 4 bits of an individual pair index the code table directly. */
-constexpr int MP_IC = 64;
-constexpr int MP_THREADS = 128;
-
-template <int K>
-struct MP {
-    static constexpr int T = K * (K + 1) / 2;
-    static constexpr int N = ((T + 15) / 16) * 16;
-    static constexpr uint32_t NCOLS = tmem_cols_for(N);
-    static constexpr int E = T + K;
-    static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* one BF16 weight tile: 16 KB */
-    static constexpr uint32_t B_BYTES = N * MP_IC * 2;
-    static constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
-    static constexpr int QS = MP_IC + 2;                        /* q row stride (floats) */
-    static constexpr uint32_t QBUF = K * QS * 4;                /* q of one chunk, FP32 [k][i] */
-    static constexpr uint32_t OFF_Q = 2 * STAGE_BYTES;
-    static constexpr uint32_t OFF_TAB = OFF_Q + 2 * QBUF;
-    static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024;
-    static constexpr uint32_t A_LBO = 2048, A_SBO = 128;
-    static constexpr uint32_t B_LBO = 16 * N, B_SBO = 128;
-    static constexpr int PREF_Q = (K * MP_IC + MP_THREADS - 1) / MP_THREADS;
-};
-
 /* 64 individuals' codes of SNP column j from individual ic (a multiple of 64) */
 __device__ __forceinline__ uint4 col_load64(const uint8_t *__restrict__ bed, int64_t pitch, int64_t j, bool valid,
                                             int64_t ic)
@@ -489,202 +815,11 @@ __device__ __forceinline__ uint4 col_load64(const uint8_t *__restrict__ bed, int
                  : make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
 }
 
+/* 4-bit code pair of individuals 2m, 2m+1 in a 64-individual word */
 __device__ __forceinline__ uint32_t pair_code(const uint4 &g, int m)
 {
     const uint32_t w = (m < 8) ? g.x : ((m < 16) ? g.y : ((m < 24) ? g.z : g.w));
     return (w >> (4 * (m & 7))) & 15u;
-}
-
-template <int K>
-__global__ void __launch_bounds__(MP_THREADS)
-k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
-                const double *__restrict__ q, const double *__restrict__ p, int64_t islice,
-                double *__restrict__ out, int *__restrict__ err)
-{
-    using C = MP<K>;
-    constexpr int T = C::T, N = C::N, E = C::E;
-    extern __shared__ __align__(1024) uint8_t smraw[];
-    uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    __shared__ uint64_t mbar[2];
-    __shared__ uint32_t tmem_holder;
-
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int64_t j = (int64_t)blockIdx.x * 128 + tid;
-    const bool valid = j < J;
-    const int64_t ia = (int64_t)blockIdx.y * islice;
-    const int64_t ib = min(I, ia + islice);
-    const int nchunk = (int)((ib - ia + MP_IC - 1) / MP_IC);
-    const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
-
-    if (warp == 0) tmem_alloc_warp(&tmem_holder, C::NCOLS);
-    if (tid == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
-        mbar_fence_init();
-    }
-    code_table_init((float4 *)(sm + C::OFF_TAB), tid, MP_THREADS);
-    double qr[C::PREF_Q];
-    auto qload = [&](int64_t ic) {
-#pragma unroll
-        for (int u = 0; u < C::PREF_Q; ++u) {
-            const int t = tid + u * MP_THREADS;              /* t = ii * K + k: coalesced */
-            const int ii = t / K;
-            qr[u] = (t < K * MP_IC && ic + ii < ib) ? q[(size_t)K * ic + t] : 1.0 / K;
-        }
-    };
-    auto qstore = [&](float *Qb) {
-#pragma unroll
-        for (int u = 0; u < C::PREF_Q; ++u) {
-            const int t = tid + u * MP_THREADS;
-            if (t < K * MP_IC) {
-                const int ii = t / K, k = t - ii * K;
-                Qb[k * C::QS + ii] = (float)qr[u];
-            }
-        }
-    };
-    uint4 gcur = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), gnext = gcur;
-    if (nchunk > 0) {
-        qload(ia);
-        qstore((float *)(sm + C::OFF_Q));
-        gcur = col_load64(bed, pitch, j, valid, ia);
-    }
-    if (nchunk > 1) {
-        qload(ia + MP_IC);
-        gnext = col_load64(bed, pitch, j, valid, ia + MP_IC);
-    }
-    tc_fence_before_sync();
-    __syncthreads();
-    tc_fence_after_sync();
-    const uint32_t tmem = tmem_holder;
-
-    float2 pd[K], pbd[K];            /* p_k and 1 - p_k duplicated into pairs */
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const double pv = valid ? p[(size_t)K * j + k] : 0.5;
-        pd[k] = make_float2((float)pv, (float)pv);
-        const float pb = (float)(1.0 - pv);
-        pbd[k] = make_float2(pb, pb);
-    }
-    double gd[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) gd[k] = 0.0;
-    constexpr uint32_t idesc = idesc_bf16_f32(128, N);
-    bool ok = true;
-
-    for (int c = 0; c < nchunk; ++c) {
-        const int s = c & 1;
-        uint8_t *At = sm + s * C::STAGE_BYTES;
-        uint8_t *Bt = At + C::A_BYTES;
-        const float *Qb = (const float *)(sm + C::OFF_Q + s * C::QBUF);
-        if (c >= 2 && ok) {
-            if (!mbar_wait_bounded(&mbar[s], (uint32_t)(((c - 2) >> 1) & 1), MX_WAIT_LIMIT)) {
-                ok = false;
-                if (tid == 0) atomicOr(err, 1);
-            }
-        }
-        /* B tile: QQ[n][i] = q_ka(i) q_kb(i) in BF16, task (kc, nn) -> 16-byte row chunk */
-        for (int t = tid; t < 8 * N; t += MP_THREADS) {
-            const int kc = t / N, nn = t - kc * N;
-            uint32_t w[4] = {0u, 0u, 0u, 0u};
-            if (nn < T) {
-                int ka, kb;
-                tri_pair(nn, ka, kb);
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int ii = kc * 8 + 2 * e;
-                    w[e] = pack_bf16x2(Qb[ka * C::QS + ii] * Qb[kb * C::QS + ii],
-                                       Qb[ka * C::QS + ii + 1] * Qb[kb * C::QS + ii + 1]);
-                }
-            }
-            *(uint4 *)(Bt + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
-        }
-        const float2 *Q2 = (const float2 *)Qb;                  /* [k][pair] */
-        float2 ga[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) ga[k] = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int kc = 0; kc < 8; ++kc) {
-            uint32_t cp[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int m = kc * 4 + e;                       /* individuals 2m, 2m+1 of the chunk */
-                const float4 a = tab[8 * pair_code(gcur, m)];
-                float2 qp = make_float2(0.f, 0.f), om = make_float2(0.f, 0.f);
-                float2 qv[K];
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    qv[k] = Q2[k * (C::QS / 2) + m];
-                    qp = __ffma2_rn(qv[k], pd[k], qp);
-                    om = __ffma2_rn(qv[k], pbd[k], om);
-                }
-                const float2 pr = __fmul2_rn(qp, om);
-                const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
-                const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
-                const float2 z1 = __fmul2_rn(make_float2(a.x, a.y), r1);
-                const float2 z2 = __fmul2_rn(make_float2(a.z, a.w), r2);
-                const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
-                const float2 zz = make_float2(z1.x - z2.x, z1.y - z2.y);    /* nm (g/qp - (2-g)/(1-qp)) */
-#pragma unroll
-                for (int k = 0; k < K; ++k) ga[k] = __ffma2_rn(zz, qv[k], ga[k]);
-                cp[e] = pack_bf16x2(cw.x, cw.y);
-            }
-            *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
-        }
-#pragma unroll
-        for (int k = 0; k < K; ++k) gd[k] += (double)ga[k].x + (double)ga[k].y;
-        if (c + 1 < nchunk) {
-            qstore((float *)(sm + C::OFF_Q + (s ^ 1) * C::QBUF));
-            gcur = gnext;
-            if (c + 2 < nchunk) {
-                const int64_t icn = ia + (int64_t)(c + 2) * MP_IC;
-                qload(icn);
-                gnext = col_load64(bed, pitch, j, valid, icn);
-            }
-        }
-        fence_async_smem();
-        __syncthreads();
-        if (tid == 0 && ok) {
-            tc_fence_after_sync();
-            const uint32_t abase = smem_u32(At), bbase = smem_u32(Bt);
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-                const uint64_t ad = umma_desc_kmajor(abase + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
-                const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
-                tc_mma_bf16(tmem, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
-            }
-            tc_commit(&mbar[s]);
-        }
-    }
-    for (int c = max(0, nchunk - 2); c < nchunk; ++c) {
-        const int s = c & 1;
-        if (!mbar_wait_bounded(&mbar[s], (uint32_t)((c >> 1) & 1), ok ? MX_WAIT_LIMIT : 1024u)) {
-            ok = false;
-            if (tid == 0) atomicOr(err, 1);
-        }
-    }
-    tc_fence_after_sync();
-    double *o = out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E;
-    if (valid) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) o[T + k] = gd[k];
-    }
-    if (nchunk > 0) {
-#pragma unroll 1
-        for (int c0 = 0; c0 < N; c0 += 16) {
-            float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (valid) {
-#pragma unroll
-                for (int e = 0; e < 16; ++e)
-                    if (c0 + e < T) o[c0 + e] = ok ? (double)v[e] : __longlong_as_double(0x7ff8000000000000LL);
-            }
-        }
-    } else if (valid) {
-        for (int e = 0; e < T; ++e) o[e] = 0.0;
-    }
-    tc_fence_before_sync();
-    __syncthreads();
-    if (warp == 0) tmem_dealloc_warp(tmem, C::NCOLS);
 }
 
 /* ===================================================================== loglik
@@ -813,7 +948,7 @@ cudaError_t launch_q_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t p
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_q_mixed<K><<<grid, MQ_THREADS, MQ<K>::SMEM, st>>>(bed, I, J, pitch, q, pkg, pl.slice, out, err);
+    k_sweep_q_mixed<K><<<grid, MQ_CTA, MQ<K>::SMEM, st>>>(bed, I, J, pitch, q, pkg, pl.slice, out, err);
     return cudaGetLastError();
 }
 
@@ -825,11 +960,21 @@ size_t q_pkg_bytes_t(int64_t J)
 
 template <int K>
 cudaError_t launch_p_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                             const double *p, const SweepPlan &pl, double *out, int *err, cudaStream_t st)
+                             const double *p, const SweepPlan &pl, double *out, int *err, uint8_t *pkg,
+                             cudaStream_t st)
 {
+    k_p_pack<K><<<(unsigned)((I + MP_IC - 1) / MP_IC), 128, 0, st>>>(q, I, pkg);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_p_mixed<K><<<grid, MP_THREADS, MP<K>::SMEM, st>>>(bed, I, J, pitch, q, p, pl.slice, out, err);
+    k_sweep_p_mixed<K><<<grid, MP_THREADS, MP<K>::SMEM, st>>>(bed, I, J, pitch, pkg, p, pl.slice, out, err);
     return cudaGetLastError();
+}
+
+template <int K>
+size_t p_pkg_bytes_t(int64_t I)
+{
+    return (size_t)((I + MP_IC - 1) / MP_IC) * MP<K>::PKG;
 }
 
 template <int K>
@@ -902,11 +1047,19 @@ size_t sweep_q_mixed_pkg_bytes(int K, int64_t J)
 }
 
 cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                                 const double *p, const SweepPlan &pl, double *out, int *err, cudaStream_t st)
+                                 const double *p, const SweepPlan &pl, double *out, int *err, uint8_t *pkg,
+                                 cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_p_mixed_t<KK>(bed, I, J, pitch, q, p, pl, out, err, st));
+    ADMIX_DISPATCH_K(K, e = launch_p_mixed_t<KK>(bed, I, J, pitch, q, p, pl, out, err, pkg, st));
     return e;
+}
+
+size_t sweep_p_mixed_pkg_bytes(int K, int64_t I)
+{
+    size_t b = 0;
+    ADMIX_DISPATCH_K(K, b = p_pkg_bytes_t<KK>(I));
+    return b;
 }
 
 cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,

@@ -175,3 +175,9 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t b
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
 }
+
+/* plain arrival (release) on an mbarrier */
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(mbar)) : "memory");
+}
