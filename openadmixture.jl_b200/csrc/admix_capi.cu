@@ -303,7 +303,7 @@ static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst, bool fast = 
 {
     if (fast && (h->flags & ADMIX_FLAG_MIXED))
         return launch_loglik_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, which), Pof(h, which), h->llm,
-                                   h->ll_partial, dst, h->st);
+                                   h->ll_partial, dst, &h->sc->tc_err, h->pkg, h->st);
     return launch_loglik_f64(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, which), Pof(h, which), h->llp,
                              h->ll_partial, dst, h->st);
 }

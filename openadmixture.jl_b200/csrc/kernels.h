@@ -51,9 +51,10 @@ cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J
                                  cudaStream_t st);
 size_t sweep_p_mixed_pkg_bytes(int K, int64_t I);
 SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms);
+/* err and pkg are accepted for symmetry with the sweeps; the log-likelihood stays on the CUDA cores. */
 cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                                const double *p, const SweepPlan &pl, double *partial, double *out,
-                                cudaStream_t st);
+                                const double *p, const SweepPlan &pl, double *partial, double *out, int *err,
+                                uint8_t *pkg, cudaStream_t st);
 
 cudaError_t launch_mask_tail(uint8_t *bed, int64_t I, int64_t J, int64_t pitch, int sms, cudaStream_t st);
 

@@ -549,12 +549,13 @@ k_p_pack(const double *__restrict__ q, int64_t I, uint8_t *__restrict__ pkg)
     for (uint32_t t = tid; t < C::PKG / 16; t += 128) dst[t] = ((const uint4 *)buf)[t];
 }
 
-/* qp (TMEM columns 0..31) and om (32..63) of the package's chunk: 2 * 3 * KP/8 TF32 MMAs */
+/* qp (TMEM columns 0..31) and om (32..63) of a chunk: 2 * 3 * KP/8 TF32 MMAs of the P tile (the
+ * (1-P) tile follows at +PA_BYTES) with the chunk's TF32 Q tile */
 template <int K>
-__device__ __forceinline__ void issue_qp_p(uint32_t tmem, const uint8_t *sm, const uint8_t *pk)
+__device__ __forceinline__ void issue_qp_p(uint32_t tmem, const uint8_t *pa, const uint8_t *qb)
 {
     using C = MP<K>;
-    const uint32_t a0 = smem_u32(sm + C::OFF_PA), b = smem_u32(pk + C::PK_QB);
+    const uint32_t a0 = smem_u32(pa), b = smem_u32(qb);
     constexpr uint32_t id = idesc_tf32_f32(128, MP_IC);
     constexpr uint32_t alo = (C::KP / 4) * C::PA_LBO, blo = (C::KP / 4) * C::QB_LBO;
 #pragma unroll
@@ -652,7 +653,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         if (nchunk > 0) {
             if (mbar_wait_bounded(&bar_p[0], 0u, MX_WAIT_LIMIT)) {
                 ++p_waited;
-                issue_qp_p<K>(tmem, sm, sm + C::OFF_PKG);
+                issue_qp_p<K>(tmem, sm + C::OFF_PA, sm + C::OFF_PKG + C::PK_QB);
                 tc_commit(bar_q);
             } else {
                 ok = false;
@@ -695,7 +696,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 const int cn = c + 1;
                 if (mbar_wait_bounded(&bar_p[cn % MP_NPKG], (uint32_t)((cn / MP_NPKG) & 1), MX_WAIT_LIMIT)) {
                     ++p_waited;
-                    issue_qp_p<K>(tmem, sm, sm + C::OFF_PKG + (cn % MP_NPKG) * C::PKG);
+                    issue_qp_p<K>(tmem, sm + C::OFF_PA, sm + C::OFF_PKG + (cn % MP_NPKG) * C::PKG + C::PK_QB);
                     tc_commit(bar_q);
                 } else {
                     ok = false;
@@ -979,8 +980,11 @@ size_t p_pkg_bytes_t(int64_t I)
 
 template <int K>
 cudaError_t launch_ll_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                              const double *p, const SweepPlan &pl, double *partial, double *out, cudaStream_t st)
+                              const double *p, const SweepPlan &pl, double *partial, double *out, int *err,
+                              uint8_t *pkg, cudaStream_t st)
 {
+    (void)err;
+    (void)pkg;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
     k_loglik_mixed<K><<<grid, 128, 0, st>>>(bed, I, J, pitch, q, p, pl.slice, partial);
     k_sum_partials_mixed<<<1, 1024, 0, st>>>(partial, (int64_t)pl.gx * pl.S, out);
@@ -1063,9 +1067,10 @@ size_t sweep_p_mixed_pkg_bytes(int K, int64_t I)
 }
 
 cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                                const double *p, const SweepPlan &pl, double *partial, double *out, cudaStream_t st)
+                                const double *p, const SweepPlan &pl, double *partial, double *out, int *err,
+                                uint8_t *pkg, cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_ll_mixed_t<KK>(bed, I, J, pitch, q, p, pl, partial, out, st));
+    ADMIX_DISPATCH_K(K, e = launch_ll_mixed_t<KK>(bed, I, J, pitch, q, p, pl, partial, out, err, pkg, st));
     return e;
 }
