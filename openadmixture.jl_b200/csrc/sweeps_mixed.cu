@@ -583,8 +583,11 @@ __device__ __forceinline__ uint2 col_load32(const uint8_t *__restrict__ bed, int
                  : make_uint2(0x55555555u, 0x55555555u);
 }
 
+/* Warp roles as in the Q sweep: warps 0-3 producers (thread = SNP row), warp 4 controller. */
+constexpr int MP_CTA = MP_THREADS + 32;
+
 template <int K>
-__global__ void __launch_bounds__(MP_THREADS, (K <= 10 ? 4 : 2))
+__global__ void __launch_bounds__(MP_CTA, (K <= 10 ? 3 : 2))
 k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                 const uint8_t *__restrict__ pkg, const double *__restrict__ p, int64_t islice,
                 double *__restrict__ out, int *__restrict__ err)
@@ -593,27 +596,34 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     constexpr int T = C::T, N = C::N, E = C::E;
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    __shared__ uint64_t mbar[2 + MP_NPKG];              /* Hessian MMA, qp MMA, package copies */
+    /* qp ready, qp consumed (4 warps), C tile written (4 warps), Hessian done, package [3] */
+    __shared__ uint64_t mbar[4 + MP_NPKG];
     __shared__ uint32_t tmem_holder;
-    uint64_t *bar_h = &mbar[0], *bar_q = &mbar[1], *bar_p = &mbar[2];
+    __shared__ volatile int abort_flag;
+    uint64_t *bar_qp = &mbar[0], *bar_qfree = &mbar[1], *bar_afull = &mbar[2], *bar_h = &mbar[3], *bar_p = &mbar[4];
 
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp < 4;
     const int64_t j = (int64_t)blockIdx.x * 128 + tid;
-    const bool valid = j < J;
+    const bool valid = producer && j < J;
     const int64_t ia = (int64_t)blockIdx.y * islice;    /* islice is a multiple of MP_IC */
     const int64_t ib = min(I, ia + islice);
     const int nchunk = (int)((ib - ia + MP_IC - 1) / MP_IC);
     const uint8_t *pk0 = pkg + (size_t)(ia / MP_IC) * C::PKG;
-    const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
     uint8_t *At = sm + C::OFF_A;
 
-    if (warp == 0) tmem_alloc_warp(&tmem_holder, C::NCOLS);
+    if (warp == 4) tmem_alloc_warp(&tmem_holder, C::NCOLS);
     if (tid == 0) {
-        for (int b = 0; b < 2 + MP_NPKG; ++b) mbar_init(&mbar[b], 1);
+        mbar_init(bar_qp, 1);
+        mbar_init(bar_qfree, 4);
+        mbar_init(bar_afull, 4);
+        mbar_init(bar_h, 1);
+        for (int b = 0; b < MP_NPKG; ++b) mbar_init(&bar_p[b], 1);
+        abort_flag = 0;
         mbar_fence_init();
     }
-    code_table_init((float4 *)(sm + C::OFF_TAB), tid, MP_THREADS);
-    {   /* this thread's rows of the TF32 P and (1-P) tiles */
+    code_table_init((float4 *)(sm + C::OFF_TAB), tid, MP_CTA);
+    if (producer) {   /* this thread's rows of the TF32 P and (1-P) tiles */
         float hv[C::KP], lv[C::KP], hb[C::KP], lb[C::KP];
 #pragma unroll
         for (int k = 0; k < C::KP; ++k) {
@@ -633,134 +643,54 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             *(float4 *)(pb + kmaj_off(tid, C::KP + f, C::PA_LBO)) = make_float4(lb[f], lb[f + 1], lb[f + 2], lb[f + 3]);
         }
     }
-    uint2 gcur = make_uint2(0x55555555u, 0x55555555u), gnext = gcur;
-    if (nchunk > 0) gcur = col_load32(bed, pitch, j, valid, ia);
-    if (nchunk > 1) gnext = col_load32(bed, pitch, j, valid, ia + MP_IC);
     fence_async_smem();
     tc_fence_before_sync();
     __syncthreads();
     tc_fence_after_sync();
     const uint32_t tmem = tmem_holder;
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
     bool ok = true;
-    int p_issued = 0, p_waited = 0;
-    if (tid == 0) {
-        for (int c = 0; c < min(nchunk, 2); ++c) {
-            mbar_arrive_expect_tx(&bar_p[c], C::PKG);
-            bulk_g2s(sm + C::OFF_PKG + c * C::PKG, pk0 + (size_t)c * C::PKG, C::PKG, &bar_p[c]);
-            ++p_issued;
+    auto wait = [&](uint64_t *b, uint32_t parity) -> bool {
+        if (!ok) return false;
+        for (uint32_t n = 0; n < MX_WAIT_LIMIT; ++n) {
+            if (mbar_try_wait(b, parity)) return true;
+            if ((n & 255u) == 255u && abort_flag) break;
         }
-        if (nchunk > 0) {
-            if (mbar_wait_bounded(&bar_p[0], 0u, MX_WAIT_LIMIT)) {
-                ++p_waited;
-                issue_qp_p<K>(tmem, sm + C::OFF_PA, sm + C::OFF_PKG + C::PK_QB);
-                tc_commit(bar_q);
-            } else {
-                ok = false;
-                atomicOr(err, 1);
+        ok = false;
+        abort_flag = 1;
+        atomicOr(err, 1);
+        return false;
+    };
+
+    if (!producer) {
+        /* ---------------------------------------------------------------- controller warp */
+        const bool leader = lane == 0;
+        auto copy_pkg = [&](int c) {
+            if (leader) {
+                mbar_arrive_expect_tx(&bar_p[c % MP_NPKG], C::PKG);
+                bulk_g2s(sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG, pk0 + (size_t)c * C::PKG, C::PKG,
+                         &bar_p[c % MP_NPKG]);
             }
+        };
+        for (int c = 0; c < min(nchunk, MP_NPKG); ++c) copy_pkg(c);
+        if (nchunk > 0 && wait(&bar_p[0], 0u) && leader) {
+            tc_fence_after_sync();
+            issue_qp_p<K>(tmem, sm + C::OFF_PA, sm + C::OFF_PKG + C::PK_QB);
+            tc_commit(bar_qp);
         }
-    }
-    ok = __syncthreads_and(ok);
-    int q_issued = (ok && nchunk > 0) ? 1 : 0, q_done = 0, h_issued = 0, h_done = 0;
-
-    double gd[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) gd[k] = 0.0;
-    constexpr uint32_t idesc = idesc_bf16_f32(128, N);
-
-    for (int c = 0; c < nchunk; ++c) {
-        const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
-        const float *Qf = (const float *)(pk + C::PK_QF);
-        /* 1. qp and 1 - qp of this thread's SNP and the chunk's 32 individuals */
-        uint32_t rq[32], ro[32];
-        if (ok && q_done < q_issued) {
-            if (mbar_wait_bounded(bar_q, (uint32_t)(q_done & 1), MX_WAIT_LIMIT)) ++q_done;
-            else { ok = false; atomicOr(err, 1); }
-        }
-        tc_fence_after_sync();
-        tmem_ld32_nowait(tmem + lane_base, rq);
-        tmem_ld32_nowait(tmem + lane_base + C::COL_OM, ro);
-        tmem_wait_ld();
-        /* 2. the Hessian MMAs of chunk c-1 are done: the C tile and package c-1 are free */
-        if (ok && h_done < h_issued) {
-            if (mbar_wait_bounded(bar_h, (uint32_t)(h_done & 1), MX_WAIT_LIMIT)) ++h_done;
-            else { ok = false; atomicOr(err, 1); }
-        }
-        tc_fence_before_sync();
-        ok = __syncthreads_and(ok);
-        /* 3. qp / om MMAs of chunk c+1 (its package landed), copy of package c+2 */
-        if (ok && c + 1 < nchunk) {
-            if (tid == 0) {
-                tc_fence_after_sync();
+        constexpr uint32_t idesc = idesc_bf16_f32(128, N);
+        for (int c = 0; c < nchunk && ok; ++c) {
+            if (c + 1 < nchunk) {
                 const int cn = c + 1;
-                if (mbar_wait_bounded(&bar_p[cn % MP_NPKG], (uint32_t)((cn / MP_NPKG) & 1), MX_WAIT_LIMIT)) {
-                    ++p_waited;
+                const bool landed = wait(&bar_p[cn % MP_NPKG], (uint32_t)((cn / MP_NPKG) & 1));
+                if (landed && wait(bar_qfree, (uint32_t)(c & 1)) && leader) {
+                    tc_fence_after_sync();
                     issue_qp_p<K>(tmem, sm + C::OFF_PA, sm + C::OFF_PKG + (cn % MP_NPKG) * C::PKG + C::PK_QB);
-                    tc_commit(bar_q);
-                } else {
-                    ok = false;
-                    atomicOr(err, 1);
-                }
-                if (ok && c + 2 < nchunk) {
-                    const int cm = c + 2;
-                    fence_async_smem();
-                    mbar_arrive_expect_tx(&bar_p[cm % MP_NPKG], C::PKG);
-                    bulk_g2s(sm + C::OFF_PKG + (cm % MP_NPKG) * C::PKG, pk0 + (size_t)cm * C::PKG, C::PKG,
-                             &bar_p[cm % MP_NPKG]);
-                    ++p_issued;
+                    tc_commit(bar_qp);
                 }
             }
-            ++q_issued;
-        }
-        /* 4. producer: 16 individual pairs, 4 per BF16 k-chunk */
-        float2 gk[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int kc = 0; kc < 4; ++kc) {
-            uint32_t cp[4];
-            float2 zz[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int m = kc * 4 + e;                       /* individuals 2m, 2m+1 of the chunk */
-                const uint32_t w = (m < 8) ? gcur.x : gcur.y;
-                const float4 a = tab[8 * ((w >> (4 * (m & 7))) & 15u)];
-                const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
-                const float2 om = make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1]));
-                const float2 pr = __fmul2_rn(qp, om);
-                const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
-                const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
-                const float2 z1 = __fmul2_rn(make_float2(a.x, a.y), r1);
-                const float2 z2 = __fmul2_rn(make_float2(a.z, a.w), r2);
-                const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
-                zz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);              /* nm (g/qp - (2-g)/(1-qp)) */
-                cp[e] = pack_bf16x2(cw.x, cw.y);
-            }
-            *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const float4 q0 = *(const float4 *)(Qf + k * C::QS + kc * 8);
-                const float4 q1 = *(const float4 *)(Qf + k * C::QS + kc * 8 + 4);
-                gk[k] = __ffma2_rn(zz[0], make_float2(q0.x, q0.y), gk[k]);
-                gk[k] = __ffma2_rn(zz[1], make_float2(q0.z, q0.w), gk[k]);
-                gk[k] = __ffma2_rn(zz[2], make_float2(q1.x, q1.y), gk[k]);
-                gk[k] = __ffma2_rn(zz[3], make_float2(q1.z, q1.w), gk[k]);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y;
-        if (c + 1 < nchunk) {
-            gcur = gnext;
-            if (c + 2 < nchunk) gnext = col_load32(bed, pitch, j, valid, ia + (int64_t)(c + 2) * MP_IC);
-        }
-        /* 5. Hessian MMAs of chunk c */
-        fence_async_smem();
-        tc_fence_before_sync();
-        ok = __syncthreads_and(ok);
-        if (ok) {
-            if (tid == 0) {
+            if (wait(bar_afull, (uint32_t)(c & 1)) && leader) {
                 tc_fence_after_sync();
+                const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
                 const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
 #pragma unroll
                 for (int ks = 0; ks < 2; ++ks) {
@@ -770,42 +700,118 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 }
                 tc_commit(bar_h);
             }
-            ++h_issued;
-        }
-    }
-    const uint32_t lim = ok ? MX_WAIT_LIMIT : 1024u;
-    if (h_done < h_issued) {
-        if (mbar_wait_bounded(bar_h, (uint32_t)(h_done & 1), lim)) ++h_done;
-        else { ok = false; atomicOr(err, 1); }
-    }
-    if (q_done < q_issued && mbar_wait_bounded(bar_q, (uint32_t)(q_done & 1), ok ? MX_WAIT_LIMIT : 1024u)) ++q_done;
-    if (tid == 0)
-        for (int cw = p_waited; cw < p_issued; ++cw)
-            mbar_wait_bounded(&bar_p[cw % MP_NPKG], (uint32_t)((cw / MP_NPKG) & 1), 1024u);
-    ok = __syncthreads_and(ok && h_done == h_issued);
-    tc_fence_after_sync();
-    double *o = out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E;
-    if (valid) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) o[T + k] = gd[k];
-    }
-    if (nchunk > 0) {
-#pragma unroll 1
-        for (int c0 = 0; c0 < N; c0 += 16) {
-            float v[16];
-            tmem_ld16(tmem + lane_base + C::COL_H + (uint32_t)c0, v);
-            if (valid) {
-#pragma unroll
-                for (int e = 0; e < 16; ++e)
-                    if (c0 + e < T) o[c0 + e] = ok ? (double)v[e] : __longlong_as_double(0x7ff8000000000000LL);
+            if (c + MP_NPKG < nchunk && wait(bar_h, (uint32_t)(c & 1))) {
+                fence_async_smem();
+                copy_pkg(c + MP_NPKG);
             }
         }
-    } else if (valid) {
-        for (int e = 0; e < T; ++e) o[e] = 0.0;
+    } else {
+        /* ---------------------------------------------------------------- producer warps */
+        const float4 *tab = (const float4 *)(sm + C::OFF_TAB) + (tid & 7);
+        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        uint2 gcur = make_uint2(0x55555555u, 0x55555555u), gnext = gcur;
+        if (nchunk > 0) gcur = col_load32(bed, pitch, j, valid, ia);
+        if (nchunk > 1) gnext = col_load32(bed, pitch, j, valid, ia + MP_IC);
+        double gd[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) gd[k] = 0.0;
+        for (int c = 0; c < nchunk && ok; ++c) {
+            const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
+            const float *Qf = (const float *)(pk + C::PK_QF);
+            uint32_t rq[32], ro[32];
+            if (!wait(bar_qp, (uint32_t)(c & 1))) break;
+            tc_fence_after_sync();
+            tmem_ld32_nowait(tmem + lane_base, rq);
+            tmem_ld32_nowait(tmem + lane_base + C::COL_OM, ro);
+            tmem_wait_ld();
+            tc_fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_qfree);
+            if (!wait(&bar_p[c % MP_NPKG], (uint32_t)((c / MP_NPKG) & 1))) break;
+            if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the C tile is free */
+            float2 gk[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int kc = 0; kc < 4; ++kc) {
+                uint32_t cp[4];
+                float2 zz[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int m = kc * 4 + e;
+                    const uint32_t w = (m < 8) ? gcur.x : gcur.y;
+                    const float4 a = tab[8 * ((w >> (4 * (m & 7))) & 15u)];
+                    const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
+                    const float2 om = make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1]));
+                    const float2 pr = __fmul2_rn(qp, om);
+                    const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
+                    const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
+                    const float2 z1 = __fmul2_rn(make_float2(a.x, a.y), r1);
+                    const float2 z2 = __fmul2_rn(make_float2(a.z, a.w), r2);
+                    const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
+                    zz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);              /* nm (g/qp - (2-g)/(1-qp)) */
+                    cp[e] = pack_bf16x2(cw.x, cw.y);
+                }
+                *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const float4 q0 = *(const float4 *)(Qf + k * C::QS + kc * 8);
+                    const float4 q1 = *(const float4 *)(Qf + k * C::QS + kc * 8 + 4);
+                    gk[k] = __ffma2_rn(zz[0], make_float2(q0.x, q0.y), gk[k]);
+                    gk[k] = __ffma2_rn(zz[1], make_float2(q0.z, q0.w), gk[k]);
+                    gk[k] = __ffma2_rn(zz[2], make_float2(q1.x, q1.y), gk[k]);
+                    gk[k] = __ffma2_rn(zz[3], make_float2(q1.z, q1.w), gk[k]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y;
+            if (c + 1 < nchunk) {
+                gcur = gnext;
+                if (c + 2 < nchunk) gnext = col_load32(bed, pitch, j, valid, ia + (int64_t)(c + 2) * MP_IC);
+            }
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_afull);
+        }
+        if (nchunk > 0) wait(bar_h, (uint32_t)((nchunk - 1) & 1));   /* the last Hessian MMAs */
+        if (valid) {
+            double *o = out + ((size_t)blockIdx.y * J + j) * E;
+#pragma unroll
+            for (int k = 0; k < K; ++k) o[T + k] = gd[k];
+        }
+    }
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == MP_THREADS) {
+        mbar_wait_bounded(bar_h, 0u, 1024u);
+        mbar_wait_bounded(bar_h, 1u, 1024u);
+        mbar_wait_bounded(bar_qp, 0u, 1024u);
+        mbar_wait_bounded(bar_qp, 1u, 1024u);
+        for (int b = 0; b < MP_NPKG; ++b) { mbar_wait_bounded(&bar_p[b], 0u, 1024u); mbar_wait_bounded(&bar_p[b], 1u, 1024u); }
+    }
+    __syncthreads();
+    tc_fence_after_sync();
+    if (producer) {
+        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        if (nchunk > 0) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + lane_base + C::COL_H + (uint32_t)c0, v);
+                if (valid) {
+                    double *o = out + ((size_t)blockIdx.y * J + j) * E;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        if (c0 + e < T) o[c0 + e] = ok ? (double)v[e] : __longlong_as_double(0x7ff8000000000000LL);
+                }
+            }
+        } else if (valid) {
+            double *o = out + ((size_t)blockIdx.y * J + j) * E;
+            for (int e = 0; e < T; ++e) o[e] = 0.0;
+        }
     }
     tc_fence_before_sync();
     __syncthreads();
-    if (warp == 0) tmem_dealloc_warp(tmem, C::NCOLS);
+    if (warp == 4) tmem_dealloc_warp(tmem, C::NCOLS);
 }
 
 /* 64 individuals' codes of SNP column j from individual ic (a multiple of 64) */
@@ -968,7 +974,7 @@ cudaError_t launch_p_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t p
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_p_mixed<K><<<grid, MP_THREADS, MP<K>::SMEM, st>>>(bed, I, J, pitch, pkg, p, pl.slice, out, err);
+    k_sweep_p_mixed<K><<<grid, MP_CTA, MP<K>::SMEM, st>>>(bed, I, J, pitch, pkg, p, pl.slice, out, err);
     return cudaGetLastError();
 }
 
