@@ -342,7 +342,8 @@ static cudaError_t enq_update_q(admix_ctx *h, int update2)
     cudaError_t e = enq_sweep_q(h, wq, wp, &S);
     if (e != cudaSuccess) return e;
     return launch_qp(h->K, true, h->I, h->parts_q, S, Qof(h, wq), Qof(h, wo), h->status_q,
-                     &h->sc->fail_q, h->vt, (h->flags & ADMIX_FLAG_MU_GERSHGORIN) ? 1 : 0, h->st);
+                     &h->sc->fail_q, h->vt, (h->flags & ADMIX_FLAG_MU_GERSHGORIN) ? 1 : 0,
+                     (h->flags & ADMIX_FLAG_MIXED) ? 1 : 0, h->st);
 }
 
 /* update_p!: p_out = project_p(p + QP(H_p, -Xtz_p)), with q = q_next (update2 = 0) or q_next2 */
@@ -355,7 +356,7 @@ static cudaError_t enq_update_p(admix_ctx *h, int update2)
     cudaError_t e = enq_sweep_p(h, wq, wp, &S);
     if (e != cudaSuccess) return e;
     return launch_qp(h->K, false, h->J, h->parts_p, S, Pof(h, wp), Pof(h, wo), h->status_p,
-                     &h->sc->fail_p, h->vt, 0, h->st);
+                     &h->sc->fail_p, h->vt, 0, (h->flags & ADMIX_FLAG_MIXED) ? 1 : 0, h->st);
 }
 
 static cudaError_t enq_em(admix_ctx *h)
@@ -595,8 +596,8 @@ int admix_time_pass(admix_ctx *h, int32_t pass, int32_t reps, double *ms_per_lau
         case ADMIX_PASS_LOGLIK: return enq_loglik(h, ADMIX_X, &h->sc->ll_tmp, true);
         case ADMIX_PASS_QSWEEP: { int S; return enq_sweep_q(h, ADMIX_X, ADMIX_X, &S); }
         case ADMIX_PASS_PSWEEP: { int S; return enq_sweep_p(h, ADMIX_X, ADMIX_X, &S); }
-        case ADMIX_PASS_QQP: return launch_qp(h->K, true, h->I, h->parts_q, (h->flags & ADMIX_FLAG_MIXED) ? h->sqm.S : h->sq.S, Qof(h, ADMIX_X), Qof(h, ADMIX_X_TMP), h->status_q, nullptr, h->vt, mu, h->st);
-        case ADMIX_PASS_PQP: return launch_qp(h->K, false, h->J, h->parts_p, (h->flags & ADMIX_FLAG_MIXED) ? h->spm.S : h->sp.S, Pof(h, ADMIX_X), Pof(h, ADMIX_X_TMP), h->status_p, nullptr, h->vt, 0, h->st);
+        case ADMIX_PASS_QQP: return launch_qp(h->K, true, h->I, h->parts_q, (h->flags & ADMIX_FLAG_MIXED) ? h->sqm.S : h->sq.S, Qof(h, ADMIX_X), Qof(h, ADMIX_X_TMP), h->status_q, nullptr, h->vt, mu, (h->flags & ADMIX_FLAG_MIXED) ? 1 : 0, h->st);
+        case ADMIX_PASS_PQP: return launch_qp(h->K, false, h->J, h->parts_p, (h->flags & ADMIX_FLAG_MIXED) ? h->spm.S : h->sp.S, Pof(h, ADMIX_X), Pof(h, ADMIX_X_TMP), h->status_p, nullptr, h->vt, 0, (h->flags & ADMIX_FLAG_MIXED) ? 1 : 0, h->st);
         default: return enq_em(h);
         }
     };

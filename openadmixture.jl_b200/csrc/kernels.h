@@ -62,7 +62,7 @@ cudaError_t launch_mask_tail(uint8_t *bed, int64_t I, int64_t J, int64_t pitch, 
 cudaError_t prepare_qp(int K);
 cudaError_t launch_qp(int K, bool simplex, int64_t nprob, const double *parts, int S,
                       const double *x, double *x_next, int32_t *status, int32_t *fail_count,
-                      const double *vt, int mu_mode, cudaStream_t st);
+                      const double *vt, int mu_mode, int damp_retry, cudaStream_t st);
 
 /* quasi-Newton (qn.cu) */
 struct QNPlan { int blocks = 1; };

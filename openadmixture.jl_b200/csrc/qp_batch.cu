@@ -149,11 +149,17 @@ __device__ __forceinline__ void project_simplex(double (&b)[K], double *s)
     for (int i = 0; i < K; ++i) b[i] = fmax(b[i] - tmax, 0.0) + pc;
 }
 
+/* damp_retry (the mixed-precision form only): a problem whose QP fails is solved once more with
+ * the Hessian's diagonal scaled by 1 + K/512.  A BF16 Hessian rounds every pair product p_k p_k'
+ * on its own, so a problem whose exact Hessian is nearly singular can come out slightly
+ * indefinite and fail the reference's pivot tests; the scaling covers that rounding (K * 2^-9
+ * per row, Gershgorin) and only shortens the Newton step -- the fixed point is set by the
+ * gradient.  The FP64 form never retries: a failed QP leaves the reference's zero step. */
 template <int K, bool SIMPLEX>
 __global__ void __launch_bounds__(QB)
 k_qp(int64_t nprob, const double *__restrict__ parts, int S, const double *__restrict__ x,
      double *__restrict__ x_next, int32_t *__restrict__ status, int32_t *__restrict__ fail_count,
-     const double *__restrict__ vt, int mu_mode)
+     const double *__restrict__ vt, int mu_mode, int damp_retry)
 {
     constexpr int C = SIMPLEX ? 1 : 0;
     constexpr int N = K + C + 1;
@@ -173,6 +179,9 @@ k_qp(int64_t nprob, const double *__restrict__ parts, int S, const double *__res
     /* create_tableau! (qp.jl:8-76): H, border -r = Xtz (r = -Xtz, algorithms_inner.jl:201) */
     const int64_t stride = nprob * (int64_t)E;
     const double *src = parts + (size_t)pr * E;
+    int st = 0;
+    for (int attempt = 0; attempt < (damp_retry ? 2 : 1) && st == 0; ++attempt) {
+    const double dscale = attempt ? 1.0 + (double)K / 512.0 : 1.0;
 #pragma unroll 1
     for (int k2 = 0; k2 < K; ++k2) {
 #pragma unroll 1
@@ -180,6 +189,7 @@ k_qp(int64_t nprob, const double *__restrict__ parts, int S, const double *__res
             const int e = tri_index(k, k2);
             double s = 0.0;
             for (int sl = 0; sl < S; ++sl) s += src[(size_t)sl * stride + e];
+            if (k == k2) s *= dscale;
             A(k, k2) = s;
             A(k2, k) = s;
         }
@@ -231,7 +241,8 @@ k_qp(int64_t nprob, const double *__restrict__ parts, int S, const double *__res
         A(K + 1, K + 1) = 0.0;
     }
 
-    const int st = quadratic_program<K, C>(A, tmp, d, par, delta);
+    st = quadratic_program<K, C>(A, tmp, d, par, delta);
+    }   /* attempts */
     if (status) status[pr] = st;
     if (st == 0 && fail_count) atomicAdd(fail_count, 1);
 
@@ -265,13 +276,13 @@ cudaError_t prepare_qp_t()
 
 template <int K, bool SIMPLEX>
 cudaError_t launch_qp_t(int64_t nprob, const double *parts, int S, const double *x, double *x_next,
-                        int32_t *status, int32_t *fail_count, const double *vt, int mu_mode,
+                        int32_t *status, int32_t *fail_count, const double *vt, int mu_mode, int damp_retry,
                         cudaStream_t st)
 {
     const size_t smem = qp_smem<K, SIMPLEX>();
     if (nprob <= 0) return cudaSuccess;
     const unsigned grid = (unsigned)((nprob + QB - 1) / QB);
-    k_qp<K, SIMPLEX><<<grid, QB, smem, st>>>(nprob, parts, S, x, x_next, status, fail_count, vt, mu_mode);
+    k_qp<K, SIMPLEX><<<grid, QB, smem, st>>>(nprob, parts, S, x, x_next, status, fail_count, vt, mu_mode, damp_retry);
     return cudaGetLastError();
 }
 
@@ -279,11 +290,11 @@ cudaError_t launch_qp_t(int64_t nprob, const double *parts, int S, const double 
 
 cudaError_t launch_qp(int K, bool simplex, int64_t nprob, const double *parts, int S,
                       const double *x, double *x_next, int32_t *status, int32_t *fail_count,
-                      const double *vt, int mu_mode, cudaStream_t st)
+                      const double *vt, int mu_mode, int damp_retry, cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    if (simplex) { ADMIX_DISPATCH_K(K, (e = launch_qp_t<KK, true>(nprob, parts, S, x, x_next, status, fail_count, vt, mu_mode, st))); }
-    else { ADMIX_DISPATCH_K(K, (e = launch_qp_t<KK, false>(nprob, parts, S, x, x_next, status, fail_count, vt, mu_mode, st))); }
+    if (simplex) { ADMIX_DISPATCH_K(K, (e = launch_qp_t<KK, true>(nprob, parts, S, x, x_next, status, fail_count, vt, mu_mode, damp_retry, st))); }
+    else { ADMIX_DISPATCH_K(K, (e = launch_qp_t<KK, false>(nprob, parts, S, x, x_next, status, fail_count, vt, mu_mode, damp_retry, st))); }
     return e;
 }
 

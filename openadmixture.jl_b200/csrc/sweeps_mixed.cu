@@ -10,17 +10,16 @@
  *
  * Each Hessian is a GEMM whose rows are the 128 problems of a CTA (individuals or SNPs), whose
  * reduction runs over the other axis and whose columns are the K(K+1)/2 packed pairs k <= k2.
- * CUDA cores produce the BF16 weight tile (A) and the BF16 pair-product tile (B) of each chunk in
- * shared memory -- qp and 1-qp = sum_k q_k (1-p_k) in FP32 with paired __ffma2_rn, one
- * reciprocal per cell, the gradient in FP32 summed into FP64 per chunk -- and one thread issues
- * tcgen05.mma into an FP32 accumulator in tensor memory.  Tiles are double buffered, so the MMAs
- * of chunk c run while chunk c+1 is produced; completion is signalled on an mbarrier.  The
- * epilogue reads the accumulator with tcgen05.ld and writes the FP64 partial layout of the FP64
- * sweeps, so the QP kernels consume either.
+ * The K-term dot products qp = sum_k q_k p_k and sum_k q_k (1-p_k) of every cell also run on the
+ * tensor cores (TF32 split products); 1 - qp is that second sum plus 1 - sum_k q_k, which is the
+ * reference's 1 - qp for any Q.  CUDA cores turn each cell into one reciprocal, the BF16 weights
+ * of the Hessian GEMM and the FP32 gradient terms (summed into FP64 per chunk).  The epilogue
+ * reads the accumulator with tcgen05.ld and writes the FP64 partial layout of the FP64 sweeps,
+ * so the QP kernels consume either.
  *
  * Genotypes are read from the handle's padded layout: columns at a pitch that is a multiple of
  * 16 bytes, padding bytes and padding bits coded missing (01), so whole 16-byte groups can be
- * loaded without per-individual bound checks.  Requires sum_k q_k = 1 (every projected Q).
+ * loaded without per-individual bound checks.
  */
 #include "common.cuh"
 #include "kernels.h"
@@ -353,6 +352,16 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
         const int sh = valid ? (int)(i & 3) * 2 : 0;
         const uint32_t gmask = valid ? 0xFFFFu : 0u;    /* rows beyond I read code pair 01|01 */
+        /* 1 - qp = sum_k q_k (1 - p_k) + (1 - sum_k q_k): exact for any Q (the reference forms 1 - qp;
+         * EM priming leaves sum_k q_k < 1 where genotypes are missing) */
+        float sres = 0.f;
+        if (valid) {
+            double sq = 0.0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) sq += q[(size_t)K * i + k];
+            sres = (float)(1.0 - sq);
+        }
+        const float2 sres2 = make_float2(sres, sres);
         double gd[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) gd[k] = 0.0;
@@ -387,7 +396,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const uint32_t tb = gw >> sh;
                     const float4 a = tab[8 * ((tb & 3u) | ((tb >> 6) & 12u))];
                     const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
-                    const float2 om = make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1]));
+                    const float2 om = __fadd2_rn(make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1])), sres2);
                     const float2 pr = __fmul2_rn(qp, om);
                     const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
                     const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
@@ -491,7 +500,8 @@ struct MP {
     static constexpr int QS = MP_IC + 4;                        /* FP32 q row stride (floats) */
     static constexpr uint32_t PK_QB = B_BYTES;
     static constexpr uint32_t PK_QF = PK_QB + QB_BYTES;
-    static constexpr uint32_t PKG = PK_QF + K * QS * 4;
+    static constexpr uint32_t PK_S = PK_QF + K * QS * 4;         /* 1 - sum_k q_k per individual */
+    static constexpr uint32_t PKG = PK_S + MP_IC * 4;
     static constexpr uint32_t OFF_A = 0;
     static constexpr uint32_t OFF_PKG = A_BYTES;
     static constexpr uint32_t OFF_PA = OFF_PKG + MP_NPKG * PKG; /* P tile, then (1-P) tile */
@@ -517,6 +527,14 @@ k_p_pack(const double *__restrict__ q, int64_t I, uint8_t *__restrict__ pkg)
     float *qf = (float *)(buf + C::PK_QF);
     for (uint32_t t = tid; t < C::PKG / 16; t += 128) ((uint4 *)buf)[t] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
+    if (tid < MP_IC) {   /* 1 - qp = sum_k q_k (1 - p_k) + (1 - sum_k q_k), exact for any Q */
+        double sq = 1.0;
+        if (ic + tid < I) {
+            sq = 0.0;
+            for (int k = 0; k < K; ++k) sq += q[(size_t)K * (ic + tid) + k];
+        }
+        ((float *)(buf + C::PK_S))[tid] = (float)(1.0 - sq);
+    }
     for (int t = tid; t < K * MP_IC; t += 128) {
         const int ii = t / K, k = t - ii * K;
         const float a = (ic + ii < I) ? (float)q[(size_t)K * ic + t] : 1.0f / K;
@@ -718,6 +736,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         for (int c = 0; c < nchunk && ok; ++c) {
             const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
             const float *Qf = (const float *)(pk + C::PK_QF);
+            const float2 *Sres = (const float2 *)(pk + C::PK_S);
             uint32_t rq[32], ro[32];
             if (!wait(bar_qp, (uint32_t)(c & 1))) break;
             tc_fence_after_sync();
@@ -742,7 +761,8 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const uint32_t w = (m < 8) ? gcur.x : gcur.y;
                     const float4 a = tab[8 * ((w >> (4 * (m & 7))) & 15u)];
                     const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
-                    const float2 om = make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1]));
+                    const float2 om = __fadd2_rn(make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1])),
+                                                 Sres[m]);
                     const float2 pr = __fmul2_rn(qp, om);
                     const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
                     const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
@@ -845,6 +865,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
 {
     constexpr int PREF = (K * ML_IC + 127) / 128;
     __shared__ float2 Qs[2][K][ML_IC / 2];
+    __shared__ float2 Ss[2][ML_IC / 2];                 /* 1 - sum_k q_k per individual */
     __shared__ double red[4];
     const int tid = threadIdx.x;
     const int64_t j = (int64_t)blockIdx.x * 128 + tid;
@@ -860,7 +881,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
         const float pb = (float)(1.0 - pv);
         pbd[k] = make_float2(pb, pb);
     }
-    float qr[PREF];
+    float qr[PREF], sreg = 0.f;
     uint4 gnext = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), g = gnext;
     auto load = [&](int64_t ic) {
 #pragma unroll
@@ -868,6 +889,14 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
             const int t = tid + u * 128;                 /* t = k * IC + ii */
             const int k = t / ML_IC, ii = t - k * ML_IC;
             qr[u] = (t < K * ML_IC && ic + ii < ib) ? (float)q[(size_t)K * (ic + ii) + k] : 1.0f / K;
+        }
+        if (tid < ML_IC) {   /* 1 - qp = sum_k q_k (1 - p_k) + (1 - sum_k q_k), exact for any Q */
+            double sq = 1.0;
+            if (ic + tid < ib) {
+                sq = 0.0;
+                for (int k = 0; k < K; ++k) sq += q[(size_t)K * (ic + tid) + k];
+            }
+            sreg = (float)(1.0 - sq);
         }
         gnext = col_load64(bed, pitch, j, valid, ic);
     };
@@ -880,6 +909,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
                 ((float *)Qs[s][k])[ii] = qr[u];
             }
         }
+        if (tid < ML_IC) ((float *)Ss[s])[tid] = sreg;
     };
     if (nchunk > 0) { load(ia); store(0); g = gnext; }
     if (nchunk > 1) load(ia + ML_IC);
@@ -891,7 +921,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
 #pragma unroll
         for (int m = 0; m < ML_IC / 2; ++m) {
             const uint32_t code4 = pair_code(g, m);
-            float2 qp = make_float2(0.f, 0.f), om = make_float2(0.f, 0.f);
+            float2 qp = make_float2(0.f, 0.f), om = Ss[s][m];
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 const float2 qv = Qs[s][k][m];

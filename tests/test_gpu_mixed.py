@@ -101,3 +101,25 @@ def test_mixed_loglik_in_iteration_matches_fp64_verifier(oa, K, I, J):
         ll_qn = recs[-1]["ll_qn"]
         assert rel_err(ll_basic, h.loglik(oa.X_NEXT2)) < 1e-8
         assert rel_err(ll_qn, h.loglik(oa.X_TMP)) < 1e-8
+
+
+@pytest.mark.parametrize("K", [3, 8])
+def test_mixed_sweeps_match_fp64_after_em_priming(oa, K):
+    """After EM priming sum_k q_k < 1 where genotypes are missing (the reference's EM Q-step
+    divides by 2J); the mixed sweeps must still use the reference's 1 - qp, not sum_k q_k (1-p_k)."""
+    spec = oa.COHORTS["c1"].scaled(I=700, J=5000, K=K, seed=60 + K, miss=0.05)
+    g, _, _ = oa.make_cohort(spec)
+    d = oa.AdmixData(g.I, g.J, K, 3, rng=2)
+    with oa.CuAdmixData(d, g) as h:
+        oa.init_em(d, g, 2, d_cu=h, quiet=True)
+    assert np.abs(d.q.sum(0) - 1).max() > 1e-3          # the primed Q is off the simplex
+    h64 = oa.CuAdmixData(d, g)
+    hmx = oa.CuAdmixData(d, g, flags=oa.ADMIX_FLAG_MIXED)
+    for h in (h64, hmx):
+        h.upload(oa.X, d.x)
+    for side in ("q", "p"):
+        H0, z0 = getattr(h64, f"grad_hess_{side}")(oa.X, oa.X)
+        H1, z1 = getattr(hmx, f"grad_hess_{side}")(oa.X, oa.X)
+        assert _row_rel(z1, z0) < (GRAD_TOL if side == "q" else 1e-4), side
+        assert _row_rel(H1, H0) < HESS_TOL, side
+    h64.close(); hmx.close()
