@@ -83,6 +83,17 @@ def run_pass_only(args):
     return 0
 
 
+def max_over_ranks(value: float, world: int, device: str) -> float:
+    """The largest value over all ranks (device-timed milliseconds: the job's time is its
+    slowest rank's).  One collective on every rank when world > 1."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -343,10 +354,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, "cuda")
     work = spec.I * spec.J * spec.K ** 2
     value = world * work * args.steps / (ms_max / 1e3)
 
@@ -414,10 +422,7 @@ def run_ours(args, rank, world, local_rank):
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1) / e2e_steps
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_ms = float(te.item())
+    e2e_ms = max_over_ranks(e2e_ms, world, "cuda")
     xbytes = 8 * K * (spec.I + spec.J)
 
     d_cu.close()          # frees its copy of the genotypes before the time-to-converge legs
@@ -529,10 +534,7 @@ def run_batch(args, rank, world, local_rank):
     rec = b.run_qn(args.steps, 0.0)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    t = torch.tensor([rec["ms_device"]], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = max_over_ranks(rec["ms_device"], world, "cuda")
     value = world * work * args.steps / (ms / 1e3)
 
     # end to end through the public API: every member's q, p from pinned host memory, one batch
