@@ -28,6 +28,27 @@
 namespace {
 
 constexpr uint32_t MX_WAIT_LIMIT = 1u << 22;   /* polls; an MMA batch completes in microseconds */
+/* Hessian accumulation blocks: every MX_HBLOCK chunks the FP32 TMEM accumulator is drained into
+ * the row's FP64 partials and the next MMA starts a fresh sum, so no FP32 partial sum sees more
+ * than 4 * MX_HBLOCK MMA accumulations (whose rounding is not to nearest) whatever J or I is. */
+constexpr int MX_HBLOCK = 256;
+
+/* add (or, for the first block, store) TMEM columns col .. col+N-1 of this thread's lane into the
+ * FP64 Hessian entries o[0 .. T-1] */
+template <int N, int T>
+__device__ __forceinline__ void hess_drain(uint32_t taddr, double *o, bool first, bool valid)
+{
+#pragma unroll 1
+    for (int c0 = 0; c0 < N; c0 += 16) {
+        float v[16];
+        tmem_ld16(taddr + (uint32_t)c0, v);
+        if (valid) {
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+                if (c0 + e < T) o[c0 + e] = first ? (double)v[e] : o[c0 + e] + (double)v[e];
+        }
+    }
+}
 
 __device__ __forceinline__ float rcp_approx(float x)
 {
@@ -332,7 +353,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                         for (int ks = 0; ks < 2; ++ks) {
                             const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
                             const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
-                            tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c > 0 || term > 0 || ks > 0) ? 1u : 0u);
+                            tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || term > 0 || ks > 0) ? 1u : 0u);
                         }
                     }
                     tc_commit(bar_h);
@@ -381,6 +402,12 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             if (!wait(&bar_p[c % MQ_NPKG], (uint32_t)((c / MQ_NPKG) & 1))) break;
             if (!wait(&bar_g[c & 1], (uint32_t)((c >> 1) & 1))) break;
             if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the weight tile is free */
+            if (c > 0 && c % MX_HBLOCK == 0) {   /* drain the block of chunks c-MX_HBLOCK .. c-1 */
+                tc_fence_after_sync();
+                hess_drain<N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E,
+                                 c == MX_HBLOCK, valid);
+                tc_fence_before_sync();
+            }
             const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);
             float2 gk[K], zs = make_float2(0.f, 0.f);
 #pragma unroll
@@ -453,11 +480,14 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             for (int c0 = 0; c0 < N; c0 += 16) {
                 float v[16];
                 tmem_ld16(tmem + lane_base + C::COL_H + (uint32_t)c0, v);
-                if (valid) {
+                if (valid) {   /* the last accumulation block, added to the drained ones */
                     double *o = out + ((size_t)blockIdx.y * I + i) * E;
+                    const bool first = nchunk <= MX_HBLOCK;
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        if (c0 + e < T) o[c0 + e] = ok ? (double)v[e] : __longlong_as_double(0x7ff8000000000000LL);
+                        if (c0 + e < T)
+                            o[c0 + e] = ok ? (first ? (double)v[e] : o[c0 + e] + (double)v[e])
+                                           : __longlong_as_double(0x7ff8000000000000LL);
                 }
             }
         } else if (valid) {
@@ -714,7 +744,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 for (int ks = 0; ks < 2; ++ks) {
                     const uint64_t ad = umma_desc_kmajor(abase + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
                     const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
-                    tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+                    tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || ks > 0) ? 1u : 0u);
                 }
                 tc_commit(bar_h);
             }
@@ -748,6 +778,12 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             if (lane == 0) mbar_arrive(bar_qfree);
             if (!wait(&bar_p[c % MP_NPKG], (uint32_t)((c / MP_NPKG) & 1))) break;
             if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the C tile is free */
+            if (c > 0 && c % MX_HBLOCK == 0) {   /* drain the block of chunks c-MX_HBLOCK .. c-1 */
+                tc_fence_after_sync();
+                hess_drain<N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E,
+                                 c == MX_HBLOCK, valid);
+                tc_fence_before_sync();
+            }
             float2 gk[K];
 #pragma unroll
             for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
@@ -817,11 +853,14 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             for (int c0 = 0; c0 < N; c0 += 16) {
                 float v[16];
                 tmem_ld16(tmem + lane_base + C::COL_H + (uint32_t)c0, v);
-                if (valid) {
+                if (valid) {   /* the last accumulation block, added to the drained ones */
                     double *o = out + ((size_t)blockIdx.y * J + j) * E;
+                    const bool first = nchunk <= MX_HBLOCK;
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        if (c0 + e < T) o[c0 + e] = ok ? (double)v[e] : __longlong_as_double(0x7ff8000000000000LL);
+                        if (c0 + e < T)
+                            o[c0 + e] = ok ? (first ? (double)v[e] : o[c0 + e] + (double)v[e])
+                                           : __longlong_as_double(0x7ff8000000000000LL);
                 }
             }
         } else if (valid) {
