@@ -123,6 +123,10 @@ int admix_update_p(admix_ctx *h, int32_t update2, int32_t *qp_status);
 
 /* One full iteration i on the device: 2 Q + 2 P SQP updates, loglik, ZAL secant update
  * (quasi_newton.jl:5-9,29-31), projection (projections.jl), loglik, accept/reject. */
+/* fix_q / fix_p of admixture_qn! (algorithms_outer.jl:63-116, passed through by run_admixture,
+ * driver.jl:169-197): later iterations (admix_qn_iteration, admix_run_qn, batches) copy the fixed
+ * block (q_next .= q, q_next2 .= q, likewise p) instead of updating it.  Default: neither. */
+int admix_set_fixed(admix_ctx *h, int32_t fix_q, int32_t fix_p);
 int admix_qn_iteration(admix_ctx *h, int32_t iter, admix_iterinfo *out);
 /* Iterations iter_offset+1 .. n_iter until reldiff < rtol.  hist (n_iter entries, may be
  * NULL) receives one record per iteration run. */

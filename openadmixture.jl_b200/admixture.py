@@ -284,8 +284,15 @@ def admixture_qn(d: AdmixData, g, iter: int = 1000, rtol: float = 1e-7, *, d_cu:
     d_cu = _require_gpu(d_cu)
     if mode != "ZAL":
         raise NotImplementedError(f"mode={mode!r}: only the :ZAL mode run_admixture uses is on the device path")
-    if fix_p or fix_q:
-        raise NotImplementedError("fix_p / fix_q are not on the device path")
+    d_cu._chk(N.admix_lib().admix_set_fixed(d_cu.handle, int(bool(fix_q)), int(bool(fix_p))))
+    try:
+        return _admixture_qn_loop(d, d_cu, iter, rtol, iter_count_offset, verbose, quiet)
+    finally:
+        d_cu._chk(N.admix_lib().admix_set_fixed(d_cu.handle, 0, 0))
+
+
+def _admixture_qn_loop(d: AdmixData, d_cu: CuAdmixData, iter: int, rtol: float, iter_count_offset: int,
+                       verbose: bool, quiet: bool) -> list[dict]:
     d_cu.upload(X, d.x)
     if math.isnan(d.ll_new):
         d.ll_new = d_cu.loglik(X)

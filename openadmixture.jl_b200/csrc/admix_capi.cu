@@ -24,6 +24,7 @@ struct admix_ctx {
     int64_t pitch = 0;               /* column stride of the device genotypes: Ib rounded up to 16 */
     int K = 0, Q = 0;
     uint32_t flags = 0;
+    int fix = 0;                     /* bit 0: fix_q, bit 1: fix_p (admixture_qn!'s keywords) */
     int dev = 0, sms = 148;
     cudaStream_t st = nullptr;
     uint8_t *bed = nullptr;
@@ -373,11 +374,15 @@ static cudaError_t enq_em(admix_ctx *h)
 static cudaError_t enq_iteration(admix_ctx *h)
 {
     const int64_t nx = (int64_t)h->K * (h->I + h->J);
+    /* fix_q / fix_p (algorithms_outer.jl:98-116): the fixed block is copied, not updated */
+    const size_t nq = sizeof(double) * (size_t)h->K * h->I, np = sizeof(double) * (size_t)h->K * h->J;
+    auto copy_q = [&](int dst) { return cudaMemcpyAsync(Qof(h, dst), Qof(h, ADMIX_X), nq, cudaMemcpyDeviceToDevice, h->st); };
+    auto copy_p = [&](int dst) { return cudaMemcpyAsync(Pof(h, dst), Pof(h, ADMIX_X), np, cudaMemcpyDeviceToDevice, h->st); };
     cudaError_t e = launch_iter_begin(h->sc, h->st);
-    if (e == cudaSuccess) e = enq_update_q(h, 0);
-    if (e == cudaSuccess) e = enq_update_p(h, 0);
-    if (e == cudaSuccess) e = enq_update_q(h, 1);
-    if (e == cudaSuccess) e = enq_update_p(h, 1);
+    if (e == cudaSuccess) e = (h->fix & 1) ? copy_q(ADMIX_X_NEXT) : enq_update_q(h, 0);
+    if (e == cudaSuccess) e = (h->fix & 2) ? copy_p(ADMIX_X_NEXT) : enq_update_p(h, 0);
+    if (e == cudaSuccess) e = (h->fix & 1) ? copy_q(ADMIX_X_NEXT2) : enq_update_q(h, 1);
+    if (e == cudaSuccess) e = (h->fix & 2) ? copy_p(ADMIX_X_NEXT2) : enq_update_p(h, 1);
     if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_NEXT2, &h->sc->ll_basic, true);
     if (e == cudaSuccess) e = launch_qn(h->Q, h->I, h->J, h->K, h->x[ADMIX_X], h->x[ADMIX_X_NEXT], h->x[ADMIX_X_NEXT2],
                                         h->U, h->V, h->x[ADMIX_X_TMP], h->qn_partial, h->qnp, h->sc, h->sms, h->st);
@@ -542,6 +547,19 @@ static int run_one(admix_ctx *h, int32_t iter, admix_iterinfo *out)
         out->ll_prev = s.ll_prev; out->ll_basic = s.ll_basic; out->ll_qn = s.ll_qn;
         out->ll_new = s.ll_new; out->reldiff = s.reldiff; out->iter = iter;
         out->accepted_qn = s.accepted; out->qp_fail_q = s.fail_q; out->qp_fail_p = s.fail_p;
+    }
+    return ADMIX_OK;
+}
+
+int admix_set_fixed(admix_ctx *h, int32_t fix_q, int32_t fix_p)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    const int fix = (fix_q ? 1 : 0) | (fix_p ? 2 : 0);
+    if (fix != h->fix) {
+        CK(h, cudaStreamSynchronize(h->st));
+        if (h->iter_graph) { cudaGraphExecDestroy(h->iter_graph); h->iter_graph = nullptr; }
+        if (h->iter_graph_def) { cudaGraphDestroy(h->iter_graph_def); h->iter_graph_def = nullptr; }
+        h->fix = fix;
     }
     return ADMIX_OK;
 }
@@ -1014,6 +1032,7 @@ int admix_batch_run_qn(admix_batch *b, int32_t n_iter, double rtol, int32_t *n_d
     }
     rc = batch_sync_members(b);
     if (rc != ADMIX_OK) return rc;
+    batch_invalidate(b);                                /* members' fixed-block modes may have changed */
     std::vector<int> active(n), done(n, 0), conv(n, 0);
     for (int t = 0; t < n; ++t) active[t] = t;
     std::vector<admix_iterinfo> rec((size_t)n);

@@ -485,7 +485,7 @@ typedef struct {
     double *vt;                                 /* K x K */
     double ll_prev, ll_new;
     int32_t mu_mode;
-    int32_t pad;
+    int32_t fix;                                /* bit 0: fix_q, bit 1: fix_p (algorithms_outer.jl:98-116) */
 } orc_state;
 
 static double *Qof(orc_state *s, double *x) { (void)s; return x; }
@@ -658,8 +658,10 @@ void orc_qn_step(orc_state *s, int iter)
     }
 }
 
-/* One iteration of admixture_qn! (algorithms_outer.jl:92-159), mode = :ZAL, no fix_q/fix_p.
- * info[0..4] = (prev, basic, qn, new, reldiff).  Returns 1 when reldiff < rtol. */
+/* One iteration of admixture_qn! (algorithms_outer.jl:92-159), mode = :ZAL.  With fix_q / fix_p
+ * (s->fix bits 0 / 1) the block is copied instead of updated: q_next .= q, q_next2 .= q
+ * (algorithms_outer.jl:98-116), likewise p.  info[0..4] = (prev, basic, qn, new, reldiff).
+ * Returns 1 when reldiff < rtol. */
 int orc_qn_iteration(orc_state *s, int iter, double rtol, double *info,
                      int32_t *st_q, int32_t *st_p)
 {
@@ -667,10 +669,11 @@ int orc_qn_iteration(orc_state *s, int iter, double rtol, double *info,
     const int64_t I = s->I, J = s->J;
     s->ll_prev = s->ll_new;
     double ll_prev = s->ll_prev;
-    orc_update_q(s, 0, st_q);
-    orc_update_p(s, 0, st_p);
-    orc_update_q(s, 1, st_q);
-    orc_update_p(s, 1, st_p);
+    const size_t nq = sizeof(double) * (size_t)K * I, np = sizeof(double) * (size_t)K * J;
+    if (s->fix & 1) memcpy(Qof(s, s->x_next), Qof(s, s->x), nq); else orc_update_q(s, 0, st_q);
+    if (s->fix & 2) memcpy(Pof(s, s->x_next), Pof(s, s->x), np); else orc_update_p(s, 0, st_p);
+    if (s->fix & 1) memcpy(Qof(s, s->x_next2), Qof(s, s->x), nq); else orc_update_q(s, 1, st_q);
+    if (s->fix & 2) memcpy(Pof(s, s->x_next2), Pof(s, s->x), np); else orc_update_p(s, 1, st_p);
     s->ll_prev = ll_prev;
     double ll_basic = orc_loglik_x(s, s->x_next2);
     orc_qn_step(s, iter);

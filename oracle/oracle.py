@@ -32,7 +32,7 @@ class OrcState(C.Structure):
         ("XtX_q", _D), ("Xtz_q", _D), ("XtX_p", _D), ("Xtz_p", _D),
         ("U", _D), ("V", _D), ("vt", _D),
         ("ll_prev", C.c_double), ("ll_new", C.c_double),
-        ("mu_mode", C.c_int32), ("pad", C.c_int32),
+        ("mu_mode", C.c_int32), ("fix", C.c_int32),
     ]
 
 
@@ -170,7 +170,7 @@ class OracleRun:
     """Oracle mirror of AdmixData + the outer loop (structs.jl, algorithms_outer.jl)."""
 
     def __init__(self, bed: np.ndarray, I: int, J: int, K: int, Q: int, x0: np.ndarray,
-                 mu_mode: int = MU_AS_EXECUTED):
+                 mu_mode: int = MU_AS_EXECUTED, fix_q: bool = False, fix_p: bool = False):
         self.bed = np.ascontiguousarray(bed)
         self.I, self.J, self.K, self.Q = I, J, K, Q
         n = I + J
@@ -188,6 +188,7 @@ class OracleRun:
         s.U, s.V, s.vt = _d(self.U), _d(self.V), _d(self.vt)
         s.ll_prev = math.nan; s.ll_new = math.nan
         s.mu_mode = mu_mode
+        s.fix = (1 if fix_q else 0) | (2 if fix_p else 0)
         self.s = s
 
     @property

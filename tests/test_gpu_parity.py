@@ -298,3 +298,38 @@ def test_device_generated_cohort_and_device_create(oa):
         h.close()
     assert lls[0][0] == lls[1][0]
     assert np.array_equal(lls[0][1][0], lls[1][1][0]) and np.array_equal(lls[0][1][1], lls[1][1][1])
+
+
+@pytest.mark.parametrize("fix_q,fix_p", [(False, True), (True, False)])
+def test_fixed_block_iterations_match_oracle(oa, orc, fix_q, fix_p):
+    """admixture_qn!(...; fix_q, fix_p) (algorithms_outer.jl:98-116): the fixed block is copied,
+    not updated; the other block and the QN step match the oracle, and the fixed block ends as
+    it started (up to the projection the reference applies to the QN point)."""
+    K = 4
+    g = _cohort(oa, I=300, J=1500, K=K, seed=44)
+    d, d_cu = _handle(oa, g, K, Q=3, seed=6)
+    r = orc.OracleRun(g.data, g.I, g.J, K, 3, d.x, fix_q=fix_q, fix_p=fix_p)
+    r.init_em(3)
+    d.x[:] = r.x
+    d.ll_new = r.ll_new
+    x0 = d.x.copy()
+    recs = oa.admixture_qn(d, g, 5, 0.0, d_cu=d_cu, quiet=True, fix_q=fix_q, fix_p=fix_p)
+    for it, rec in enumerate(recs, start=1):
+        o = r.qn_iteration(it)
+        for k in ("ll_prev", "ll_basic", "ll_qn", "ll_new"):
+            assert rel_err(rec[k], o[k]) < 1e-8, (it, k, rec[k], o[k])
+    assert np.max(np.abs(d.x - r.x)) < 1e-6
+    fixed = slice(0, g.I) if fix_q else slice(g.I, None)
+    moved = slice(g.I, None) if fix_q else slice(0, g.I)
+    diff = d.x[fixed] - x0[fixed]
+    if fix_q:   # the QN point's simplex projection: one shift per individual, rows summing to 1
+        assert np.max(np.ptp(diff, axis=1)) < 1e-9
+        assert np.max(np.abs(d.x[: g.I].sum(1) - 1.0)) < 1e-9
+    else:       # P of the EM point is already inside [1e-5, 1 - 1e-5]
+        assert np.max(np.abs(diff)) < 1e-12
+    assert np.max(np.abs(d.x[moved] - x0[moved])) > 1e-3
+    # the mode is per call: the next plain call updates both blocks again
+    x1 = d.x.copy()
+    oa.admixture_qn(d, g, 1, 0.0, d_cu=d_cu, quiet=True)
+    assert np.max(np.abs(d.x[fixed] - x1[fixed])) > 1e-6
+    d_cu.close()

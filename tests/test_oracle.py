@@ -260,3 +260,20 @@ def test_loglik_tiling_matches_plain_sum(oa, orc):
     qp = q @ p.T
     want = np.sum(nm * (gg * np.log(qp) + (2 - gg) * np.log(1 - qp)))
     assert rel_err(orc.loglik(g.data, g.I, g.J, 4, q, p), want) < 1e-12
+
+
+def test_oracle_fix_p_keeps_p_and_raises_loglik(oa, orc):
+    """fix_p (supervised projection analysis): P is carried over unchanged, Q is fitted, and the
+    log-likelihood never decreases (algorithms_outer.jl:98-116)."""
+    spec = oa.COHORTS["c1"].scaled(I=150, J=600, K=3, seed=17)
+    g, q, p = oa.make_cohort(spec)
+    x0 = oa.init_x(g.I, g.J, 3, 2)
+    x0[g.I:] = p                                       # the true P, fixed
+    r = orc.OracleRun(g.data, g.I, g.J, 3, 3, x0, fix_p=True)
+    r.ll_new = float("nan")
+    lls = []
+    for it in range(1, 8):
+        lls.append(r.qn_iteration(it)["ll_new"])
+    assert np.all(np.diff(lls) >= -1e-9 * abs(lls[0]))
+    assert np.max(np.abs(r.x[g.I:] - np.clip(p, 1e-5, 1 - 1e-5))) < 1e-12
+    assert np.max(np.abs(r.x[: g.I] - x0[: g.I])) > 1e-2
