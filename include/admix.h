@@ -74,6 +74,15 @@ int admix_create(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed,
  * (src_pitch >= ceil(I/4)).  The bytes are copied; the caller keeps ownership of d_bed. */
 int admix_create_device(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *d_bed, int64_t src_pitch,
                         uint32_t flags, admix_ctx **out);
+/* Out-of-core variant of admix_create for cohorts whose packed genotypes do not fit in device
+ * memory (the reference needs the whole BED on the device, cuda/structs.jl:36-37): the genotypes
+ * stay in the caller's host memory -- page-locked in place for the handle's lifetime, so they
+ * must stay valid and unchanged until admix_destroy -- and every pass streams them in blocks of
+ * block_snps SNPs (a positive multiple of 32) through two device buffers, the copy of the next
+ * block overlapping the compute of the current one.  Results equal admix_create's up to the
+ * order of the FP64 sums. */
+int admix_create_streamed(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed, int64_t block_snps,
+                          uint32_t flags, admix_ctx **out);
 int admix_destroy(admix_ctx *h);
 /* Last error message of h (or of the calling thread's last failed admix_create when h is NULL). */
 const char *admix_last_error(const admix_ctx *h);

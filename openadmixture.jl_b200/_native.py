@@ -69,6 +69,8 @@ _U8 = C.POINTER(C.c_uint8)
 ADMIX_SIGNATURES = {
     "admix_create": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, C.c_int32, _U8, C.c_uint32, C.POINTER(_P)]),
     "admix_create_device": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, C.c_int32, _P, C.c_int64, C.c_uint32, C.POINTER(_P)]),
+    "admix_create_streamed": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, C.c_int32, _U8, C.c_int64, C.c_uint32,
+                                        C.POINTER(_P)]),
     "admix_destroy": (C.c_int, [_P]),
     "admix_last_error": (C.c_char_p, [_P]),
     "admix_device_bytes": (C.c_int, [_P, _I64]),

@@ -75,12 +75,21 @@ class CuAdmixData:
     genotypes, the four iterates, the secant matrices and the sweep workspaces, owned by one
     libadmix handle."""
 
-    def __init__(self, d: AdmixData, g: Genotypes, *, flags: int = 0):
+    def __init__(self, d: AdmixData, g: Genotypes, *, flags: int = 0, stream_block: int | None = None):
+        """stream_block: keep the genotypes in host memory and stream them through the device in
+        blocks of that many SNPs (a multiple of 32) -- for cohorts larger than device memory."""
         if (g.I, g.J) != (d.I, d.J):
             raise ValueError(f"genotypes are {g.I} x {g.J}, AdmixData is {d.I} x {d.J}")
         lib = N.admix_lib()
         h = C.c_void_p()
-        if isinstance(g, DeviceGenotypes):
+        self._host_bed = None
+        if stream_block is not None:
+            if isinstance(g, DeviceGenotypes):
+                raise ValueError("stream_block needs genotypes in host memory")
+            self._host_bed = np.ascontiguousarray(g.data)      # must outlive the handle
+            N.check(lib.admix_create_streamed(d.I, d.J, d.K, d.Q, N.u8ptr(self._host_bed), int(stream_block), flags,
+                                              C.byref(h)), None)
+        elif isinstance(g, DeviceGenotypes):
             N.check(lib.admix_create_device(d.I, d.J, d.K, d.Q, C.c_void_p(g.data.data_ptr()), g.Ib, flags,
                                             C.byref(h)), None)
         else:
@@ -195,12 +204,13 @@ def _require_gpu(d_cu) -> CuAdmixData:
     return d_cu
 
 
-def _cu_admixture_base(d: AdmixData, g: Genotypes, I: int, J: int, *, flags: int = 0):
+def _cu_admixture_base(d: AdmixData, g: Genotypes, I: int, J: int, *, flags: int = 0,
+                       stream_block: int | None = None):
     """Allocate the device state and upload the genotype bytes once (cuda/structs.jl:33-39).
     Returns (d_cu, g_cu); the genotypes live inside d_cu, so g_cu is the same object."""
     if (I, J) != (d.I, d.J):
         raise ValueError("I, J disagree with AdmixData")
-    d_cu = CuAdmixData(d, g, flags=flags)
+    d_cu = CuAdmixData(d, g, flags=flags, stream_block=stream_block)
     return d_cu, d_cu
 
 
@@ -334,7 +344,7 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
                   admix_rtol: float = 1e-7, admix_n_em_iters: int = 5, T=np.float64, Q: int = 3,
                   use_gpu: bool = True, verbose: bool = False, progress_bar: bool = False,
                   fix_q: bool = False, fix_p: bool = False, init_q=None, init_p=None,
-                  quiet: bool = False, flags: int = 0, warm_start=None):
+                  quiet: bool = False, flags: int = 0, warm_start=None, stream_block: int | None = None):
     """run_admixture(filename, K; ...) (driver.jl:35-75) -> (d, clusters, aims).
 
     ``filename`` is a .bed path, an in-memory Genotypes or a DeviceGenotypes.  ``rng`` is an
@@ -345,7 +355,9 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
     (driver.jl:180); a given one overwrites the primed value.  warm_start ("learned", a model
     path or a WarmStartMLP) starts from the learned encoder's Q and the closed-form P instead
     of the random start, with no EM; where no model applies it falls back to the random start +
-    EM.  Explicit init_q / init_p take precedence over the warm start."""
+    EM.  Explicit init_q / init_p take precedence over the warm start.  stream_block keeps the
+    genotypes in host memory and streams them in blocks of that many SNPs (cohorts larger than
+    device memory)."""
     if sparsity is not None:
         raise NotImplementedError("sparsity (SKFR AIM pre-selection) is outside the likelihood engine")
     if T not in (np.float64, float, "Float64"):
@@ -356,7 +368,7 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
     if not quiet:
         print(f"Loaded {g.I} samples and {g.J} SNPs")
     d = AdmixData(g.I, g.J, K, Q, rng=rng)
-    d_cu, g_cu = _cu_admixture_base(d, g, g.I, g.J, flags=flags)
+    d_cu, g_cu = _cu_admixture_base(d, g, g.I, g.J, flags=flags, stream_block=stream_block)
     try:
         if warm_start is not None and (init_q is None or init_p is None):
             from . import warmstart

@@ -29,6 +29,17 @@ struct admix_ctx {
     cudaStream_t st = nullptr;
     uint8_t *bed = nullptr;
     bool owns_bed = true;            /* false for batch members: the batch owns the genotypes */
+    /* out-of-core: the packed genotypes stay in the caller's (page-locked) host memory and every
+     * pass streams SNP blocks of blk columns through two device buffers */
+    bool streamed = false;
+    const uint8_t *host_bed = nullptr;
+    bool host_registered = false;
+    int64_t blk = 0;
+    int nblk = 1;
+    uint8_t *sbuf[2] = {nullptr, nullptr};
+    cudaStream_t cst = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_copied[2] = {nullptr, nullptr}, ev_freed[2] = {nullptr, nullptr};
+    double *ll_blk = nullptr;
     double *xbuf = nullptr;          /* 4 * K(I+J): x, x_next, x_next2, x_tmp */
     double *x[4] = {nullptr, nullptr, nullptr, nullptr};
     double *parts_q = nullptr, *parts_p = nullptr;
@@ -112,6 +123,15 @@ static void release(admix_ctx *h)
     if (h->iter_graph) cudaGraphExecDestroy(h->iter_graph);
     if (h->iter_graph_def) cudaGraphDestroy(h->iter_graph_def);
     if (h->bed && h->owns_bed) cudaFree(h->bed);
+    for (int b = 0; b < 2; ++b) {
+        if (h->sbuf[b]) cudaFree(h->sbuf[b]);
+        if (h->ev_copied[b]) cudaEventDestroy(h->ev_copied[b]);
+        if (h->ev_freed[b]) cudaEventDestroy(h->ev_freed[b]);
+    }
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ll_blk) cudaFree(h->ll_blk);
+    if (h->cst) { cudaStreamSynchronize(h->cst); cudaStreamDestroy(h->cst); }
+    if (h->host_registered) cudaHostUnregister((void *)h->host_bed);
     void *dps[] = {h->pkg, h->xbuf, h->parts_q, h->parts_p, h->U, h->V, h->vt, h->status_q,
                    h->status_p, h->ll_partial, h->qn_partial, h->sc, h->counts};
     for (void *p : dps)
@@ -143,7 +163,8 @@ static cudaError_t upload_genotypes(uint8_t *dst, int64_t pitch, const uint8_t *
 }
 
 static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed, bool on_device,
-                         int64_t src_pitch, uint32_t flags, admix_ctx **out, uint8_t *shared_bed = nullptr)
+                         int64_t src_pitch, uint32_t flags, admix_ctx **out, uint8_t *shared_bed = nullptr,
+                         int64_t stream_blk = 0)
 {
     if (!out) return fail(nullptr, ADMIX_ERR_ARG, "out is NULL");
     *out = nullptr;
@@ -182,7 +203,25 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     h->llm = plan_loglik_mixed(I, J, h->sms);
     h->qnp = plan_qn(nx, h->sms);
 
-    if (shared_bed) {
+    if (stream_blk > 0) {
+        h->streamed = true;
+        h->host_bed = bed;
+        h->blk = stream_blk;
+        h->nblk = (int)((J + stream_blk - 1) / stream_blk);
+        for (int b = 0; b < 2; ++b) {
+            TRY(dalloc(h, &h->sbuf[b], (size_t)h->pitch * stream_blk + 64));
+            TRYC(cudaMemsetAsync(h->sbuf[b], 0x55, (size_t)h->pitch * stream_blk + 64, h->st));
+            TRYC(cudaEventCreateWithFlags(&h->ev_copied[b], cudaEventDisableTiming));
+            TRYC(cudaEventCreateWithFlags(&h->ev_freed[b], cudaEventDisableTiming));
+        }
+        TRYC(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+        TRYC(cudaStreamCreateWithFlags(&h->cst, cudaStreamNonBlocking));
+        TRY(dalloc(h, &h->ll_blk, (size_t)h->nblk));
+        cudaError_t re = cudaHostRegister((void *)bed, (size_t)h->Ib * J, cudaHostRegisterDefault);
+        if (re == cudaSuccess) h->host_registered = true;
+        else if (re == cudaErrorHostMemoryAlreadyRegistered) cudaGetLastError();   /* already page-locked */
+        else TRYC(re);
+    } else if (shared_bed) {
         h->bed = shared_bed;
         h->owns_bed = false;
     } else {
@@ -190,7 +229,8 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     }
     TRY(dalloc(h, &h->xbuf, (size_t)4 * nx));
     for (int w = 0; w < 4; ++w) h->x[w] = h->xbuf + (size_t)w * nx;
-    TRY(dalloc(h, &h->parts_q, (size_t)std::max(h->sq.S, (flags & ADMIX_FLAG_MIXED) ? h->sqm.S : 1) * I * E));
+    TRY(dalloc(h, &h->parts_q, (size_t)std::max(std::max(h->sq.S, (flags & ADMIX_FLAG_MIXED) ? h->sqm.S : 1),
+                                                  h->nblk) * I * E));
     TRY(dalloc(h, &h->parts_p, (size_t)std::max(h->sp.S, (flags & ADMIX_FLAG_MIXED) ? h->spm.S : 1) * J * E));
     TRY(dalloc(h, &h->U, (size_t)nx * Q));
     TRY(dalloc(h, &h->V, (size_t)nx * Q));
@@ -206,7 +246,7 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     TRYC(cudaMallocHost((void **)&h->sc_host, sizeof(DevScalars)));
     TRYC(cudaMallocHost((void **)&h->iter_host, sizeof(int32_t)));
 
-    if (!shared_bed) TRYC(upload_genotypes(h->bed, h->pitch, bed, src_pitch, I, J, on_device, h->sms, h->st));
+    if (!shared_bed && !h->streamed) TRYC(upload_genotypes(h->bed, h->pitch, bed, src_pitch, I, J, on_device, h->sms, h->st));
     TRYC(cudaMemsetAsync(h->xbuf, 0, sizeof(double) * 4 * nx, h->st));
     TRYC(cudaMemsetAsync(h->U, 0, sizeof(double) * nx * Q, h->st));
     TRYC(cudaMemsetAsync(h->V, 0, sizeof(double) * nx * Q, h->st));
@@ -241,6 +281,14 @@ int admix_create_device(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_
         return fail(nullptr, ADMIX_ERR_ARG, "d_bed is not device memory");
     }
     return create_common(I, J, K, Q, d_bed, true, src_pitch, flags, out);
+}
+
+int admix_create_streamed(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8_t *bed, int64_t block_snps,
+                          uint32_t flags, admix_ctx **out)
+{
+    if (block_snps < 32 || block_snps % 32 != 0)
+        return fail(nullptr, ADMIX_ERR_ARG, "block_snps must be a positive multiple of 32 (got %lld)", (long long)block_snps);
+    return create_common(I, J, K, Q, bed, false, (I + 3) / 4, flags, out, nullptr, std::min<int64_t>(block_snps, (J + 31) / 32 * 32));
 }
 
 int admix_destroy(admix_ctx *h)
@@ -299,39 +347,113 @@ int admix_get_ll(admix_ctx *h, double *ll_new)
 
 /* ---- stream-ordered building blocks (no synchronisation) ---- */
 
+/* Run fn(bed, j0, nj, b) for every SNP block.  In-HBM handles: one call over all SNPs.  Streamed
+ * handles: block b is copied (2D, into the 16-byte pitch, padding coded missing) from page-locked
+ * host memory into device buffer b & 1 on the copy stream while block b-1 computes; events order
+ * the reuse of each buffer, so the whole pass can be captured into a graph. */
+template <class F>
+static cudaError_t for_blocks(admix_ctx *h, F fn)
+{
+    if (!h->streamed) return fn((const uint8_t *)h->bed, (int64_t)0, h->J, 0);
+    cudaError_t e = cudaEventRecord(h->ev_fork, h->st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->cst, h->ev_fork, 0);
+    for (int b = 0; b < h->nblk && e == cudaSuccess; ++b) {
+        const int s = b & 1;
+        const int64_t j0 = (int64_t)b * h->blk, nj = std::min(h->blk, h->J - j0);
+        if (b >= 2) e = cudaStreamWaitEvent(h->cst, h->ev_freed[s], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(h->sbuf[s], (size_t)h->pitch, h->host_bed + (size_t)j0 * h->Ib, (size_t)h->Ib,
+                                  (size_t)h->Ib, (size_t)nj, cudaMemcpyHostToDevice, h->cst);
+        if (e == cudaSuccess) e = launch_mask_tail(h->sbuf[s], h->I, nj, h->pitch, h->sms, h->cst);
+        if (e == cudaSuccess) e = cudaEventRecord(h->ev_copied[s], h->cst);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(h->st, h->ev_copied[s], 0);
+        if (e == cudaSuccess) e = fn((const uint8_t *)h->sbuf[s], j0, nj, b);
+        if (e == cudaSuccess) e = cudaEventRecord(h->ev_freed[s], h->st);
+    }
+    return e;
+}
+
+/* plans of one streamed block: one slice, so block b's Q-side partials are slice b and its
+ * P-side rows land at their global SNP index */
+static SweepPlan block_plan(SweepPlan pl, int64_t len)
+{
+    pl.S = 1;
+    pl.slice = len;
+    return pl;
+}
+
+/* number of Q-side partial slices the QP / EM finaliser must add */
+static int q_slices(const admix_ctx *h)
+{
+    if (h->streamed) return h->nblk;
+    return (h->flags & ADMIX_FLAG_MIXED) ? h->sqm.S : h->sq.S;
+}
+
 /* FP64 log-likelihood (the verifier); fast = 1 selects the FP32-cell form in mixed mode */
 static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst, bool fast = false)
 {
-    if (fast && (h->flags & ADMIX_FLAG_MIXED))
-        return launch_loglik_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, which), Pof(h, which), h->llm,
-                                   h->ll_partial, dst, &h->sc->tc_err, h->pkg, h->st);
-    return launch_loglik_f64(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, which), Pof(h, which), h->llp,
-                             h->ll_partial, dst, h->st);
+    const bool mx = fast && (h->flags & ADMIX_FLAG_MIXED);
+    auto one = [&](const uint8_t *bed, int64_t j0, int64_t nj, int b) -> cudaError_t {
+        double *o = h->streamed ? h->ll_blk + b : dst;
+        const double *P = Pof(h, which) + (size_t)h->K * j0;
+        if (mx) {
+            const SweepPlan pl = h->streamed ? plan_loglik_mixed(h->I, nj, h->sms) : h->llm;
+            return launch_loglik_mixed(h->K, bed, h->I, nj, h->pitch, Qof(h, which), P, pl, h->ll_partial, o,
+                                       &h->sc->tc_err, h->pkg, h->st);
+        }
+        const LoglikPlan pl = h->streamed ? plan_loglik(h->I, nj, h->sms) : h->llp;
+        return launch_loglik_f64(h->K, bed, h->I, nj, h->pitch, Qof(h, which), P, pl, h->ll_partial, o, h->st);
+    };
+    cudaError_t e = for_blocks(h, one);
+    if (e == cudaSuccess && h->streamed) e = launch_sum_doubles(h->ll_blk, h->nblk, dst, h->st);
+    return e;
 }
 
-/* Q-side gradient / Hessian sweep into parts_q; returns the number of slices written. */
-static cudaError_t enq_sweep_q(admix_ctx *h, int wq, int wp, int *S)
+/* Q-side gradient / Hessian sweep (mode 0) or EM sums (mode 1, FP64) into parts_q; returns the
+ * number of slices written. */
+static cudaError_t enq_sweep_q_mode(admix_ctx *h, int mode, int wq, int wp, int *S)
 {
-    if (h->flags & ADMIX_FLAG_MIXED) {
-        *S = h->sqm.S;
-        return launch_sweep_q_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sqm, h->parts_q,
-                                    &h->sc->tc_err, h->pkg, h->st);
-    }
-    *S = h->sq.S;
-    return launch_sweep_q_f64(h->K, 0, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sq, h->parts_q, h->st);
+    const bool mx = mode == 0 && (h->flags & ADMIX_FLAG_MIXED);
+    /* entries per individual: T + K (gradient / Hessian) or K (EM sums) */
+    const size_t slice = (size_t)h->I * (mode == 0 ? h->K * (h->K + 1) / 2 + h->K : h->K);
+    *S = q_slices(h);
+    return for_blocks(h, [&](const uint8_t *bed, int64_t j0, int64_t nj, int b) -> cudaError_t {
+        const double *P = Pof(h, wp) + (size_t)h->K * j0;
+        double *out = h->parts_q + (size_t)b * slice;
+        if (mx) {
+            const SweepPlan pl = h->streamed ? block_plan(h->sqm, nj) : h->sqm;
+            return launch_sweep_q_mixed(h->K, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, &h->sc->tc_err,
+                                        h->pkg, h->st);
+        }
+        const SweepPlan pl = h->streamed ? block_plan(h->sq, nj) : h->sq;
+        return launch_sweep_q_f64(h->K, mode, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, h->st);
+    });
 }
 
-/* P-side gradient / Hessian sweep into parts_p; returns the number of slices written. */
-static cudaError_t enq_sweep_p(admix_ctx *h, int wq, int wp, int *S)
+/* P-side gradient / Hessian sweep (mode 0) or EM sums (mode 1, FP64) into parts_p */
+static cudaError_t enq_sweep_p_mode(admix_ctx *h, int mode, int wq, int wp, int *S)
 {
-    if (h->flags & ADMIX_FLAG_MIXED) {
-        *S = h->spm.S;
-        return launch_sweep_p_mixed(h->K, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->spm, h->parts_p,
-                                    &h->sc->tc_err, h->pkg, h->st);
-    }
-    *S = h->sp.S;
-    return launch_sweep_p_f64(h->K, 0, h->bed, h->I, h->J, h->pitch, Qof(h, wq), Pof(h, wp), h->sp, h->parts_p, h->st);
+    const bool mx = mode == 0 && (h->flags & ADMIX_FLAG_MIXED);
+    /* entries per SNP: T + K (gradient / Hessian) or 2K (EM sums) */
+    const size_t row = (size_t)(mode == 0 ? h->K * (h->K + 1) / 2 + h->K : 2 * h->K);
+    *S = h->streamed ? 1 : (mx ? h->spm.S : h->sp.S);
+    return for_blocks(h, [&](const uint8_t *bed, int64_t j0, int64_t nj, int b) -> cudaError_t {
+        (void)b;
+        const double *P = Pof(h, wp) + (size_t)h->K * j0;
+        double *out = h->parts_p + (size_t)j0 * row;
+        if (mx) {
+            const SweepPlan pl = h->streamed ? block_plan(plan_sweep_p_mixed(h->K, h->I, nj, h->sms), (h->I + 31) / 32 * 32)
+                                             : h->spm;
+            return launch_sweep_p_mixed(h->K, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, &h->sc->tc_err,
+                                        h->pkg, h->st);
+        }
+        const SweepPlan pl = h->streamed ? block_plan(plan_sweep_p(h->K, h->I, nj, h->sms), (h->I + 3) / 4 * 4) : h->sp;
+        return launch_sweep_p_f64(h->K, mode, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, h->st);
+    });
 }
+
+static cudaError_t enq_sweep_q(admix_ctx *h, int wq, int wp, int *S) { return enq_sweep_q_mode(h, 0, wq, wp, S); }
+static cudaError_t enq_sweep_p(admix_ctx *h, int wq, int wp, int *S) { return enq_sweep_p_mode(h, 0, wq, wp, S); }
 
 /* update_q!: q_out = project_q(q + QP(H_q, -Xtz_q)) */
 static cudaError_t enq_update_q(admix_ctx *h, int update2)
@@ -363,10 +485,11 @@ static cudaError_t enq_update_p(admix_ctx *h, int update2)
 static cudaError_t enq_em(admix_ctx *h)
 {
     /* em_q! then em_p! (mode :base, both from (q, p)), then p, q <- next (algorithms_outer.jl:23-30) */
-    cudaError_t e = launch_sweep_q_f64(h->K, 1, h->bed, h->I, h->J, h->pitch, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st);
-    if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st);
-    if (e == cudaSuccess) e = launch_sweep_p_f64(h->K, 1, h->bed, h->I, h->J, h->pitch, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st);
-    if (e == cudaSuccess) e = launch_emp_finalize(h->J, h->K, h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st);
+    int Sq = 1, Sp = 1;
+    cudaError_t e = enq_sweep_q_mode(h, 1, ADMIX_X, ADMIX_X, &Sq);
+    if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, h->streamed ? h->nblk : h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st);
+    if (e == cudaSuccess) e = enq_sweep_p_mode(h, 1, ADMIX_X, ADMIX_X, &Sp);
+    if (e == cudaSuccess) e = launch_emp_finalize(h->J, h->K, h->streamed ? 1 : h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st);
     return e;
 }
 
@@ -414,8 +537,9 @@ int admix_loglik(admix_ctx *h, int32_t which, double *out)
 int admix_em_q(admix_ctx *h)
 {
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
-    CK(h, launch_sweep_q_f64(h->K, 1, h->bed, h->I, h->J, h->pitch, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sq, h->parts_q, h->st));
-    CK(h, launch_emq_finalize(h->I, h->K, h->J, h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st));
+    int S = 1;
+    CK(h, enq_sweep_q_mode(h, 1, ADMIX_X, ADMIX_X, &S));
+    CK(h, launch_emq_finalize(h->I, h->K, h->J, h->streamed ? h->nblk : h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st));
     CK(h, cudaStreamSynchronize(h->st));
     return ADMIX_OK;
 }
@@ -423,8 +547,9 @@ int admix_em_q(admix_ctx *h)
 int admix_em_p(admix_ctx *h)
 {
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
-    CK(h, launch_sweep_p_f64(h->K, 1, h->bed, h->I, h->J, h->pitch, Qof(h, ADMIX_X), Pof(h, ADMIX_X), h->sp, h->parts_p, h->st));
-    CK(h, launch_emp_finalize(h->J, h->K, h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st));
+    int S = 1;
+    CK(h, enq_sweep_p_mode(h, 1, ADMIX_X, ADMIX_X, &S));
+    CK(h, launch_emp_finalize(h->J, h->K, h->streamed ? 1 : h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st));
     CK(h, cudaStreamSynchronize(h->st));
     return ADMIX_OK;
 }
@@ -614,8 +739,8 @@ int admix_time_pass(admix_ctx *h, int32_t pass, int32_t reps, double *ms_per_lau
         case ADMIX_PASS_LOGLIK: return enq_loglik(h, ADMIX_X, &h->sc->ll_tmp, true);
         case ADMIX_PASS_QSWEEP: { int S; return enq_sweep_q(h, ADMIX_X, ADMIX_X, &S); }
         case ADMIX_PASS_PSWEEP: { int S; return enq_sweep_p(h, ADMIX_X, ADMIX_X, &S); }
-        case ADMIX_PASS_QQP: return launch_qp(h->K, true, h->I, h->parts_q, (h->flags & ADMIX_FLAG_MIXED) ? h->sqm.S : h->sq.S, Qof(h, ADMIX_X), Qof(h, ADMIX_X_TMP), h->status_q, nullptr, h->vt, mu, (h->flags & ADMIX_FLAG_MIXED) ? 1 : 0, h->st);
-        case ADMIX_PASS_PQP: return launch_qp(h->K, false, h->J, h->parts_p, (h->flags & ADMIX_FLAG_MIXED) ? h->spm.S : h->sp.S, Pof(h, ADMIX_X), Pof(h, ADMIX_X_TMP), h->status_p, nullptr, h->vt, 0, (h->flags & ADMIX_FLAG_MIXED) ? 1 : 0, h->st);
+        case ADMIX_PASS_QQP: return launch_qp(h->K, true, h->I, h->parts_q, q_slices(h), Qof(h, ADMIX_X), Qof(h, ADMIX_X_TMP), h->status_q, nullptr, h->vt, mu, (h->flags & ADMIX_FLAG_MIXED) ? 1 : 0, h->st);
+        case ADMIX_PASS_PQP: return launch_qp(h->K, false, h->J, h->parts_p, h->streamed ? 1 : ((h->flags & ADMIX_FLAG_MIXED) ? h->spm.S : h->sp.S), Pof(h, ADMIX_X), Pof(h, ADMIX_X_TMP), h->status_p, nullptr, h->vt, 0, (h->flags & ADMIX_FLAG_MIXED) ? 1 : 0, h->st);
         default: return enq_em(h);
         }
     };
@@ -666,7 +791,10 @@ int admix_decode_counts(admix_ctx *h, int64_t *miss_per_snp, int64_t *miss_per_i
 {
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
     CK(h, cudaMemsetAsync(h->counts, 0, sizeof(unsigned long long) * (h->I + h->J), h->st));
-    CK(h, launch_decode_counts(h->bed, h->I, h->J, h->pitch, h->counts + h->I, h->counts, h->sms, h->st));
+    CK(h, for_blocks(h, [&](const uint8_t *bed, int64_t j0, int64_t nj, int b) -> cudaError_t {
+        (void)b;
+        return launch_decode_counts(bed, h->I, nj, h->pitch, h->counts + h->I + j0, h->counts, h->sms, h->st);
+    }));
     if (miss_per_snp) CK(h, cudaMemcpyAsync(miss_per_snp, h->counts + h->I, sizeof(int64_t) * h->J, cudaMemcpyDeviceToHost, h->st));
     if (miss_per_ind) CK(h, cudaMemcpyAsync(miss_per_ind, h->counts, sizeof(int64_t) * h->I, cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaStreamSynchronize(h->st));

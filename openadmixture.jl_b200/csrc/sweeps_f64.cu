@@ -510,6 +510,12 @@ cudaError_t launch_expand_hess(int64_t nprob, int K, int S, const double *parts,
     return cudaGetLastError();
 }
 
+cudaError_t launch_sum_doubles(const double *src, int64_t n, double *dst, cudaStream_t st)
+{
+    k_sum_partials<<<1, 1024, 0, st>>>(src, n, dst);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                  unsigned long long *miss_snp, unsigned long long *miss_ind,
                                  int sms, cudaStream_t st)

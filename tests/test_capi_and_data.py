@@ -134,3 +134,13 @@ def test_batch_create_rejects_bad_arguments_without_touching_a_gpu(oa):
     assert lib.admix_batch_create_device(40, 4, None, 9, 2, ok, 3, 0, C.byref(b)) == N.ADMIX_ERR_ARG
     assert lib.admix_batch_run_qn(None, 5, 1e-7, None, None, None, None) == N.ADMIX_ERR_ARG
     assert lib.admix_batch_destroy(None) == N.ADMIX_OK
+
+
+def test_streamed_create_rejects_bad_block_size(oa):
+    from openadmixture_b200 import _native as N
+    lib = N.admix_lib()
+    h = C.c_void_p()
+    bed = np.zeros((64, 1), np.uint8)
+    assert lib.admix_create_streamed(4, 64, 3, 3, N.u8ptr(bed), 48, 0, C.byref(h)) == N.ADMIX_ERR_ARG
+    assert b"multiple of 32" in lib.admix_last_error(None)
+    assert lib.admix_create_streamed(4, 64, 3, 3, N.u8ptr(bed), 0, 0, C.byref(h)) == N.ADMIX_ERR_ARG

@@ -333,3 +333,45 @@ def test_fixed_block_iterations_match_oracle(oa, orc, fix_q, fix_p):
     oa.admixture_qn(d, g, 1, 0.0, d_cu=d_cu, quiet=True)
     assert np.max(np.abs(d.x[fixed] - x1[fixed])) > 1e-6
     d_cu.close()
+
+
+@pytest.mark.parametrize("flags", [0, 2])
+def test_streamed_handle_matches_resident_handle(oa, flags):
+    """admix_create_streamed: the genotypes stay in host memory and every pass streams SNP blocks
+    (here 3: 1024 + 1024 + 953 SNPs); results equal the device-resident handle's up to the order
+    of the FP64 sums."""
+    K = 4
+    g = _cohort(oa, I=437, J=3001, K=K, seed=52)
+    d = oa.AdmixData(g.I, g.J, K, 3, rng=3)
+    hr = oa.CuAdmixData(d, g, flags=flags)
+    hs = oa.CuAdmixData(d, g, flags=flags, stream_block=1024)
+    for h in (hr, hs):
+        h.upload(oa.X, d.x)
+    assert rel_err(hs.loglik(oa.X), hr.loglik(oa.X)) < 1e-13
+    tol = 1e-12 if flags == 0 else 1e-6
+    for side in ("q", "p"):
+        H0, z0 = getattr(hr, f"grad_hess_{side}")(oa.X, oa.X)
+        H1, z1 = getattr(hs, f"grad_hess_{side}")(oa.X, oa.X)
+        assert np.max(np.abs(z1 - z0)) <= tol * np.abs(z0).max(), side
+        assert np.max(np.abs(H1 - H0)) <= (tol if flags == 0 else 2e-2) * np.abs(H0).max(), side
+    assert all(np.array_equal(a, b) for a, b in zip(hs.decode_counts(), hr.decode_counts()))
+    d1, d2 = oa.AdmixData(g.I, g.J, K, 3, rng=3), oa.AdmixData(g.I, g.J, K, 3, rng=3)
+    oa.init_em(d1, g, 3, d_cu=hr, quiet=True)
+    oa.init_em(d2, g, 3, d_cu=hs, quiet=True)
+    assert rel_err(d2.ll_new, d1.ll_new) < 1e-12
+    r1 = oa.admixture_qn(d1, g, 4, 0.0, d_cu=hr, quiet=True)
+    r2 = oa.admixture_qn(d2, g, 4, 0.0, d_cu=hs, quiet=True)
+    # FP64: the same iteration up to the order of FP64 sums.  Mixed: the BF16 Hessian sums restart
+    # at every streamed block, so the Hessians differ at ~1e-4 and early iterates drift apart a
+    # little (the optimum does not move; test_run_admixture_streamed checks the converged value).
+    for a, b in zip(r1, r2):
+        assert rel_err(b["ll_new"], a["ll_new"]) < (1e-10 if flags == 0 else 1e-5)
+    hr.close(); hs.close()
+
+
+@pytest.mark.parametrize("flags", [0, 2])
+def test_run_admixture_streamed(oa, flags):
+    g = _cohort(oa, I=300, J=2000, K=3, seed=53)
+    d0, _, _ = oa.run_admixture(g, 3, rng=5, quiet=True)
+    d1, _, _ = oa.run_admixture(g, 3, rng=5, quiet=True, stream_block=512, flags=flags)
+    assert rel_err(d1.ll_new, d0.ll_new) < (1e-9 if flags == 0 else 1e-6)
