@@ -890,7 +890,9 @@ __device__ __forceinline__ uint32_t pair_code(const uint4 &g, int m)
 
 /* ===================================================================== loglik
  * loglikelihood_loop_skipmissing (loops.jl:517-539) with FP32 cells: thread = SNP, individuals
- * in pairs; each cell contributes qp^g (1-qp)^(2-g) (1 when missing), two cells' factors are
+ * in pairs; qp is an FP32 FMA chain and 1 - qp is formed from it by one subtraction (exact for
+ * qp >= 1/2), as the reference forms it; each cell contributes qp^g (1-qp)^(2-g) (1 when
+ * missing), two cells' factors are
  * multiplied in FP32 and folded into an FP64 running product whose exponent moves into an
  * integer every 12 pairs; one FP64 log per thread at the end.  Every product is rounded to
  * nearest, so the rounding error is a random walk far below the convergence test's resolution. */
@@ -903,8 +905,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
                double *__restrict__ partial)
 {
     constexpr int PREF = (K * ML_IC + 127) / 128;
-    __shared__ float2 Qs[2][K][ML_IC / 2];
-    __shared__ float2 Ss[2][ML_IC / 2];                 /* 1 - sum_k q_k per individual */
+    __shared__ float4 Qs[2][K][ML_IC / 4];              /* q of individuals 4m .. 4m+3 */
     __shared__ double red[4];
     const int tid = threadIdx.x;
     const int64_t j = (int64_t)blockIdx.x * 128 + tid;
@@ -912,15 +913,13 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
     const int64_t ia = (int64_t)blockIdx.y * islice;
     const int64_t ib = min(I, ia + islice);
     const int nchunk = (int)((ib - ia + ML_IC - 1) / ML_IC);
-    float2 pd[K], pbd[K];
+    float2 pd[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const double pv = valid ? p[(size_t)K * j + k] : 0.5;
         pd[k] = make_float2((float)pv, (float)pv);
-        const float pb = (float)(1.0 - pv);
-        pbd[k] = make_float2(pb, pb);
     }
-    float qr[PREF], sreg = 0.f;
+    float qr[PREF];
     uint4 gnext = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), g = gnext;
     auto load = [&](int64_t ic) {
 #pragma unroll
@@ -928,14 +927,6 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
             const int t = tid + u * 128;                 /* t = k * IC + ii */
             const int k = t / ML_IC, ii = t - k * ML_IC;
             qr[u] = (t < K * ML_IC && ic + ii < ib) ? (float)q[(size_t)K * (ic + ii) + k] : 1.0f / K;
-        }
-        if (tid < ML_IC) {   /* 1 - qp = sum_k q_k (1 - p_k) + (1 - sum_k q_k), exact for any Q */
-            double sq = 1.0;
-            if (ic + tid < ib) {
-                sq = 0.0;
-                for (int k = 0; k < K; ++k) sq += q[(size_t)K * (ic + tid) + k];
-            }
-            sreg = (float)(1.0 - sq);
         }
         gnext = col_load64(bed, pitch, j, valid, ic);
     };
@@ -948,7 +939,6 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
                 ((float *)Qs[s][k])[ii] = qr[u];
             }
         }
-        if (tid < ML_IC) ((float *)Ss[s])[tid] = sreg;
     };
     if (nchunk > 0) { load(ia); store(0); g = gnext; }
     if (nchunk > 1) load(ia + ML_IC);
@@ -958,15 +948,22 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
     for (int c = 0; c < nchunk; ++c) {
         const int s = c & 1;
 #pragma unroll
-        for (int m = 0; m < ML_IC / 2; ++m) {
-            const uint32_t code4 = pair_code(g, m);
-            float2 qp = make_float2(0.f, 0.f), om = Ss[s][m];
+        for (int m2 = 0; m2 < ML_IC / 4; ++m2) {
+            /* qp of two individual pairs (one 16-byte broadcast load of q per k) */
+            float2 qpa = make_float2(0.f, 0.f), qpb = make_float2(0.f, 0.f);
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                const float2 qv = Qs[s][k][m];
-                qp = __ffma2_rn(qv, pd[k], qp);
-                om = __ffma2_rn(qv, pbd[k], om);
+                const float4 qv = Qs[s][k][m2];
+                qpa = __ffma2_rn(make_float2(qv.x, qv.y), pd[k], qpa);
+                qpb = __ffma2_rn(make_float2(qv.z, qv.w), pd[k], qpb);
             }
+#pragma unroll
+            for (int hm = 0; hm < 2; ++hm) {
+            const int m = 2 * m2 + hm;
+            const uint32_t code4 = pair_code(g, m);
+            const float2 qp = hm ? qpb : qpa;
+            /* 1 - qp as the reference forms it, from the (unbiased) FP32 qp */
+            const float2 om = make_float2(1.f - qp.x, 1.f - qp.y);
             /* factor per code: 00 -> om^2, 01 -> 1, 10 -> qp om, 11 -> qp^2 */
             const uint32_t c0 = code4 & 3u, c1 = code4 >> 2;
             const float u0 = (c0 & 2u) ? qp.x : om.x, v0 = (c0 == 3u) ? qp.x : om.x;
@@ -978,6 +975,7 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
                 const int64_t bits = __double_as_longlong(prod);
                 ex += ((bits >> 52) & 0x7FF) - 1023;
                 prod = __longlong_as_double((bits & ~(0x7FFLL << 52)) | (1023LL << 52));
+            }
             }
         }
         const int64_t bits = __double_as_longlong(prod);
