@@ -484,10 +484,19 @@ static cudaError_t enq_update_p(admix_ctx *h, int update2)
 
 static cudaError_t enq_em(admix_ctx *h)
 {
-    /* em_q! then em_p! (mode :base, both from (q, p)), then p, q <- next (algorithms_outer.jl:23-30) */
+    /* em_q! then em_p! (mode :base, both from (q, p)), then p, q <- next (algorithms_outer.jl:23-30).
+     * The EM Q-step's sums are the Q-side gradient, so the mixed form takes them from its
+     * tensor-core gradient / Hessian sweep; the P-step (two sums per entry) stays FP64. */
     int Sq = 1, Sp = 1;
-    cudaError_t e = enq_sweep_q_mode(h, 1, ADMIX_X, ADMIX_X, &Sq);
-    if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, h->streamed ? h->nblk : h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st);
+    cudaError_t e;
+    if (h->flags & ADMIX_FLAG_MIXED) {
+        const int T = h->K * (h->K + 1) / 2;
+        e = enq_sweep_q_mode(h, 0, ADMIX_X, ADMIX_X, &Sq);
+        if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, Sq, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st, T + h->K, T);
+    } else {
+        e = enq_sweep_q_mode(h, 1, ADMIX_X, ADMIX_X, &Sq);
+        if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, h->streamed ? h->nblk : h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st);
+    }
     if (e == cudaSuccess) e = enq_sweep_p_mode(h, 1, ADMIX_X, ADMIX_X, &Sp);
     if (e == cudaSuccess) e = launch_emp_finalize(h->J, h->K, h->streamed ? 1 : h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st);
     return e;
@@ -561,10 +570,13 @@ static int enq_init_em(admix_ctx *h, int32_t iters, double *ll_hist)
         CK(h, enq_em(h));
         CK(h, cudaMemcpyAsync(Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), sizeof(double) * h->K * h->J, cudaMemcpyDeviceToDevice, h->st));
         CK(h, cudaMemcpyAsync(Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), sizeof(double) * h->K * h->I, cudaMemcpyDeviceToDevice, h->st));
-        CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_tmp));
-        if (ll_hist) CK(h, cudaMemcpyAsync(ll_hist + it, &h->sc->ll_tmp, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        /* the per-iteration values are reported only; the mixed form uses its FP32-cell pass */
+        if (ll_hist) {
+            CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_tmp, true));
+            CK(h, cudaMemcpyAsync(ll_hist + it, &h->sc->ll_tmp, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        }
     }
-    CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new));
+    CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new));   /* FP64: the first QN iteration's ll_prev */
     return ADMIX_OK;
 }
 

@@ -28,7 +28,7 @@ cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, i
 /* fixed-order FP64 sum of n doubles into *dst (one block) */
 cudaError_t launch_sum_doubles(const double *src, int64_t n, double *dst, cudaStream_t st);
 cudaError_t launch_emq_finalize(int64_t I, int K, int64_t J, int S, const double *parts,
-                                const double *q, double *q_next, int sms, cudaStream_t st);
+                                const double *q, double *q_next, int sms, cudaStream_t st, int E = 0, int off = 0);
 cudaError_t launch_emp_finalize(int64_t J, int K, int S, const double *parts, const double *p,
                                 double *p_next, int sms, cudaStream_t st);
 cudaError_t launch_expand_hess(int64_t nprob, int K, int S, const double *parts, double *XtX,

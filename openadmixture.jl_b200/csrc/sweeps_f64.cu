@@ -183,13 +183,17 @@ k_sweep_q_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pit
 }
 
 /* em_q! finalisation (algorithms_inner.jl:89): q_next[k,i] = q[k,i] * sum_s acc / (2J). */
-__global__ void k_emq_finalize(int64_t I, int K, int64_t J, int S, const double *__restrict__ parts,
+/* q_next[k,i] = q[k,i] sum_j (z1 p_k + z2 (1-p_k)) / 2J from S slices of per-individual rows of E
+ * entries whose sums start at entry off (E = K, off = 0 for the EM sweep; E = T + K, off = T for
+ * the gradient entries of a gradient / Hessian sweep, which are the same sums) */
+__global__ void k_emq_finalize(int64_t I, int K, int64_t J, int S, int E, int off, const double *__restrict__ parts,
                                const double *__restrict__ q, double *__restrict__ q_next)
 {
     const int64_t n = (int64_t)K * I;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / K, k = t - i * K;
         double s = 0.0;
-        for (int sl = 0; sl < S; ++sl) s += parts[(size_t)sl * n + t];
+        for (int sl = 0; sl < S; ++sl) s += parts[((size_t)sl * I + i) * E + off + k];
         q_next[t] = q[t] * s / (double)(2 * J);
     }
 }
@@ -489,9 +493,9 @@ static int grid_for(int64_t n, int sms)
 }
 
 cudaError_t launch_emq_finalize(int64_t I, int K, int64_t J, int S, const double *parts,
-                                const double *q, double *q_next, int sms, cudaStream_t st)
+                                const double *q, double *q_next, int sms, cudaStream_t st, int E, int off)
 {
-    k_emq_finalize<<<grid_for((int64_t)K * I, sms), 256, 0, st>>>(I, K, J, S, parts, q, q_next);
+    k_emq_finalize<<<grid_for((int64_t)K * I, sms), 256, 0, st>>>(I, K, J, S, E > 0 ? E : K, off, parts, q, q_next);
     return cudaGetLastError();
 }
 
