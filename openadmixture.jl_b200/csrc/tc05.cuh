@@ -162,7 +162,7 @@ __device__ __forceinline__ void tf32_split(float x, float &hi, float &lo)
     lo = __uint_as_float(l);
 }
 
-/* Bulk asynchronous copy global -> this CTA's shared memory (no multicast), completing `bytes`
+/* Bulk asynchronous copy global -> this CTA's own shared memory, completing `bytes`
  * of transaction count on the mbarrier; both addresses 16-byte aligned, bytes a multiple of 16. */
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *mbar)
 {
