@@ -431,9 +431,11 @@ static cudaError_t enq_sweep_q_mode(admix_ctx *h, int mode, int wq, int wp, int 
 }
 
 /* P-side gradient / Hessian sweep (mode 0) or EM sums (mode 1, FP64) into parts_p */
+/* mode 0: gradient / Hessian (tensor-core pipeline in the mixed form); 1: the EM sums in FP64;
+ * 2: the EM sums on the mixed pipeline (mixed handles only) */
 static cudaError_t enq_sweep_p_mode(admix_ctx *h, int mode, int wq, int wp, int *S)
 {
-    const bool mx = mode == 0 && (h->flags & ADMIX_FLAG_MIXED);
+    const bool mx = (mode == 0 && (h->flags & ADMIX_FLAG_MIXED)) || mode == 2;
     /* entries per SNP: T + K (gradient / Hessian) or 2K (EM sums) */
     const size_t row = (size_t)(mode == 0 ? h->K * (h->K + 1) / 2 + h->K : 2 * h->K);
     *S = h->streamed ? 1 : (mx ? h->spm.S : h->sp.S);
@@ -444,8 +446,8 @@ static cudaError_t enq_sweep_p_mode(admix_ctx *h, int mode, int wq, int wp, int 
         if (mx) {
             const SweepPlan pl = h->streamed ? block_plan(plan_sweep_p_mixed(h->K, h->I, nj, h->sms), (h->I + 31) / 32 * 32)
                                              : h->spm;
-            return launch_sweep_p_mixed(h->K, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, &h->sc->tc_err,
-                                        h->pkg, h->st);
+            return launch_sweep_p_mixed(h->K, mode == 2 ? 1 : 0, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out,
+                                        &h->sc->tc_err, h->pkg, h->st);
         }
         const SweepPlan pl = h->streamed ? block_plan(plan_sweep_p(h->K, h->I, nj, h->sms), (h->I + 3) / 4 * 4) : h->sp;
         return launch_sweep_p_f64(h->K, mode, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, h->st);
@@ -486,10 +488,12 @@ static cudaError_t enq_em(admix_ctx *h)
 {
     /* em_q! then em_p! (mode :base, both from (q, p)), then p, q <- next (algorithms_outer.jl:23-30).
      * The EM Q-step's sums are the Q-side gradient, so the mixed form takes them from its
-     * tensor-core gradient / Hessian sweep; the P-step (two sums per entry) stays FP64. */
+     * tensor-core gradient / Hessian sweep; its P-step sums come from the EM mode of the mixed
+     * P pipeline (FP32 cells, FP64 across chunks). */
     int Sq = 1, Sp = 1;
     cudaError_t e;
-    if (h->flags & ADMIX_FLAG_MIXED) {
+    const bool mixed = (h->flags & ADMIX_FLAG_MIXED) != 0;
+    if (mixed) {
         const int T = h->K * (h->K + 1) / 2;
         e = enq_sweep_q_mode(h, 0, ADMIX_X, ADMIX_X, &Sq);
         if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, Sq, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st, T + h->K, T);
@@ -497,8 +501,8 @@ static cudaError_t enq_em(admix_ctx *h)
         e = enq_sweep_q_mode(h, 1, ADMIX_X, ADMIX_X, &Sq);
         if (e == cudaSuccess) e = launch_emq_finalize(h->I, h->K, h->J, h->streamed ? h->nblk : h->sq.S, h->parts_q, Qof(h, ADMIX_X), Qof(h, ADMIX_X_NEXT), h->sms, h->st);
     }
-    if (e == cudaSuccess) e = enq_sweep_p_mode(h, 1, ADMIX_X, ADMIX_X, &Sp);
-    if (e == cudaSuccess) e = launch_emp_finalize(h->J, h->K, h->streamed ? 1 : h->sp.S, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st);
+    if (e == cudaSuccess) e = enq_sweep_p_mode(h, mixed ? 2 : 1, ADMIX_X, ADMIX_X, &Sp);
+    if (e == cudaSuccess) e = launch_emp_finalize(h->J, h->K, Sp, h->parts_p, Pof(h, ADMIX_X), Pof(h, ADMIX_X_NEXT), h->sms, h->st);
     return e;
 }
 
@@ -523,11 +527,32 @@ static cudaError_t enq_iteration(admix_ctx *h)
     return e;
 }
 
+/* The tensor-core sweeps of the mixed form bound every pipeline wait; one that runs out sets
+ * tc_err and leaves NaN in its outputs.  After the stream has drained and sc_host holds the
+ * device's flag, report it as a failed call and clear it. */
+static int tc_err_check(admix_ctx *h)
+{
+    if (!h->sc_host->tc_err) return ADMIX_OK;
+    h->sc_host->tc_err = 0;
+    CK(h, cudaMemsetAsync(&h->sc->tc_err, 0, sizeof(int32_t), h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return fail(h, ADMIX_ERR_CUDA, "a tensor-core sweep gave up waiting on its pipeline; this call's results are invalid");
+}
+
+/* drain the stream and check the flag (mixed handles only: the FP64 kernels never wait) */
+static int tc_err_sync(admix_ctx *h)
+{
+    if (h->flags & ADMIX_FLAG_MIXED)
+        CK(h, cudaMemcpyAsync(&h->sc_host->tc_err, &h->sc->tc_err, sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return tc_err_check(h);
+}
+
 static int read_scalars(admix_ctx *h)
 {
     CK(h, cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaStreamSynchronize(h->st));
-    return ADMIX_OK;
+    return tc_err_check(h);
 }
 
 extern "C" {
@@ -586,8 +611,7 @@ int admix_init_em(admix_ctx *h, int32_t iters, double *ll_hist)
     if (iters < 0) return fail(h, ADMIX_ERR_ARG, "iters must be >= 0");
     int rc = enq_init_em(h, iters, ll_hist);
     if (rc != ADMIX_OK) return rc;
-    CK(h, cudaStreamSynchronize(h->st));
-    return ADMIX_OK;
+    return tc_err_sync(h);
 }
 
 static int grad_hess_common(admix_ctx *h, bool qside, int32_t wq, int32_t wp, double *XtX, double *Xtz)
@@ -618,7 +642,7 @@ static int grad_hess_common(admix_ctx *h, bool qside, int32_t wq, int32_t wp, do
     cudaFree(d_XtX);
     cudaFree(d_Xtz);
     if (e != cudaSuccess) return fail(h, ADMIX_ERR_CUDA, "grad/hess sweep failed: %s", cudaGetErrorString(e));
-    return ADMIX_OK;
+    return tc_err_sync(h);
 }
 
 int admix_grad_hess_q(admix_ctx *h, int32_t which_q, int32_t which_p, double *XtX, double *Xtz)
@@ -636,8 +660,7 @@ int admix_update_q(admix_ctx *h, int32_t update2, int32_t *qp_status)
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
     CK(h, enq_update_q(h, update2 ? 1 : 0));
     if (qp_status) CK(h, cudaMemcpyAsync(qp_status, h->status_q, sizeof(int32_t) * h->I, cudaMemcpyDeviceToHost, h->st));
-    CK(h, cudaStreamSynchronize(h->st));
-    return ADMIX_OK;
+    return tc_err_sync(h);
 }
 
 int admix_update_p(admix_ctx *h, int32_t update2, int32_t *qp_status)
@@ -645,8 +668,7 @@ int admix_update_p(admix_ctx *h, int32_t update2, int32_t *qp_status)
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
     CK(h, enq_update_p(h, update2 ? 1 : 0));
     if (qp_status) CK(h, cudaMemcpyAsync(qp_status, h->status_p, sizeof(int32_t) * h->J, cudaMemcpyDeviceToHost, h->st));
-    CK(h, cudaStreamSynchronize(h->st));
-    return ADMIX_OK;
+    return tc_err_sync(h);
 }
 
 static int ensure_graph(admix_ctx *h)
@@ -1117,7 +1139,11 @@ int admix_batch_init_em(admix_batch *b, int32_t iters, double *ll_hist)
         int rc = enq_init_em(b->m[t], iters, ll_hist ? ll_hist + t * (size_t)iters : nullptr);
         if (rc != ADMIX_OK) return bfail(b, rc, "member %d: %s", (int)t, b->m[t]->err);
     }
-    return batch_sync_members(b);
+    for (size_t t = 0; t < b->m.size(); ++t) {
+        const int rc = tc_err_sync(b->m[t]);
+        if (rc != ADMIX_OK) return bfail(b, rc, "member %d: %s", (int)t, b->m[t]->err);
+    }
+    return ADMIX_OK;
 }
 
 int admix_batch_set_split(admix_batch *b, int32_t divisor)
@@ -1194,6 +1220,12 @@ int admix_batch_run_qn(admix_batch *b, int32_t n_iter, double rtol, int32_t *n_d
         total += f;
         std::vector<int> still;
         for (int t : active) {
+            if (e != cudaSuccess) break;
+            rc = tc_err_check(b->m[t]);   /* sc_host was copied inside the graph */
+            if (rc != ADMIX_OK) {
+                rc = bfail(b, rc, "member %d: %s", t, b->m[t]->err);
+                break;
+            }
             const DevScalars &s = *b->m[t]->sc_host;
             admix_iterinfo &r = rec[t];
             r.ll_prev = s.ll_prev; r.ll_basic = s.ll_basic; r.ll_qn = s.ll_qn; r.ll_new = s.ll_new;
@@ -1203,6 +1235,7 @@ int admix_batch_run_qn(admix_batch *b, int32_t n_iter, double rtol, int32_t *n_d
             if (s.reldiff < rtol) conv[t] = 1;
             else still.push_back(t);
         }
+        if (rc != ADMIX_OK) break;
         active.swap(still);
     }
     cudaEventDestroy(e0);

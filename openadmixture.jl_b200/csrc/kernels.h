@@ -47,10 +47,11 @@ cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J
 size_t sweep_q_mixed_pkg_bytes(int K, int64_t J);
 
 SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms);
-/* The mixed P sweep first builds its per-chunk Q packages in pkg (sweep_p_mixed_pkg_bytes). */
-cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                                 const double *p, const SweepPlan &pl, double *out, int *err, uint8_t *pkg,
-                                 cudaStream_t st);
+/* The mixed P sweep first builds its per-chunk Q packages in pkg (sweep_p_mixed_pkg_bytes).
+ * mode 0: gradient / Hessian rows (T + K); mode 1: the EM P-step's two sums (2K, k_emp_finalize). */
+cudaError_t launch_sweep_p_mixed(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
+                                 const double *q, const double *p, const SweepPlan &pl, double *out, int *err,
+                                 uint8_t *pkg, cudaStream_t st);
 size_t sweep_p_mixed_pkg_bytes(int K, int64_t I);
 SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms);
 /* err and pkg are accepted for symmetry with the sweeps; the log-likelihood stays on the CUDA cores. */

@@ -631,24 +631,31 @@ __device__ __forceinline__ uint2 col_load32(const uint8_t *__restrict__ bed, int
                  : make_uint2(0x55555555u, 0x55555555u);
 }
 
-/* Warp roles as in the Q sweep: warps 0-3 producers (thread = SNP row), warp 4 controller. */
+/* Warp roles as in the Q sweep: warps 0-3 producers (thread = SNP row), warp 4 controller.
+ *
+ * EMS = true is the EM P-step of em_p! (algorithms_inner.jl:108-141, loops.jl:700-721) on the
+ * same pipeline: per SNP the two sums sum_i nm g q_k / qp and sum_i nm (2-g) q_k / (1-qp)
+ * (rows of 2K, the FP64 EM sweep's layout, finalised by k_emp_finalize), with no Hessian tile,
+ * MMAs or drains; a package slot is handed back once the four producer warps have read it. */
 constexpr int MP_CTA = MP_THREADS + 32;
 
-template <int K>
+template <int K, bool EMS>
 __global__ void __launch_bounds__(MP_CTA, (K <= 10 ? 3 : 2))
 k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                 const uint8_t *__restrict__ pkg, const double *__restrict__ p, int64_t islice,
                 double *__restrict__ out, int *__restrict__ err)
 {
     using C = MP<K>;
-    constexpr int T = C::T, N = C::N, E = C::E;
+    constexpr int T = C::T, N = C::N, E = EMS ? 2 * K : C::E;
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    /* qp ready, qp consumed (4 warps), C tile written (4 warps), Hessian done, package [3] */
-    __shared__ uint64_t mbar[4 + MP_NPKG];
+    /* qp ready, qp consumed (4 warps), C tile written (4 warps), Hessian done, package landed [3],
+     * package read (4 warps, EM sums only) [3] */
+    __shared__ uint64_t mbar[4 + 2 * MP_NPKG];
     __shared__ uint32_t tmem_holder;
     __shared__ volatile int abort_flag;
     uint64_t *bar_qp = &mbar[0], *bar_qfree = &mbar[1], *bar_afull = &mbar[2], *bar_h = &mbar[3], *bar_p = &mbar[4];
+    uint64_t *bar_read = &mbar[4 + MP_NPKG];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool producer = warp < 4;
@@ -667,6 +674,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         mbar_init(bar_afull, 4);
         mbar_init(bar_h, 1);
         for (int b = 0; b < MP_NPKG; ++b) mbar_init(&bar_p[b], 1);
+        for (int b = 0; b < MP_NPKG; ++b) mbar_init(&bar_read[b], 4);
         abort_flag = 0;
         mbar_fence_init();
     }
@@ -736,6 +744,14 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     tc_commit(bar_qp);
                 }
             }
+            if constexpr (EMS) {
+                /* slot c % 3's (c / 3)-th reading; its next one needs the copy issued here */
+                if (c + MP_NPKG < nchunk && wait(&bar_read[c % MP_NPKG], (uint32_t)((c / MP_NPKG) & 1))) {
+                    fence_async_smem();
+                    copy_pkg(c + MP_NPKG);
+                }
+                continue;
+            }
             if (wait(bar_afull, (uint32_t)(c & 1)) && leader) {
                 tc_fence_after_sync();
                 const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
@@ -760,55 +776,89 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         uint2 gcur = make_uint2(0x55555555u, 0x55555555u), gnext = gcur;
         if (nchunk > 0) gcur = col_load32(bed, pitch, j, valid, ia);
         if (nchunk > 1) gnext = col_load32(bed, pitch, j, valid, ia + MP_IC);
-        double gd[K];
+        double gd[K], hd[EMS ? K : 1];
 #pragma unroll
         for (int k = 0; k < K; ++k) gd[k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < (EMS ? K : 1); ++k) hd[k] = 0.0;
         for (int c = 0; c < nchunk && ok; ++c) {
             const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
             const float *Qf = (const float *)(pk + C::PK_QF);
             const float2 *Sres = (const float2 *)(pk + C::PK_S);
-            uint32_t rq[32], ro[32];
+            /* qp / om of the chunk's 32 individuals; the EM sums hold twice the accumulators, so
+             * they read the columns in two halves of 16 (individuals 0-15, then 16-31) */
+            constexpr int RC = EMS ? 16 : 32;
+            uint32_t rq[RC], ro[RC];
+            auto release_qp = [&]() {
+                tc_fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(bar_qfree);
+            };
             if (!wait(bar_qp, (uint32_t)(c & 1))) break;
             tc_fence_after_sync();
-            tmem_ld32_nowait(tmem + lane_base, rq);
-            tmem_ld32_nowait(tmem + lane_base + C::COL_OM, ro);
-            tmem_wait_ld();
-            tc_fence_before_sync();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(bar_qfree);
-            if (!wait(&bar_p[c % MP_NPKG], (uint32_t)((c / MP_NPKG) & 1))) break;
-            if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the C tile is free */
-            if (c > 0 && c % MX_HBLOCK == 0) {   /* drain the block of chunks c-MX_HBLOCK .. c-1 */
-                tc_fence_after_sync();
-                hess_drain<N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E,
-                                 c == MX_HBLOCK, valid);
-                tc_fence_before_sync();
+            if constexpr (EMS) {
+                tmem_ld16_raw(tmem + lane_base, rq);
+                tmem_ld16_raw(tmem + lane_base + C::COL_OM, ro);
+                tmem_wait_ld();
+            } else {
+                tmem_ld32_nowait(tmem + lane_base, rq);
+                tmem_ld32_nowait(tmem + lane_base + C::COL_OM, ro);
+                tmem_wait_ld();
+                release_qp();
             }
-            float2 gk[K];
+            if (!wait(&bar_p[c % MP_NPKG], (uint32_t)((c / MP_NPKG) & 1))) break;
+            if constexpr (!EMS) {
+                if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the C tile is free */
+                if (c > 0 && c % MX_HBLOCK == 0) {   /* drain the block of chunks c-MX_HBLOCK .. c-1 */
+                    tc_fence_after_sync();
+                    hess_drain<N, T>(tmem + lane_base + C::COL_H,
+                                     out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E, c == MX_HBLOCK, valid);
+                    tc_fence_before_sync();
+                }
+            }
+            float2 gk[K], hk[EMS ? K : 1];
 #pragma unroll
             for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
 #pragma unroll
+            for (int k = 0; k < (EMS ? K : 1); ++k) hk[k] = make_float2(0.f, 0.f);
+#pragma unroll
             for (int kc = 0; kc < 4; ++kc) {
+                if constexpr (EMS) {
+                    if (kc == 2) {   /* the second half of the columns; then the qp columns are free */
+                        tc_fence_after_sync();
+                        tmem_ld16_raw(tmem + lane_base + 16u, rq);
+                        tmem_ld16_raw(tmem + lane_base + C::COL_OM + 16u, ro);
+                        tmem_wait_ld();
+                        release_qp();
+                    }
+                }
                 uint32_t cp[4];
-                float2 zz[4];
+                float2 zz[4], z2s[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int m = kc * 4 + e;
+                    const int r = 2 * (EMS ? (m & 7) : m);   /* this pair's column in rq / ro */
                     const uint32_t w = (m < 8) ? gcur.x : gcur.y;
                     const float4 a = tab[8 * ((w >> (4 * (m & 7))) & 15u)];
-                    const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
-                    const float2 om = __fadd2_rn(make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1])),
+                    const float2 qp = make_float2(__uint_as_float(rq[r]), __uint_as_float(rq[r + 1]));
+                    const float2 om = __fadd2_rn(make_float2(__uint_as_float(ro[r]), __uint_as_float(ro[r + 1])),
                                                  Sres[m]);
                     const float2 pr = __fmul2_rn(qp, om);
                     const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
                     const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
                     const float2 z1 = __fmul2_rn(make_float2(a.x, a.y), r1);
                     const float2 z2 = __fmul2_rn(make_float2(a.z, a.w), r2);
-                    const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
-                    zz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);              /* nm (g/qp - (2-g)/(1-qp)) */
-                    cp[e] = pack_bf16x2(cw.x, cw.y);
+                    if constexpr (EMS) {
+                        zz[e] = z1;                                             /* nm g / qp */
+                        z2s[e] = z2;                                            /* nm (2-g) / (1-qp) */
+                    } else {
+                        const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
+                        zz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);              /* nm (g/qp - (2-g)/(1-qp)) */
+                        cp[e] = pack_bf16x2(cw.x, cw.y);
+                    }
                 }
-                *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
+                if constexpr (!EMS)
+                    *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
                     const float4 q0 = *(const float4 *)(Qf + k * C::QS + kc * 8);
@@ -817,23 +867,51 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     gk[k] = __ffma2_rn(zz[1], make_float2(q0.z, q0.w), gk[k]);
                     gk[k] = __ffma2_rn(zz[2], make_float2(q1.x, q1.y), gk[k]);
                     gk[k] = __ffma2_rn(zz[3], make_float2(q1.z, q1.w), gk[k]);
+                    if constexpr (EMS) {
+                        hk[k] = __ffma2_rn(z2s[0], make_float2(q0.x, q0.y), hk[k]);
+                        hk[k] = __ffma2_rn(z2s[1], make_float2(q0.z, q0.w), hk[k]);
+                        hk[k] = __ffma2_rn(z2s[2], make_float2(q1.x, q1.y), hk[k]);
+                        hk[k] = __ffma2_rn(z2s[3], make_float2(q1.z, q1.w), hk[k]);
+                    }
                 }
+            }
+            if constexpr (EMS) {   /* the package is read: hand its slot back */
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar_read[c % MP_NPKG]);
             }
 #pragma unroll
             for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y;
+            if constexpr (EMS) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) hd[k] += (double)hk[k].x + (double)hk[k].y;
+            }
             if (c + 1 < nchunk) {
                 gcur = gnext;
                 if (c + 2 < nchunk) gnext = col_load32(bed, pitch, j, valid, ia + (int64_t)(c + 2) * MP_IC);
             }
-            fence_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(bar_afull);
+            if constexpr (!EMS) {
+                fence_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(bar_afull);
+            }
         }
-        if (nchunk > 0) wait(bar_h, (uint32_t)((nchunk - 1) & 1));   /* the last Hessian MMAs */
-        if (valid) {
-            double *o = out + ((size_t)blockIdx.y * J + j) * E;
+        if constexpr (EMS) {
+            if (valid) {   /* a thread whose wait gave up writes NaN sums (and err is set) */
+                double *o = out + ((size_t)blockIdx.y * J + j) * E;
+                const double bad = __longlong_as_double(0x7ff8000000000000LL);
 #pragma unroll
-            for (int k = 0; k < K; ++k) o[T + k] = gd[k];
+                for (int k = 0; k < K; ++k) {
+                    o[k] = ok ? gd[k] : bad;
+                    o[K + k] = ok ? hd[k] : bad;
+                }
+            }
+        } else {
+            if (nchunk > 0) wait(bar_h, (uint32_t)((nchunk - 1) & 1));   /* the last Hessian MMAs */
+            if (valid) {
+                double *o = out + ((size_t)blockIdx.y * J + j) * E;
+#pragma unroll
+                for (int k = 0; k < K; ++k) o[T + k] = gd[k];
+            }
         }
     }
     ok = __syncthreads_and(ok);
@@ -846,7 +924,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     }
     __syncthreads();
     tc_fence_after_sync();
-    if (producer) {
+    if (producer && !EMS) {
         const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
         if (nchunk > 0) {
 #pragma unroll 1
@@ -1009,7 +1087,8 @@ template <int K>
 cudaError_t prepare_mixed_t()
 {
     cudaError_t e = cudaFuncSetAttribute(k_sweep_q_mixed<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MQ<K>::SMEM);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_sweep_p_mixed<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MP<K>::SMEM);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_sweep_p_mixed<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MP<K>::SMEM);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_sweep_p_mixed<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MP<K>::SMEM);
     return e;
 }
 
@@ -1033,7 +1112,7 @@ size_t q_pkg_bytes_t(int64_t J)
 }
 
 template <int K>
-cudaError_t launch_p_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
+cudaError_t launch_p_mixed_t(int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                              const double *p, const SweepPlan &pl, double *out, int *err, uint8_t *pkg,
                              cudaStream_t st)
 {
@@ -1041,7 +1120,10 @@ cudaError_t launch_p_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t p
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_p_mixed<K><<<grid, MP_CTA, MP<K>::SMEM, st>>>(bed, I, J, pitch, pkg, p, pl.slice, out, err);
+    if (mode == 1)
+        k_sweep_p_mixed<K, true><<<grid, MP_CTA, MP<K>::SMEM, st>>>(bed, I, J, pitch, pkg, p, pl.slice, out, err);
+    else
+        k_sweep_p_mixed<K, false><<<grid, MP_CTA, MP<K>::SMEM, st>>>(bed, I, J, pitch, pkg, p, pl.slice, out, err);
     return cudaGetLastError();
 }
 
@@ -1123,12 +1205,13 @@ size_t sweep_q_mixed_pkg_bytes(int K, int64_t J)
     return b;
 }
 
-cudaError_t launch_sweep_p_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                                 const double *p, const SweepPlan &pl, double *out, int *err, uint8_t *pkg,
-                                 cudaStream_t st)
+cudaError_t launch_sweep_p_mixed(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
+                                 const double *q, const double *p, const SweepPlan &pl, double *out, int *err,
+                                 uint8_t *pkg, cudaStream_t st)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_p_mixed_t<KK>(bed, I, J, pitch, q, p, pl, out, err, pkg, st));
+    if (mode != 0 && mode != 1) return e;
+    ADMIX_DISPATCH_K(K, e = launch_p_mixed_t<KK>(mode, bed, I, J, pitch, q, p, pl, out, err, pkg, st));
     return e;
 }
 

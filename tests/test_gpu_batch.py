@@ -1,7 +1,8 @@
 """GPU tests of batches (restarts and K sweeps over one cohort): with the single-problem work
 split a batch reproduces each member's solo run bit for bit (same kernels, same plans, only
-run concurrently); after the autotuner picks another split the members reach the same optima;
-converged members leave the batch while the others continue."""
+run concurrently); after the autotuner picks another split the EM iterates agree with the solo
+runs' and the members at the cohort's own K reach the same optima; converged members leave the
+batch while the others continue."""
 import ctypes as C
 
 import numpy as np
@@ -53,19 +54,40 @@ def test_batch_matches_solo_runs_bit_for_bit(oa, cohort, flags):
     assert rec["ms_device"] > 0
 
 
+def _solo_em(oa, g, K, seed, flags, em):
+    from openadmixture_b200 import _native as N
+    d = oa.AdmixData(g.I, g.J, K, 3)
+    d.x[:] = oa.init_x(g.I, g.J, K, seed)
+    with oa.CuAdmixData(d, g, flags=flags) as h:
+        h.upload(oa.X, d.x)
+        hist = np.zeros(max(em, 1))
+        h._chk(N.admix_lib().admix_init_em(h.handle, em, N.dptr(hist)))
+        return h.download(oa.X)
+
+
 def test_autotuned_batch_reaches_the_same_optima(oa, cohort):
+    """Another work split regroups the FP64 sums across chunks (EM iterates agree with the solo
+    run's to 1e-10) and the mixed form's FP32 Hessian blocks (a ~1e-7 perturbation).  At the
+    cohort's own K = 6 every member reaches the solo run's optimum; below it, several merges of
+    the 6 populations are local optima and such a perturbation may settle a run in another, so
+    those members are held to convergence only."""
     g = cohort
-    Ks = [2, 3, 4, 5, 3, 3]
-    seeds = [0, 0, 0, 0, 1, 2]
+    Ks = [6, 6, 6, 2, 3, 4]
+    seeds = [0, 1, 2, 0, 0, 0]
     with oa.AdmixBatch(g, Ks, flags=2, seeds=seeds) as b:
         d, ms = b.autotune()
         assert d >= 1 and (d & (d - 1)) == 0 and ms > 0
         b.init_em(5)
+        x_em = [b.x(m) for m in range(len(Ks))]
         rec = b.run_qn(500, 1e-7)
         ll = [b.members[m].loglik(oa.X) for m in range(len(Ks))]
     assert rec["converged"].all()
     for m, (K, s) in enumerate(zip(Ks, seeds)):
+        assert np.abs(x_em[m] - _solo_em(oa, g, K, s, 2, 5)).max() < 1e-10, m
+        if K != 6:
+            continue
         x, nd, cv, _, _ = _solo(oa, g, K, s, 2, 5, 500, 1e-7)
+        assert cv, m
         d_ = oa.AdmixData(g.I, g.J, K, 3)
         with oa.CuAdmixData(d_, g) as h:
             h.upload(oa.X, x)

@@ -123,3 +123,25 @@ def test_mixed_sweeps_match_fp64_after_em_priming(oa, K):
         assert _row_rel(z1, z0) < (GRAD_TOL if side == "q" else 1e-4), side
         assert _row_rel(H1, H0) < HESS_TOL, side
     h64.close(); hmx.close()
+
+
+@pytest.mark.parametrize("K,I,J,miss", [(3, 777, 2001, 0.0), (8, 1000, 3000, 0.05), (12, 333, 1500, 0.02)])
+def test_mixed_em_matches_fp64(oa, K, I, J, miss):
+    """init_em! in the mixed form takes both EM half-steps' sums from FP32 cells added in FP64
+    across chunks (the Q half from the tensor-core gradient sweep, the P half from the EM mode
+    of the mixed P sweep); after 5 steps its iterates are within 1e-5 of the FP64 EM's and
+    the FP64 log-likelihood of the result within 1e-6 relative."""
+    spec = oa.COHORTS["c1"].scaled(I=I, J=J, K=K, seed=110 + K, miss=miss)
+    g, _, _ = oa.make_cohort(spec)
+    runs = []
+    for flags in (0, oa.ADMIX_FLAG_MIXED):
+        d = oa.AdmixData(I, J, K, 3, rng=7)
+        with oa.CuAdmixData(d, g, flags=flags) as h:
+            hist = oa.init_em(d, g, 5, d_cu=h, quiet=True)
+        runs.append((d.x.copy(), d.ll_new, hist))
+    (x0, ll0, h0), (x1, ll1, h1) = runs
+    assert np.all(np.isfinite(x1))
+    dx = float(np.abs(x1 - x0).max())
+    assert dx < 1e-5, dx
+    assert rel_err(ll1, ll0) < 1e-6, (ll1, ll0)
+    assert rel_err(h1[-1], h0[-1]) < 1e-6, (h1[-1], h0[-1])
