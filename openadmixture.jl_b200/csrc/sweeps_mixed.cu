@@ -390,15 +390,14 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
             const float *Pf = (const float *)(pk + C::PK_PF);
             const uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF;
-            uint32_t rq[32], ro[32];
+            /* qp / om of the chunk's 32 SNPs, read in two halves of 16 columns (SNPs 0-15, then
+             * 16-31) to keep the producer within its registers */
+            uint32_t rq[16], ro[16];
             if (!wait(bar_qp, (uint32_t)(c & 1))) break;
             tc_fence_after_sync();
-            tmem_ld32_nowait(tmem + lane_base, rq);
-            tmem_ld32_nowait(tmem + lane_base + 32u, ro);
+            tmem_ld16_raw(tmem + lane_base, rq);
+            tmem_ld16_raw(tmem + lane_base + 32u, ro);
             tmem_wait_ld();
-            tc_fence_before_sync();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(bar_qfree);
             if (!wait(&bar_p[c % MQ_NPKG], (uint32_t)((c / MQ_NPKG) & 1))) break;
             if (!wait(&bar_g[c & 1], (uint32_t)((c >> 1) & 1))) break;
             if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the weight tile is free */
@@ -414,16 +413,26 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
 #pragma unroll
             for (int kc = 0; kc < 4; ++kc) {
+                if (kc == 2) {   /* the second half of the columns; then the qp columns are free */
+                    tc_fence_after_sync();
+                    tmem_ld16_raw(tmem + lane_base + 16u, rq);
+                    tmem_ld16_raw(tmem + lane_base + 48u, ro);
+                    tmem_wait_ld();
+                    tc_fence_before_sync();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(bar_qfree);
+                }
                 uint32_t w1p[4], w2p[4];
                 float2 dz[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int m = kc * 4 + e;
+                    const int r = 2 * (m & 7);   /* this pair's column in rq / ro */
                     const uint32_t gw = ((uint32_t)G2[m * 32] & gmask) | (~gmask & 0x5555u);
                     const uint32_t tb = gw >> sh;
                     const float4 a = tab[8 * ((tb & 3u) | ((tb >> 6) & 12u))];
-                    const float2 qp = make_float2(__uint_as_float(rq[2 * m]), __uint_as_float(rq[2 * m + 1]));
-                    const float2 om = __fadd2_rn(make_float2(__uint_as_float(ro[2 * m]), __uint_as_float(ro[2 * m + 1])), sres2);
+                    const float2 qp = make_float2(__uint_as_float(rq[r]), __uint_as_float(rq[r + 1]));
+                    const float2 om = __fadd2_rn(make_float2(__uint_as_float(ro[r]), __uint_as_float(ro[r + 1])), sres2);
                     const float2 pr = __fmul2_rn(qp, om);
                     const float2 rr = make_float2(rcp_approx(pr.x), rcp_approx(pr.y));
                     const float2 r1 = __fmul2_rn(om, rr), r2 = __fmul2_rn(qp, rr);
@@ -785,27 +794,14 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
             const float *Qf = (const float *)(pk + C::PK_QF);
             const float2 *Sres = (const float2 *)(pk + C::PK_S);
-            /* qp / om of the chunk's 32 individuals; the EM sums hold twice the accumulators, so
-             * they read the columns in two halves of 16 (individuals 0-15, then 16-31) */
-            constexpr int RC = EMS ? 16 : 32;
-            uint32_t rq[RC], ro[RC];
-            auto release_qp = [&]() {
-                tc_fence_before_sync();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(bar_qfree);
-            };
+            /* qp / om of the chunk's 32 individuals, read in two halves of 16 columns
+             * (individuals 0-15, then 16-31) to keep the producer within its registers */
+            uint32_t rq[16], ro[16];
             if (!wait(bar_qp, (uint32_t)(c & 1))) break;
             tc_fence_after_sync();
-            if constexpr (EMS) {
-                tmem_ld16_raw(tmem + lane_base, rq);
-                tmem_ld16_raw(tmem + lane_base + C::COL_OM, ro);
-                tmem_wait_ld();
-            } else {
-                tmem_ld32_nowait(tmem + lane_base, rq);
-                tmem_ld32_nowait(tmem + lane_base + C::COL_OM, ro);
-                tmem_wait_ld();
-                release_qp();
-            }
+            tmem_ld16_raw(tmem + lane_base, rq);
+            tmem_ld16_raw(tmem + lane_base + C::COL_OM, ro);
+            tmem_wait_ld();
             if (!wait(&bar_p[c % MP_NPKG], (uint32_t)((c / MP_NPKG) & 1))) break;
             if constexpr (!EMS) {
                 if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the C tile is free */
@@ -823,21 +819,21 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             for (int k = 0; k < (EMS ? K : 1); ++k) hk[k] = make_float2(0.f, 0.f);
 #pragma unroll
             for (int kc = 0; kc < 4; ++kc) {
-                if constexpr (EMS) {
-                    if (kc == 2) {   /* the second half of the columns; then the qp columns are free */
-                        tc_fence_after_sync();
-                        tmem_ld16_raw(tmem + lane_base + 16u, rq);
-                        tmem_ld16_raw(tmem + lane_base + C::COL_OM + 16u, ro);
-                        tmem_wait_ld();
-                        release_qp();
-                    }
+                if (kc == 2) {   /* the second half of the columns; then the qp columns are free */
+                    tc_fence_after_sync();
+                    tmem_ld16_raw(tmem + lane_base + 16u, rq);
+                    tmem_ld16_raw(tmem + lane_base + C::COL_OM + 16u, ro);
+                    tmem_wait_ld();
+                    tc_fence_before_sync();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(bar_qfree);
                 }
                 uint32_t cp[4];
                 float2 zz[4], z2s[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int m = kc * 4 + e;
-                    const int r = 2 * (EMS ? (m & 7) : m);   /* this pair's column in rq / ro */
+                    const int r = 2 * (m & 7);   /* this pair's column in rq / ro */
                     const uint32_t w = (m < 8) ? gcur.x : gcur.y;
                     const float4 a = tab[8 * ((w >> (4 * (m & 7))) & 15u)];
                     const float2 qp = make_float2(__uint_as_float(rq[r]), __uint_as_float(rq[r + 1]));
