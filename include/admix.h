@@ -42,7 +42,12 @@ extern "C" {
 /* admix_create flags */
 #define ADMIX_FLAG_MU_GERSHGORIN  1u  /* simplex tableau adds the Gerschgorin mu of qp.jl:54-58
                                           (default: mu = 0, what the aliased mul! yields) */
-#define ADMIX_FLAG_MIXED          2u  /* mixed-precision form of the Q/P sweeps */
+#define ADMIX_FLAG_MIXED          2u  /* mixed-precision form: the iteration's Q/P gradient / Hessian
+                                          sweeps (tcgen05 BF16 Hessians, FP32 gradient cells, FP64
+                                          sums), its log-likelihoods (FP32 cells, FP64 reduction) and
+                                          admix_init_em's EM sums; admix_loglik, admix_em_q/_p, the
+                                          QPs and the QN step stay FP64.  A mixed call whose
+                                          tensor-core pipeline wait runs out returns ADMIX_ERR_CUDA. */
 
 #define ADMIX_MAX_K 16
 #define ADMIX_MAX_Q 8
