@@ -125,7 +125,8 @@ def test_mixed_sweeps_match_fp64_after_em_priming(oa, K):
     h64.close(); hmx.close()
 
 
-@pytest.mark.parametrize("K,I,J,miss", [(3, 777, 2001, 0.0), (8, 1000, 3000, 0.05), (12, 333, 1500, 0.02)])
+@pytest.mark.parametrize("K,I,J,miss", [(1, 100, 700, 0.0), (3, 777, 2001, 0.0), (8, 1000, 3000, 0.05),
+                                        (12, 333, 1500, 0.02), (16, 515, 900, 0.01)])
 def test_mixed_em_matches_fp64(oa, K, I, J, miss):
     """init_em! in the mixed form takes both EM half-steps' sums from FP32 cells added in FP64
     across chunks (the Q half from the tensor-core gradient sweep, the P half from the EM mode
