@@ -357,11 +357,19 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
     of the random start, with no EM; where no model applies it falls back to the random start +
     EM.  Explicit init_q / init_p take precedence over the warm start.  stream_block keeps the
     genotypes in host memory and streams them in blocks of that many SNPs (cohorts larger than
-    device memory)."""
+    device memory).
+
+    T = Float32 (np.float32 or "Float32"): the reference then holds and computes every array in
+    Float32 (AdmixData{T}, structs.jl:9-91) for speed.  Here it selects the mixed form
+    (ADMIX_FLAG_MIXED: FP32 cells and tensor-core Hessians with FP64 sums, QPs and state), which
+    is faster than the FP64 form and more accurate than an all-Float32 run; the returned
+    AdmixData holds Float32 arrays."""
     if sparsity is not None:
         raise NotImplementedError("sparsity (SKFR AIM pre-selection) is outside the likelihood engine")
-    if T not in (np.float64, float, "Float64"):
-        raise NotImplementedError("only T = Float64 is on the device path")
+    if T in (np.float32, "Float32"):
+        flags |= N.ADMIX_FLAG_MIXED
+    elif T not in (np.float64, float, "Float64"):
+        raise NotImplementedError(f"T = {T!r}: Float64 and Float32 are supported")
     if not use_gpu:
         raise NotImplementedError("use_gpu=False is the reference's CPU path; this engine runs on the GPU")
     g = filename if isinstance(filename, (Genotypes, DeviceGenotypes)) else read_bed(filename)
@@ -390,4 +398,7 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
                      verbose=verbose, progress_bar=progress_bar, quiet=quiet)
     finally:
         d_cu.close()
+    if T in (np.float32, "Float32"):
+        for name in ("x", "x_next", "x_next2", "x_tmp"):
+            setattr(d, name, getattr(d, name).astype(np.float32))
     return d, None, None

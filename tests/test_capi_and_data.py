@@ -57,6 +57,8 @@ def test_engine_requires_gpu_path(oa):
         oa.run_admixture(oa.Genotypes(np.zeros((8, 2), np.uint8), 8, 8), 2, use_gpu=False)
     with pytest.raises(NotImplementedError):
         oa.run_admixture(oa.Genotypes(np.zeros((8, 2), np.uint8), 8, 8), 2, sparsity=100)
+    with pytest.raises(NotImplementedError, match="Float64 and Float32"):
+        oa.run_admixture(oa.Genotypes(np.zeros((8, 2), np.uint8), 8, 8), 2, T=np.float16)
 
 
 def test_admixdata_init_matches_reference_contract(oa):
