@@ -955,13 +955,6 @@ __device__ __forceinline__ uint4 col_load64(const uint8_t *__restrict__ bed, int
                  : make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
 }
 
-/* 4-bit code pair of individuals 2m, 2m+1 in a 64-individual word */
-__device__ __forceinline__ uint32_t pair_code(const uint4 &g, int m)
-{
-    const uint32_t w = (m < 8) ? g.x : ((m < 16) ? g.y : ((m < 24) ? g.z : g.w));
-    return (w >> (4 * (m & 7))) & 15u;
-}
-
 /* ===================================================================== loglik
  * loglikelihood_loop_skipmissing (loops.jl:517-539) with FP32 cells: thread = SNP, individuals
  * in pairs; qp is an FP32 FMA chain and 1 - qp is formed from it by one subtraction (exact for
@@ -1034,16 +1027,19 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
 #pragma unroll
             for (int hm = 0; hm < 2; ++hm) {
             const int m = 2 * m2 + hm;
-            const uint32_t code4 = pair_code(g, m);
+            /* the pair's 4 code bits, tested in place in their 32-bit word */
+            const uint32_t w = (m < 8) ? g.x : ((m < 16) ? g.y : ((m < 24) ? g.z : g.w));
+            const int b = 4 * (m & 7);
             const float2 qp = hm ? qpb : qpa;
             /* 1 - qp as the reference forms it, from the (unbiased) FP32 qp */
             const float2 om = make_float2(1.f - qp.x, 1.f - qp.y);
-            /* factor per code: 00 -> om^2, 01 -> 1, 10 -> qp om, 11 -> qp^2 */
-            const uint32_t c0 = code4 & 3u, c1 = code4 >> 2;
-            const float u0 = (c0 & 2u) ? qp.x : om.x, v0 = (c0 == 3u) ? qp.x : om.x;
-            const float u1 = (c1 & 2u) ? qp.y : om.y, v1 = (c1 == 3u) ? qp.y : om.y;
-            const float f0 = (c0 == 1u) ? 1.f : u0 * v0;
-            const float f1 = (c1 == 1u) ? 1.f : u1 * v1;
+            /* factor per code: 00 -> om^2, 01 -> 1 (missing), 10 -> qp om, 11 -> qp^2; the three
+             * products are formed for both cells and one is selected */
+            const float2 oo = __fmul2_rn(om, om), qo = __fmul2_rn(qp, om), qq = __fmul2_rn(qp, qp);
+            const bool lo0 = (w >> b) & 1u, hi0 = (w >> (b + 1)) & 1u;
+            const bool lo1 = (w >> (b + 2)) & 1u, hi1 = (w >> (b + 3)) & 1u;
+            const float f0 = hi0 ? (lo0 ? qq.x : qo.x) : (lo0 ? 1.f : oo.x);
+            const float f1 = hi1 ? (lo1 ? qq.y : qo.y) : (lo1 ? 1.f : oo.y);
             prod *= (double)(f0 * f1);
             if ((m % 12) == 11) {
                 const int64_t bits = __double_as_longlong(prod);
