@@ -965,6 +965,8 @@ __device__ __forceinline__ uint4 col_load64(const uint8_t *__restrict__ bed, int
  * nearest, so the rounding error is a random walk far below the convergence test's resolution. */
 constexpr int ML_IC = 64;
 
+constexpr int ML_JT = 2;   /* SNPs per thread (j and j + 128): each broadcast load of q serves both */
+
 template <int K>
 __global__ void __launch_bounds__(128)
 k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
@@ -975,19 +977,27 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
     __shared__ float4 Qs[2][K][ML_IC / 4];              /* q of individuals 4m .. 4m+3 */
     __shared__ double red[4];
     const int tid = threadIdx.x;
-    const int64_t j = (int64_t)blockIdx.x * 128 + tid;
-    const bool valid = j < J;
+    const int64_t j0 = (int64_t)blockIdx.x * (128 * ML_JT) + tid;
     const int64_t ia = (int64_t)blockIdx.y * islice;
     const int64_t ib = min(I, ia + islice);
     const int nchunk = (int)((ib - ia + ML_IC - 1) / ML_IC);
-    float2 pd[K];
+    bool valid[ML_JT];
+    float2 pd[ML_JT][K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const double pv = valid ? p[(size_t)K * j + k] : 0.5;
-        pd[k] = make_float2((float)pv, (float)pv);
+    for (int t = 0; t < ML_JT; ++t) {
+        const int64_t j = j0 + 128 * t;
+        valid[t] = j < J;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double pv = valid[t] ? p[(size_t)K * j + k] : 0.5;
+            pd[t][k] = make_float2((float)pv, (float)pv);
+        }
     }
     float qr[PREF];
-    uint4 gnext = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), g = gnext;
+    const uint4 none = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
+    uint4 g[ML_JT], gnext[ML_JT];
+#pragma unroll
+    for (int t = 0; t < ML_JT; ++t) g[t] = gnext[t] = none;
     auto load = [&](int64_t ic) {
 #pragma unroll
         for (int u = 0; u < PREF; ++u) {
@@ -995,7 +1005,8 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
             const int k = t / ML_IC, ii = t - k * ML_IC;
             qr[u] = (t < K * ML_IC && ic + ii < ib) ? (float)q[(size_t)K * (ic + ii) + k] : 1.0f / K;
         }
-        gnext = col_load64(bed, pitch, j, valid, ic);
+#pragma unroll
+        for (int t = 0; t < ML_JT; ++t) gnext[t] = col_load64(bed, pitch, j0 + 128 * t, valid[t], ic);
     };
     auto store = [&](int s) {
 #pragma unroll
@@ -1007,58 +1018,86 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
             }
         }
     };
-    if (nchunk > 0) { load(ia); store(0); g = gnext; }
-    if (nchunk > 1) load(ia + ML_IC);
-    __syncthreads();
-    double prod = 1.0;
-    int64_t ex = 0;
-    for (int c = 0; c < nchunk; ++c) {
-        const int s = c & 1;
-#pragma unroll
-        for (int m2 = 0; m2 < ML_IC / 4; ++m2) {
-            /* qp of two individual pairs (one 16-byte broadcast load of q per k) */
-            float2 qpa = make_float2(0.f, 0.f), qpb = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const float4 qv = Qs[s][k][m2];
-                qpa = __ffma2_rn(make_float2(qv.x, qv.y), pd[k], qpa);
-                qpb = __ffma2_rn(make_float2(qv.z, qv.w), pd[k], qpb);
-            }
-#pragma unroll
-            for (int hm = 0; hm < 2; ++hm) {
-            const int m = 2 * m2 + hm;
-            /* the pair's 4 code bits, tested in place in their 32-bit word */
-            const uint32_t w = (m < 8) ? g.x : ((m < 16) ? g.y : ((m < 24) ? g.z : g.w));
-            const int b = 4 * (m & 7);
-            const float2 qp = hm ? qpb : qpa;
-            /* 1 - qp as the reference forms it, from the (unbiased) FP32 qp */
-            const float2 om = make_float2(1.f - qp.x, 1.f - qp.y);
-            /* factor per code: 00 -> om^2, 01 -> 1 (missing), 10 -> qp om, 11 -> qp^2; the three
-             * products are formed for both cells and one is selected */
-            const float2 oo = __fmul2_rn(om, om), qo = __fmul2_rn(qp, om), qq = __fmul2_rn(qp, qp);
-            const bool lo0 = (w >> b) & 1u, hi0 = (w >> (b + 1)) & 1u;
-            const bool lo1 = (w >> (b + 2)) & 1u, hi1 = (w >> (b + 3)) & 1u;
-            const float f0 = hi0 ? (lo0 ? qq.x : qo.x) : (lo0 ? 1.f : oo.x);
-            const float f1 = hi1 ? (lo1 ? qq.y : qo.y) : (lo1 ? 1.f : oo.y);
-            prod *= (double)(f0 * f1);
-            if ((m % 12) == 11) {
-                const int64_t bits = __double_as_longlong(prod);
-                ex += ((bits >> 52) & 0x7FF) - 1023;
-                prod = __longlong_as_double((bits & ~(0x7FFLL << 52)) | (1023LL << 52));
-            }
-            }
-        }
+    auto fold = [&](double &prod, int64_t &ex) {   /* move the exponent into the integer */
         const int64_t bits = __double_as_longlong(prod);
         ex += ((bits >> 52) & 0x7FF) - 1023;
         prod = __longlong_as_double((bits & ~(0x7FFLL << 52)) | (1023LL << 52));
+    };
+    if (nchunk > 0) {
+        load(ia);
+        store(0);
+#pragma unroll
+        for (int t = 0; t < ML_JT; ++t) g[t] = gnext[t];
+    }
+    if (nchunk > 1) load(ia + ML_IC);
+    __syncthreads();
+    double prod[ML_JT];
+    int64_t ex[ML_JT];
+#pragma unroll
+    for (int t = 0; t < ML_JT; ++t) { prod[t] = 1.0; ex[t] = 0; }
+    for (int c = 0; c < nchunk; ++c) {
+        const int s = c & 1;
+        uint4 gw[ML_JT];   /* the chunk's 4 code words per SNP, consumed from .x and shifted down */
+#pragma unroll
+        for (int t = 0; t < ML_JT; ++t) gw[t] = g[t];
+#pragma unroll 1
+        for (int wd = 0; wd < 4; ++wd) {   /* 16 individuals per 32-bit code word */
+#pragma unroll
+            for (int m2l = 0; m2l < 4; ++m2l) {
+                const int m2 = 4 * wd + m2l;
+                /* qp of two individual pairs for both SNPs (one 16-byte broadcast load of q per k) */
+                float2 qpa[ML_JT], qpb[ML_JT];
+#pragma unroll
+                for (int t = 0; t < ML_JT; ++t) qpa[t] = qpb[t] = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const float4 qv = Qs[s][k][m2];
+#pragma unroll
+                    for (int t = 0; t < ML_JT; ++t) {
+                        qpa[t] = __ffma2_rn(make_float2(qv.x, qv.y), pd[t][k], qpa[t]);
+                        qpb[t] = __ffma2_rn(make_float2(qv.z, qv.w), pd[t][k], qpb[t]);
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < ML_JT; ++t) {
+#pragma unroll
+                    for (int hm = 0; hm < 2; ++hm) {
+                        /* the pair's 4 code bits, tested in place in their 32-bit word */
+                        const uint32_t w = gw[t].x;
+                        const int b = 4 * (2 * m2l + hm);
+                        const float2 qp = hm ? qpb[t] : qpa[t];
+                        /* 1 - qp as the reference forms it, from the (unbiased) FP32 qp */
+                        const float2 om = make_float2(1.f - qp.x, 1.f - qp.y);
+                        /* factor per code: 00 -> om^2, 01 -> 1 (missing), 10 -> qp om, 11 -> qp^2;
+                         * the three products are formed for both cells and one is selected */
+                        const float2 oo = __fmul2_rn(om, om), qo = __fmul2_rn(qp, om), qq = __fmul2_rn(qp, qp);
+                        const bool lo0 = (w >> b) & 1u, hi0 = (w >> (b + 1)) & 1u;
+                        const bool lo1 = (w >> (b + 2)) & 1u, hi1 = (w >> (b + 3)) & 1u;
+                        const float f0 = hi0 ? (lo0 ? qq.x : qo.x) : (lo0 ? 1.f : oo.x);
+                        const float f1 = hi1 ? (lo1 ? qq.y : qo.y) : (lo1 ? 1.f : oo.y);
+                        prod[t] *= (double)(f0 * f1);
+                    }
+                }
+            }
+            /* 8 pairs per word: each pair's factor is >= 1e-20, so the product stays normal */
+#pragma unroll
+            for (int t = 0; t < ML_JT; ++t) {
+                fold(prod[t], ex[t]);
+                gw[t] = make_uint4(gw[t].y, gw[t].z, gw[t].w, 0u);
+            }
+        }
         if (c + 1 < nchunk) {
             store(s ^ 1);
-            g = gnext;
+#pragma unroll
+            for (int t = 0; t < ML_JT; ++t) g[t] = gnext[t];
             if (c + 2 < nchunk) load(ia + (int64_t)(c + 2) * ML_IC);
         }
         __syncthreads();
     }
-    double ll = valid ? (log(prod) + (double)ex * 0.69314718055994530942) : 0.0;
+    double ll = 0.0;
+#pragma unroll
+    for (int t = 0; t < ML_JT; ++t)
+        if (valid[t]) ll += log(prod[t]) + (double)ex[t] * 0.69314718055994530942;
     for (int o = 16; o > 0; o >>= 1) ll += __shfl_down_sync(0xffffffffu, ll, o);
     if ((tid & 31) == 0) red[tid >> 5] = ll;
     __syncthreads();
@@ -1178,7 +1217,8 @@ SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms)
 
 SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms)
 {
-    return plan_rows(J, I, sms, 8, ML_IC);
+    /* CTAs of 128 threads x ML_JT SNPs; 6 CTAs per SM fit at K <= 12 (80-96 registers) */
+    return plan_rows((J + ML_JT - 1) / ML_JT, I, sms, 6, ML_IC);
 }
 
 cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
