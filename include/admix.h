@@ -141,6 +141,12 @@ int admix_update_p(admix_ctx *h, int32_t update2, int32_t *qp_status);
  * driver.jl:169-197): later iterations (admix_qn_iteration, admix_run_qn, batches) copy the fixed
  * block (q_next .= q, q_next2 .= q, likewise p) instead of updating it.  Default: neither. */
 int admix_set_fixed(admix_ctx *h, int32_t fix_q, int32_t fix_p);
+/* (No counterpart in the reference.)  Self-test of the mixed form's failure reporting: runs a
+ * kernel whose bounded mbarrier wait nothing completes, so it gives up after 1024 polls and sets
+ * the error flag exactly as a tensor-core sweep's pipeline wait would; returns ADMIX_ERR_CUDA
+ * with the same message, and the flag is cleared, so the handle stays usable.  Mixed-form
+ * handles only (ADMIX_ERR_STATE otherwise). */
+int admix_selftest_wait_timeout(admix_ctx *h);
 int admix_qn_iteration(admix_ctx *h, int32_t iter, admix_iterinfo *out);
 /* Iterations iter_offset+1 .. n_iter until reldiff < rtol.  hist (n_iter entries, may be
  * NULL) receives one record per iteration run. */

@@ -536,7 +536,7 @@ static int tc_err_check(admix_ctx *h)
     h->sc_host->tc_err = 0;
     CK(h, cudaMemsetAsync(&h->sc->tc_err, 0, sizeof(int32_t), h->st));
     CK(h, cudaStreamSynchronize(h->st));
-    return fail(h, ADMIX_ERR_CUDA, "a tensor-core sweep gave up waiting on its pipeline; this call's results are invalid");
+    return fail(h, ADMIX_ERR_CUDA, "a tensor-core pipeline wait gave up (bounded wait ran out); this call's results are invalid");
 }
 
 /* drain the stream and check the flag (mixed handles only: the FP64 kernels never wait) */
@@ -653,6 +653,14 @@ int admix_grad_hess_q(admix_ctx *h, int32_t which_q, int32_t which_p, double *Xt
 int admix_grad_hess_p(admix_ctx *h, int32_t which_q, int32_t which_p, double *XtX, double *Xtz)
 {
     return grad_hess_common(h, false, which_q, which_p, XtX, Xtz);
+}
+
+int admix_selftest_wait_timeout(admix_ctx *h)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (!(h->flags & ADMIX_FLAG_MIXED)) return fail(h, ADMIX_ERR_STATE, "the self-test needs a mixed-form handle");
+    CK(h, launch_wait_probe(&h->sc->tc_err, 1024u, h->st));
+    return tc_err_sync(h);
 }
 
 int admix_update_q(admix_ctx *h, int32_t update2, int32_t *qp_status)

@@ -1104,6 +1104,18 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
     if (tid == 0) partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = red[0] + red[1] + red[2] + red[3];
 }
 
+/* A bounded mbarrier wait that nothing completes: it gives up after `polls` polls and raises the
+ * error flag as the sweeps' pipeline waits do (the failure-reporting self-test). */
+__global__ void k_wait_probe(int *__restrict__ err, uint32_t polls)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+        if (!mbar_wait_bounded(&bar, 0u, polls)) atomicOr(err, 1);
+    }
+}
+
 __global__ void __launch_bounds__(1024)
 k_sum_partials_mixed(const double *__restrict__ partial, int64_t n, double *__restrict__ out)
 {
@@ -1245,6 +1257,12 @@ cudaError_t launch_sweep_p_mixed(int K, int mode, const uint8_t *bed, int64_t I,
     if (mode != 0 && mode != 1) return e;
     ADMIX_DISPATCH_K(K, e = launch_p_mixed_t<KK>(mode, bed, I, J, pitch, q, p, pl, out, err, pkg, st));
     return e;
+}
+
+cudaError_t launch_wait_probe(int *err, uint32_t polls, cudaStream_t st)
+{
+    k_wait_probe<<<1, 32, 0, st>>>(err, polls);
+    return cudaGetLastError();
 }
 
 size_t sweep_p_mixed_pkg_bytes(int K, int64_t I)

@@ -161,3 +161,26 @@ def test_run_admixture_float32_runs_the_mixed_form(oa):
     assert d32.q.shape == d64.q.shape and d32.p.shape == d64.p.shape
     assert rel_err(d32.ll_new, d64.ll_new) < 1e-6
     assert np.abs(d32.q - d64.q).max() < 1e-2
+
+
+def test_timed_out_pipeline_wait_is_reported_and_the_handle_recovers(oa):
+    """A bounded pipeline wait that runs out (admix_selftest_wait_timeout: an mbarrier that
+    nothing completes, 1024 polls) fails the call with ADMIX_ERR_CUDA and clears the flag: the
+    same handle's next EM and QN iterations succeed and equal a fresh handle's bit for bit."""
+    from openadmixture_b200 import _native as N
+    lib = N.admix_lib()
+    spec = oa.COHORTS["c1"].scaled(I=300, J=1200, K=3, seed=5)
+    g, _, _ = oa.make_cohort(spec)
+    with oa.CuAdmixData(oa.AdmixData(g.I, g.J, 3, 3, rng=3), g) as h64:
+        assert lib.admix_selftest_wait_timeout(h64.handle) == N.ADMIX_ERR_STATE
+    lls = []
+    for probe in (True, False):
+        d = oa.AdmixData(g.I, g.J, 3, 3, rng=3)
+        with oa.CuAdmixData(d, g, flags=oa.ADMIX_FLAG_MIXED) as h:
+            if probe:
+                assert lib.admix_selftest_wait_timeout(h.handle) == N.ADMIX_ERR_CUDA
+                assert b"gave up" in lib.admix_last_error(h.handle)
+            oa.init_em(d, g, 2, d_cu=h, quiet=True)
+            recs = oa.admixture_qn(d, g, 3, 0.0, d_cu=h, quiet=True)
+            lls.append(recs[-1]["ll_new"])
+    assert lls[0] == lls[1]
