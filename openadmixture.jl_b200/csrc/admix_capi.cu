@@ -239,7 +239,17 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     if (flags & ADMIX_FLAG_MIXED)
         TRY(dalloc(h, &h->pkg, std::max(sweep_q_mixed_pkg_bytes(K, J), sweep_p_mixed_pkg_bytes(K, I))));
     TRY(dalloc(h, &h->status_p, (size_t)J));
-    TRY(dalloc(h, &h->ll_partial, std::max((size_t)h->llp.gx * h->llp.gy, (size_t)h->llm.gx * h->llm.S)));
+    /* per-CTA log-likelihood partials: the resident plans, and for a streamed handle the plans of
+     * a full block and of the last block (the mixed plan's count can grow as its SNP range shrinks) */
+    auto ll_parts = [&](int64_t nj) {
+        const LoglikPlan a = plan_loglik(I, nj, h->sms);
+        const SweepPlan b = plan_loglik_mixed(I, nj, h->sms);
+        return std::max((size_t)a.gx * a.gy, (size_t)b.gx * b.S);
+    };
+    size_t n_ll = std::max((size_t)h->llp.gx * h->llp.gy, (size_t)h->llm.gx * h->llm.S);
+    if (h->streamed)
+        n_ll = std::max(n_ll, std::max(ll_parts(std::min<int64_t>(h->blk, J)), ll_parts(J - (int64_t)(h->nblk - 1) * h->blk)));
+    TRY(dalloc(h, &h->ll_partial, n_ll));
     TRY(dalloc(h, &h->qn_partial, (size_t)h->qnp.blocks * (Q * Q + Q)));
     TRY(dalloc(h, &h->sc, 1));
     TRY(dalloc(h, &h->counts, (size_t)(I + J)));
