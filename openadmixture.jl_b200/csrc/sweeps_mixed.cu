@@ -968,7 +968,7 @@ constexpr int ML_IC = 64;
 constexpr int ML_JT = 2;   /* SNPs per thread (j and j + 128): each broadcast load of q serves both */
 
 template <int K>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, (K <= 10 ? 6 : 4))
 k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                const double *__restrict__ q, const double *__restrict__ p, int64_t islice,
                double *__restrict__ partial)
@@ -1060,14 +1060,15 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
                 }
 #pragma unroll
                 for (int t = 0; t < ML_JT; ++t) {
+                    float2 fa, fb;   /* (first, second) cell factors of pair a (hm = 0) and pair b */
 #pragma unroll
                     for (int hm = 0; hm < 2; ++hm) {
                         /* the pair's 4 code bits, tested in place in their 32-bit word */
                         const uint32_t w = gw[t].x;
                         const int b = 4 * (2 * m2l + hm);
                         const float2 qp = hm ? qpb[t] : qpa[t];
-                        /* 1 - qp as the reference forms it, from the (unbiased) FP32 qp */
-                        const float2 om = make_float2(1.f - qp.x, 1.f - qp.y);
+                        /* 1 - qp as the reference forms it (one rounding), from the unbiased FP32 qp */
+                        const float2 om = __ffma2_rn(qp, make_float2(-1.f, -1.f), make_float2(1.f, 1.f));
                         /* factor per code: 00 -> om^2, 01 -> 1 (missing), 10 -> qp om, 11 -> qp^2;
                          * the three products are formed for both cells and one is selected */
                         const float2 oo = __fmul2_rn(om, om), qo = __fmul2_rn(qp, om), qq = __fmul2_rn(qp, qp);
@@ -1075,8 +1076,13 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
                         const bool lo1 = (w >> (b + 2)) & 1u, hi1 = (w >> (b + 3)) & 1u;
                         const float f0 = hi0 ? (lo0 ? qq.x : qo.x) : (lo0 ? 1.f : oo.x);
                         const float f1 = hi1 ? (lo1 ? qq.y : qo.y) : (lo1 ? 1.f : oo.y);
-                        prod[t] *= (double)(f0 * f1);
+                        if (hm) fb = make_float2(f0, f1);
+                        else fa = make_float2(f0, f1);
                     }
+                    /* the two pairs' products f0 f1 in one paired multiply, each into the FP64 product */
+                    const float2 ff = __fmul2_rn(make_float2(fa.x, fb.x), make_float2(fa.y, fb.y));
+                    prod[t] *= (double)ff.x;
+                    prod[t] *= (double)ff.y;
                 }
             }
             /* 8 pairs per word: each pair's factor is >= 1e-20, so the product stays normal */
@@ -1229,7 +1235,7 @@ SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms)
 
 SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms)
 {
-    /* CTAs of 128 threads x ML_JT SNPs; 6 CTAs per SM fit at K <= 12 (80-96 registers) */
+    /* CTAs of 128 threads x ML_JT SNPs; 6 CTAs per SM fit at K <= 10 (80 registers) */
     return plan_rows((J + ML_JT - 1) / ML_JT, I, sms, 6, ML_IC);
 }
 
