@@ -53,6 +53,7 @@ struct admix_ctx {
     unsigned long long *counts = nullptr;
     LoglikPlan llp;
     SweepPlan sq, sp, sqm, spm, llm; /* *m: mixed-precision Q sweep, P sweep, loglik */
+    int64_t cap_sqm = 1, cap_spm = 1, cap_llm = 1;   /* slice counts the partial buffers hold */
     QNPlan qnp;
     size_t bytes = 0;
     cudaGraphExec_t iter_graph = nullptr;
@@ -200,8 +201,11 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     h->sp = plan_sweep_p(K, I, J, h->sms);
     h->sqm = plan_sweep_q_mixed(K, I, J, h->sms);
     h->spm = plan_sweep_p_mixed(K, I, J, h->sms);
-    h->llm = plan_loglik_mixed(I, J, h->sms);
+    h->llm = plan_loglik_mixed(K, I, J, h->sms);
     h->qnp = plan_qn(nx, h->sms);
+    h->cap_sqm = h->sqm.S;
+    h->cap_spm = h->spm.S;
+    h->cap_llm = h->llm.S;
 
     if (stream_blk > 0) {
         h->streamed = true;
@@ -243,7 +247,7 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
      * a full block and of the last block (the mixed plan's count can grow as its SNP range shrinks) */
     auto ll_parts = [&](int64_t nj) {
         const LoglikPlan a = plan_loglik(I, nj, h->sms);
-        const SweepPlan b = plan_loglik_mixed(I, nj, h->sms);
+        const SweepPlan b = plan_loglik_mixed(K, I, nj, h->sms);
         return std::max((size_t)a.gx * a.gy, (size_t)b.gx * b.S);
     };
     size_t n_ll = std::max((size_t)h->llp.gx * h->llp.gy, (size_t)h->llm.gx * h->llm.S);
@@ -407,7 +411,7 @@ static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst, bool fast = 
         double *o = h->streamed ? h->ll_blk + b : dst;
         const double *P = Pof(h, which) + (size_t)h->K * j0;
         if (mx) {
-            const SweepPlan pl = h->streamed ? plan_loglik_mixed(h->I, nj, h->sms) : h->llm;
+            const SweepPlan pl = h->streamed ? plan_loglik_mixed(h->K, h->I, nj, h->sms) : h->llm;
             return launch_loglik_mixed(h->K, bed, h->I, nj, h->pitch, Qof(h, which), P, pl, h->ll_partial, o,
                                        &h->sc->tc_err, h->pkg, h->st);
         }
@@ -933,15 +937,16 @@ static void batch_release(admix_batch *b)
 }
 
 /* Plans of one member as if it had sms_eff SMs to itself.  The partial-sum buffers were sized
- * for the full SM count, and every plan's slice count only shrinks with fewer SMs. */
+ * for the full SM count: the FP64 plans' slice counts only shrink with fewer SMs, and the mixed
+ * plans are held to the slice counts of the handle's first plans. */
 static void set_plans(admix_ctx *h, int sms_eff)
 {
     h->llp = plan_loglik(h->I, h->J, sms_eff);
     h->sq = plan_sweep_q(h->K, h->I, h->J, sms_eff);
     h->sp = plan_sweep_p(h->K, h->I, h->J, sms_eff);
-    h->sqm = plan_sweep_q_mixed(h->K, h->I, h->J, sms_eff);
-    h->spm = plan_sweep_p_mixed(h->K, h->I, h->J, sms_eff);
-    h->llm = plan_loglik_mixed(h->I, h->J, sms_eff);
+    h->sqm = plan_sweep_q_mixed(h->K, h->I, h->J, sms_eff, h->cap_sqm);
+    h->spm = plan_sweep_p_mixed(h->K, h->I, h->J, sms_eff, h->cap_spm);
+    h->llm = plan_loglik_mixed(h->K, h->I, h->J, sms_eff, h->cap_llm);
     if (h->iter_graph) { cudaGraphExecDestroy(h->iter_graph); h->iter_graph = nullptr; }
     if (h->iter_graph_def) { cudaGraphDestroy(h->iter_graph_def); h->iter_graph_def = nullptr; }
 }

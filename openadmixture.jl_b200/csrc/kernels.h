@@ -39,14 +39,16 @@ cudaError_t launch_decode_counts(const uint8_t *bed, int64_t I, int64_t J, int64
 
 /* mixed-precision sweeps on tensor cores (sweeps_mixed.cu) */
 cudaError_t prepare_mixed(int K);
-SweepPlan plan_sweep_q_mixed(int K, int64_t I, int64_t J, int sms);
+/* The mixed-form plans pick their slice count for whole waves of resident CTAs, at most smax
+ * slices (the partial-sum buffers of a handle are sized for its first plans). */
+SweepPlan plan_sweep_q_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax = INT64_MAX);
 /* The mixed Q sweep first builds its per-chunk P packages in pkg (sweep_q_mixed_pkg_bytes). */
 cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                  const double *p, const SweepPlan &pl, double *out, int *err, uint8_t *pkg,
                                  cudaStream_t st);
 size_t sweep_q_mixed_pkg_bytes(int K, int64_t J);
 
-SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms);
+SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax = INT64_MAX);
 /* The mixed P sweep first builds its per-chunk Q packages in pkg (sweep_p_mixed_pkg_bytes).
  * mode 0: gradient / Hessian rows (T + K); mode 1: the EM P-step's two sums (2K, k_emp_finalize). */
 cudaError_t launch_sweep_p_mixed(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
@@ -55,7 +57,7 @@ cudaError_t launch_sweep_p_mixed(int K, int mode, const uint8_t *bed, int64_t I,
 size_t sweep_p_mixed_pkg_bytes(int K, int64_t I);
 /* one CTA whose bounded wait on an mbarrier nothing completes runs out and sets *err */
 cudaError_t launch_wait_probe(int *err, uint32_t polls, cudaStream_t st);
-SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms);
+SweepPlan plan_loglik_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax = INT64_MAX);
 /* err and pkg are accepted for symmetry with the sweeps; the log-likelihood stays on the CUDA cores. */
 cudaError_t launch_loglik_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                 const double *p, const SweepPlan &pl, double *partial, double *out, int *err,

@@ -1195,19 +1195,66 @@ cudaError_t launch_ll_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t 
     return cudaGetLastError();
 }
 
-/* slices over the second axis: enough CTAs to cover the GPU, each slice a multiple of `unit` */
-SweepPlan plan_rows(int64_t rows, int64_t cols, int sms, int per_sm, int64_t unit)
+/* Slices over the second axis for CTAs of 128 rows, `per_sm` of which are resident per SM.  CTAs
+ * of one launch take equal time, so the launch lasts ceil(gx S / (sms per_sm)) waves of CTAs that
+ * each do 1/S of a row tile's work; S minimises waves / S, plus 0.5 % per extra slice (each adds a
+ * partial slice for the consumer to read).  Slices are multiples of `unit`, at least 4 units
+ * long, and at most smax. */
+SweepPlan plan_rows(int64_t rows, int64_t cols, int sms, int per_sm, int64_t unit, int64_t smax)
 {
     SweepPlan pl;
-    pl.gx = (int)((rows + 127) / 128);
-    const int64_t target = (int64_t)sms * per_sm;
-    int64_t S = (target + pl.gx - 1) / pl.gx;
-    S = std::max<int64_t>(1, std::min<int64_t>(S, (cols + 4 * unit - 1) / (4 * unit)));
-    int64_t slice = (cols + S - 1) / S;
-    slice = (slice + unit - 1) / unit * unit;
-    pl.slice = slice;
-    pl.S = (int)((cols + slice - 1) / slice);
+    pl.gx = (int)std::max<int64_t>(1, (rows + 127) / 128);
+    pl.S = 1;
+    pl.slice = std::max<int64_t>(unit, (cols + unit - 1) / unit * unit);
+    if (cols <= 0) return pl;
+    const int64_t cap = std::max<int64_t>(1, (int64_t)sms * per_sm);
+    const int64_t fill = (cap + pl.gx - 1) / pl.gx;   /* slices that fill the GPU once */
+    const int64_t top = std::min<int64_t>({std::max<int64_t>(1, (cols + 4 * unit - 1) / (4 * unit)),
+                                           std::max<int64_t>(16, 2 * fill), std::max<int64_t>(1, smax)});
+    double best = 1e300;
+    for (int64_t s = 1; s <= top; ++s) {
+        const int64_t slice = ((cols + s - 1) / s + unit - 1) / unit * unit;
+        const int64_t S = (cols + slice - 1) / slice;
+        const int64_t waves = ((int64_t)pl.gx * S + cap - 1) / cap;
+        const double cost = (double)waves / (double)S * (1.0 + 0.005 * (double)(S - 1));
+        if (cost < best - 1e-12) {
+            best = cost;
+            pl.S = (int)S;
+            pl.slice = slice;
+        }
+    }
     return pl;
+}
+
+/* resident CTAs per SM of the mixed kernels (occupancy at their shared memory; needs
+ * prepare_mixed(K) first), cached per kernel and K; `fallback` when it cannot be queried */
+template <int K>
+int resident_t(int kind)
+{
+    int n = 0;
+    cudaError_t e;
+    if (kind == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_q_mixed<K>, MQ_CTA, MQ<K>::SMEM);
+    else if (kind == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_p_mixed<K, false>, MP_CTA, MP<K>::SMEM);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_loglik_mixed<K>, 128, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int resident(int kind, int K, int fallback)
+{
+    static int cache[3][17] = {};
+    if (K < 1 || K > 16) return fallback;
+    int &c = cache[kind][K];
+    if (c <= 0) {
+        int n = 0;
+        ADMIX_DISPATCH_K(K, n = resident_t<KK>(kind));
+        if (n <= 0) return fallback;
+        c = n;
+    }
+    return c;
 }
 
 } // namespace
@@ -1220,23 +1267,21 @@ cudaError_t prepare_mixed(int K)
 }
 
 /* One CTA per 128 individuals and SNP slice. */
-SweepPlan plan_sweep_q_mixed(int K, int64_t I, int64_t J, int sms)
+SweepPlan plan_sweep_q_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax)
 {
-    (void)K;
-    return plan_rows(I, J, sms, 4, MQ_JC);
+    return plan_rows(I, J, sms, resident(0, K, 3), MQ_JC, smax);
 }
 
 /* One CTA per 128 SNPs and individual slice (slices are multiples of 64 individuals). */
-SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms)
+SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax)
 {
-    (void)K;
-    return plan_rows(J, I, sms, 4, MP_IC);
+    return plan_rows(J, I, sms, resident(1, K, 3), MP_IC, smax);
 }
 
-SweepPlan plan_loglik_mixed(int64_t I, int64_t J, int sms)
+SweepPlan plan_loglik_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax)
 {
-    /* CTAs of 128 threads x ML_JT SNPs; 6 CTAs per SM fit at K <= 10 (80 registers) */
-    return plan_rows((J + ML_JT - 1) / ML_JT, I, sms, 6, ML_IC);
+    /* CTAs of 128 threads x ML_JT SNPs */
+    return plan_rows((J + ML_JT - 1) / ML_JT, I, sms, resident(2, K, 4), ML_IC, smax);
 }
 
 cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
