@@ -47,6 +47,9 @@ def test_create_rejects_bad_arguments_without_touching_a_gpu(oa):
     # device variant: a source pitch below ceil(I/4) is rejected before any device call
     assert lib.admix_create_device(40, 4, 3, 3, None, 9, 0, C.byref(h)) == N.ADMIX_ERR_ARG
     assert b"src_pitch" in lib.admix_last_error(None)
+    # the failure-reporting self-test needs a handle
+    assert lib.admix_selftest_wait_timeout(None) == N.ADMIX_ERR_ARG
+    assert b"handle is NULL" in lib.admix_last_error(None)
 
 
 def test_engine_requires_gpu_path(oa):
