@@ -54,6 +54,10 @@ def _args():
                          "handle); times the iteration only")
     ap.add_argument("--I", type=int, default=None, help="override the configuration's I (--pass-only runs)")
     ap.add_argument("--J", type=int, default=None, help="override the configuration's J (--pass-only runs)")
+    ap.add_argument("--precision", action="store_true",
+                    help="report the mixed form's errors against the FP64 form (default for c3)")
+    ap.add_argument("--cpu-ttc", action="store_true",
+                    help="also time the oracle to convergence on the whole cohort (default for c1)")
     ap.add_argument("--pass-only", default=None,
                     choices=["loglik", "q_sweep", "p_sweep", "q_qp", "p_qp", "em"],
                     help="set up the cohort and launch one pass warmup+steps times (for profilers)")
@@ -98,11 +102,13 @@ def max_over_ranks(value: float, world: int, device: str) -> float:
 
 
 def _peaks():
+    """(HBM GB/s, burst bf16 TFLOP/s, sustained bf16 TFLOP/s, 'measured' | 'fallback')"""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
-    return 6650.0, 1590.0, "fallback"
+        burst = float(d["bf16_tflops"])
+        return float(d["hbm_gbs"]), burst, float(d.get("bf16_tflops_sustained", burst)), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
 
 
 class ClockSampler:
@@ -171,21 +177,17 @@ def _traffic(kernel: str, config: str):
     return None
 
 
-def _cpu_sample_spec(oa, spec, J_sample):
-    return spec.scaled(J=J_sample)
-
-
 def _cpu_sample_J(spec, cells=2e8):
     """SNP subset for the CPU runs: about `cells` genotype cells per pass."""
     return int(max(200, min(spec.J, cells / spec.I)))
 
 
-def cpu_baseline(oa, spec, steps=2):
+def cpu_baseline(oa, spec, steps=5):
     """The oracle (C restatement, OpenMP on all host cores) on a bounded SNP sample of the
     same cohort: QN iterations from an EM-primed start, metric scaled by the sample."""
     import oracle
     J_s = _cpu_sample_J(spec)
-    s = _cpu_sample_spec(oa, spec, J_s)
+    s = spec.scaled(J=J_s)
     g, _, _ = oa.make_cohort(s)
     x0 = oa.init_x(s.I, s.J, s.K, 5)
     r = oracle.OracleRun(g.data, s.I, s.J, s.K, 3, x0)
@@ -198,7 +200,64 @@ def cpu_baseline(oa, spec, steps=2):
     t = statistics.median(times)
     return {"value": s.I * s.J * s.K ** 2 / t, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
             "sample": f"oracle admixture_qn iteration on I={s.I}, J={s.J} (SNP subset), K={s.K}; "
-                      f"median of {steps} iteration(s), {t:.2f} s each"}
+                      f"median of {steps} iterations, {t:.2f} s each"}
+
+
+def cpu_ttc(oa, g, spec, seed):
+    """Time to converge of the oracle on the whole cohort from the random start the GPU legs use
+    (init_x(seed), 5 EM iterations, then admixture_qn! to reldiff < 1e-7): the reference's CPU
+    path restated, on all host cores."""
+    import oracle
+    x0 = oa.init_x(spec.I, spec.J, spec.K, seed)
+    host = g.to_host() if hasattr(g, "to_host") else g
+    t0 = time.perf_counter()
+    r = oracle.OracleRun(host.data, spec.I, spec.J, spec.K, 3, x0)
+    r.init_em(5)
+    hist, conv = r.admixture_qn(1000, 1e-7)
+    secs = time.perf_counter() - t0
+    return {"seconds": secs, "iterations": int(len(hist)), "converged": bool(conv), "final_ll": float(r.ll_new),
+            "cores": oracle.num_threads(), "kind": "port",
+            "start": f"init_x(seed={seed}) + 5 EM, rtol 1e-7 (the GPU legs' start)"}
+
+
+def _row_rel(a, b):
+    import numpy as np
+    a = a.reshape(a.shape[0], -1); b = b.reshape(b.shape[0], -1)
+    scale = np.abs(b).max(axis=1, keepdims=True)
+    return np.max(np.abs(a - b) / np.maximum(scale, 1e-300), axis=1)
+
+
+def precision_report(oa, g, spec, x, ll):
+    """Error of the mixed form against the FP64 form at one point (x, an EM-primed start):
+    Q- and P-side gradients and Hessians (relative to the largest entry of each problem's row;
+    max and median over problems), the signed relative bias of the Hessian diagonals, and the
+    mixed form's in-iteration log-likelihoods against the FP64 pass at the points they were taken."""
+    import numpy as np
+    out = {}
+    d = oa.AdmixData(spec.I, spec.J, spec.K, 3, rng=0)
+    with oa.CuAdmixData(d, g) as h64, oa.CuAdmixData(d, g, flags=oa.ADMIX_FLAG_MIXED) as hmx:
+        for h in (h64, hmx):
+            h.upload(oa.X, x)
+        for side in ("q", "p"):
+            H0, z0 = getattr(h64, f"grad_hess_{side}")(oa.X, oa.X)
+            H1, z1 = getattr(hmx, f"grad_hess_{side}")(oa.X, oa.X)
+            gz, gh = _row_rel(z1, z0), _row_rel(H1, H0)
+            dg0 = np.diagonal(H0, axis1=1, axis2=2)
+            dg1 = np.diagonal(H1, axis1=1, axis2=2)
+            bias = (dg1 - dg0) / dg0
+            out[f"grad_{side}"] = {"max": float(gz.max()), "median": float(np.median(gz))}
+            out[f"hess_{side}"] = {"max": float(gh.max()), "median": float(np.median(gh))}
+            out[f"hess_{side}_diag_bias"] = {"mean": float(bias.mean()), "max_abs": float(np.abs(bias).max())}
+            del H0, H1
+        d.x[:] = x
+        d.ll_new = ll
+        recs = oa.admixture_qn(d, g, 1, 0.0, d_cu=hmx, quiet=True)
+        ll_b, ll_q = hmx.loglik(oa.X_NEXT2), hmx.loglik(oa.X_TMP)     # admix_loglik: the FP64 pass
+        out["loglik_basic_rel"] = float((recs[-1]["ll_basic"] - ll_b) / abs(ll_b))
+        out["loglik_qn_rel"] = float((recs[-1]["ll_qn"] - ll_q) / abs(ll_q))
+    out["note"] = ("mixed vs FP64 form at the EM-primed start; loglik_*_rel: signed relative error of the "
+                   "mixed in-iteration log-likelihood against the FP64 pass at the same point")
+    return out
 
 
 def run_reference(args, rank, world):
@@ -207,7 +266,7 @@ def run_reference(args, rank, world):
     import oracle
     import openadmixture_b200 as oa
     spec = oa.COHORTS[args.config]
-    J_s = _cpu_sample_J(spec, 4e7)
+    J_s = _cpu_sample_J(spec)
     s = spec.scaled(J=J_s)
     g, _, _ = oa.make_cohort(s)
     r = oracle.OracleRun(g.data, s.I, s.J, s.K, 3, oa.init_x(s.I, s.J, s.K, 5))
@@ -288,6 +347,11 @@ def ttc_legs(oa, g, spec, rank, world, mixed: bool, plain: bool) -> dict:
             target = ref["ll"] - 1e-6 * abs(ref["ll"])
             r["iterations_to_target"], r["seconds_to_target"] = _hit(r, target)
             extra["final_ll_rel_vs_plain"] = abs(r["ll"] - ref["ll"]) / abs(ref["ll"])
+            # the converged Q and P against the plain FP64 solve (same start for the random legs;
+            # population labels can differ for the learned start, so only the random legs compare)
+            if name != "chosen_learned":
+                extra["final_q_maxabs_vs_plain"] = float(abs(r["x"][: g.I] - ref["x"][: g.I]).max())
+                extra["final_p_maxabs_vs_plain"] = float(abs(r["x"][g.I:] - ref["x"][g.I:]).max())
         else:
             r["iterations_to_target"] = r["seconds_to_target"] = None
         out[name] = _leg(r, extra)
@@ -336,6 +400,9 @@ def run_ours(args, rank, world, local_rank):
     t_upload = time.perf_counter() - t0
     oa.init_em(d, g, 5, d_cu=d_cu, quiet=True)
     x_em, ll_em = d.x.copy(), d.ll_new
+    precision = None
+    if (args.precision or args.config == "c3") and args.form == "mixed" and not args.stream_block:
+        precision = precision_report(oa, g, spec, x_em, ll_em)
     d_cu.upload(oa.X, x_em)
     d_cu.set_ll(ll_em)
     lib = N.admix_lib()
@@ -395,7 +462,7 @@ def run_ours(args, rank, world, local_rank):
         "p_sweep": 2 * spec.I * spec.J * (K * K + K) + 2 * spec.I * spec.J * K,
         "loglik": 2 * spec.I * spec.J * K,
     }
-    hbm, bf16, peak_kind = _peaks()
+    hbm, bf16, bf16_sus, peak_kind = _peaks()
     achieved = alg_bytes[dom] / (passes[dom] / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": kern_name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "peak_kind": peak_kind,
@@ -405,15 +472,18 @@ def run_ours(args, rank, world, local_rank):
     if mx and dom in ("q_sweep", "p_sweep"):
         terms = 2 if dom == "q_sweep" else 1          # [W1 | W2] x [PP ; PbPb]  or  C x QQ
         roof["tensor_tflops"] = 2 * spec.I * spec.J * terms * T / (passes[dom] / 1e3) / 1e12
-        roof["note"] = ("mixed form: the Hessian contraction runs on tcgen05 (tensor_tflops, far below the "
-                        "pipe's peak); the sweep is bound by the FP32 producer's issue rate, not by HBM; "
-                        "frac is the HBM fraction of its packed-genotype stream")
+        roof["tensor_peak_tflops"] = bf16_sus
+        roof["tensor_frac"] = roof["tensor_tflops"] / bf16_sus
+        roof["note"] = ("mixed form: the Hessian contraction runs on tcgen05 (tensor_tflops against the "
+                        "sustained bf16 peak: tensor_frac); the sweep is bound by the FP32 producer work per "
+                        "cell on the CUDA cores, not by HBM or the tensor pipe; frac is the HBM fraction of "
+                        "its packed-genotype stream")
     if args.stream_block:
         # 6 genotype passes per iteration, each streamed host -> device once
         roof["stream_h2d_gbs"] = 6 * bytes_bed / (ms_max / args.steps / 1e3) / 1e9
         roof["note"] = ("out-of-core handle: every pass streams the packed genotypes from page-locked host "
                         "memory; stream_h2d_gbs is the host-to-device rate the iteration sustained")
-    elif dom in flops:
+    elif not mx and dom in flops:
         roof["fp64_tflops"] = flops[dom] / (passes[dom] / 1e3) / 1e12
         roof["note"] = ("FP64 plain form: the sweep is bound by the FP64 pipe, not HBM; frac is the HBM "
                         "fraction of its packed-genotype stream")
@@ -470,6 +540,8 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(oa, spec)
+        if args.cpu_ttc or args.config == "c1":
+            cpu["ttc"] = cpu_ttc(oa, g, spec, 100 + rank)
 
     if world > 1:
         dist.barrier()
@@ -496,6 +568,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof,
         "passes_ms": passes,
         "ttc": ttc,
+        "precision": precision,
         "vs_plain": vs_plain,
         "setup_s": {"generate": t_gen, "create_upload": t_upload},
         "clocks": clk,
@@ -617,7 +690,7 @@ def run_batch(args, rank, world, local_rank):
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    hbm, _, peak_kind = _peaks()
+    hbm, _, _, peak_kind = _peaks()
     Ib = (spec.I + 3) // 4
     alg = len(Ks) * 6 * Ib * spec.J                  # 6 genotype passes per member iteration
     achieved = alg / (ms / args.steps / 1e3) / 1e9

@@ -148,6 +148,14 @@ int admix_set_fixed(admix_ctx *h, int32_t fix_q, int32_t fix_p);
  * handles only (ADMIX_ERR_STATE otherwise). */
 int admix_selftest_wait_timeout(admix_ctx *h);
 int admix_qn_iteration(admix_ctx *h, int32_t iter, admix_iterinfo *out);
+/* admixture_qn!'s `mode` keyword (algorithms_outer.jl:63-65,126-137): ADMIX_QN_ZAL (default,
+ * update_UV! / update_QN!, quasi_newton.jl:5-9,29-31) or ADMIX_QN_LBQN (limited-memory Broyden,
+ * update_UV_LBQN! / update_QN_LBQN!, quasi_newton.jl:15-58).  Later iterations (admix_qn_iteration,
+ * admix_run_qn, batches) use it; the secant history U, V is shared, as in the reference, so
+ * switching modes in the middle of a run mixes the two modes' columns. */
+#define ADMIX_QN_ZAL   0
+#define ADMIX_QN_LBQN  1
+int admix_set_qn_mode(admix_ctx *h, int32_t mode);
 /* Iterations iter_offset+1 .. n_iter until reldiff < rtol.  hist (n_iter entries, may be
  * NULL) receives one record per iteration run. */
 int admix_run_qn(admix_ctx *h, int32_t n_iter, double rtol, int32_t iter_offset,
@@ -198,9 +206,10 @@ int admix_loglik_dev(const uint8_t *d_bed, int64_t I, int64_t J, int32_t K,
  * the library, ADMIX_NOALLOC_MAX_PARTIALS doubles (256 KiB) held by every GPU that loads it.
  * Cohorts needing more partial sums (I beyond about 33 million) are rejected with
  * ADMIX_ERR_UNSUPPORTED.  The first call on a device looks up the array's device address
- * (make it before any stream capture).  All calls share the array: calls that overlap on the
- * GPU race, so serialise them.  Asynchronous on `stream`; errors are reported by
- * admix_noalloc_last_error(). */
+ * (make it before any stream capture); so does the first call after the device's context was
+ * reset and recreated, since the array may have moved.  All calls share the array: calls that
+ * overlap on the GPU race, so serialise them.  Asynchronous on `stream`; errors are reported by
+ * admix_noalloc_last_error(), which a successful call clears. */
 #define ADMIX_NOALLOC_MAX_PARTIALS 32768
 int admix_loglik_dev_noalloc(const uint8_t *d_bed, int64_t I, int64_t J, int32_t K,
                              const double *d_q, const double *d_p, double *d_out, void *stream);

@@ -25,6 +25,7 @@ ADMIX_FLAG_MIXED = 2
 ADMIX_MAX_K = 16
 ADMIX_MAX_Q = 8
 
+ADMIX_QN_ZAL, ADMIX_QN_LBQN = 0, 1
 ADMIX_PASS_LOGLIK, ADMIX_PASS_QSWEEP, ADMIX_PASS_PSWEEP, ADMIX_PASS_QQP, ADMIX_PASS_PQP, ADMIX_PASS_EM = range(6)
 
 
@@ -77,6 +78,7 @@ ADMIX_SIGNATURES = {
     "admix_set_x": (C.c_int, [_P, C.c_int32, _D, _D]),
     "admix_get_x": (C.c_int, [_P, C.c_int32, _D, _D]),
     "admix_set_ll": (C.c_int, [_P, C.c_double]),
+    "admix_set_qn_mode": (C.c_int, [_P, C.c_int32]),
     "admix_get_ll": (C.c_int, [_P, _D]),
     "admix_loglik": (C.c_int, [_P, C.c_int32, _D]),
     "admix_em_q": (C.c_int, [_P]),

@@ -289,16 +289,21 @@ def admixture_qn(d: AdmixData, g, iter: int = 1000, rtol: float = 1e-7, *, d_cu:
                  g_cu=None, mode: str = "ZAL", iter_count_offset: int = 0, fix_p: bool = False,
                  fix_q: bool = False, verbose: bool = False, progress_bar: bool = False,
                  quiet: bool = False) -> list[dict]:
-    """admixture_qn!(d, g, iter, rtol) (algorithms_outer.jl:63-193), mode :ZAL, run on the device.
+    """admixture_qn!(d, g, iter, rtol) (algorithms_outer.jl:63-193), run on the device; mode "ZAL"
+    (default) or "LBQN" (quasi_newton.jl:15-58), fix_q / fix_p as the reference's keywords.
     Returns one record per iteration (ll_prev, ll_basic, ll_qn, ll_new, reldiff, ...)."""
     d_cu = _require_gpu(d_cu)
-    if mode != "ZAL":
-        raise NotImplementedError(f"mode={mode!r}: only the :ZAL mode run_admixture uses is on the device path")
-    d_cu._chk(N.admix_lib().admix_set_fixed(d_cu.handle, int(bool(fix_q)), int(bool(fix_p))))
+    modes = {"ZAL": N.ADMIX_QN_ZAL, "LBQN": N.ADMIX_QN_LBQN}
+    if str(mode).lstrip(":") not in modes:
+        raise ValueError(f"Invalid mode {mode!r} (:ZAL or :LBQN)")      # the reference's @assert false
+    lib = N.admix_lib()
+    d_cu._chk(lib.admix_set_qn_mode(d_cu.handle, modes[str(mode).lstrip(":")]))
+    d_cu._chk(lib.admix_set_fixed(d_cu.handle, int(bool(fix_q)), int(bool(fix_p))))
     try:
         return _admixture_qn_loop(d, d_cu, iter, rtol, iter_count_offset, verbose, quiet)
     finally:
-        d_cu._chk(N.admix_lib().admix_set_fixed(d_cu.handle, 0, 0))
+        d_cu._chk(lib.admix_set_fixed(d_cu.handle, 0, 0))
+        d_cu._chk(lib.admix_set_qn_mode(d_cu.handle, N.ADMIX_QN_ZAL))
 
 
 def _admixture_qn_loop(d: AdmixData, d_cu: CuAdmixData, iter: int, rtol: float, iter_count_offset: int,

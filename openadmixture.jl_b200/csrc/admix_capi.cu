@@ -25,6 +25,7 @@ struct admix_ctx {
     int K = 0, Q = 0;
     uint32_t flags = 0;
     int fix = 0;                     /* bit 0: fix_q, bit 1: fix_p (admixture_qn!'s keywords) */
+    int qn_mode = ADMIX_QN_ZAL;      /* admixture_qn!'s mode keyword: :ZAL or :LBQN */
     int dev = 0, sms = 148;
     cudaStream_t st = nullptr;
     uint8_t *bed = nullptr;
@@ -534,8 +535,10 @@ static cudaError_t enq_iteration(admix_ctx *h)
     if (e == cudaSuccess) e = (h->fix & 1) ? copy_q(ADMIX_X_NEXT2) : enq_update_q(h, 1);
     if (e == cudaSuccess) e = (h->fix & 2) ? copy_p(ADMIX_X_NEXT2) : enq_update_p(h, 1);
     if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_NEXT2, &h->sc->ll_basic, true);
-    if (e == cudaSuccess) e = launch_qn(h->Q, h->I, h->J, h->K, h->x[ADMIX_X], h->x[ADMIX_X_NEXT], h->x[ADMIX_X_NEXT2],
-                                        h->U, h->V, h->x[ADMIX_X_TMP], h->qn_partial, h->qnp, h->sc, h->sms, h->st);
+    if (e == cudaSuccess)
+        e = (h->qn_mode == ADMIX_QN_LBQN ? launch_lbqn : launch_qn)(
+            h->Q, h->I, h->J, h->K, h->x[ADMIX_X], h->x[ADMIX_X_NEXT], h->x[ADMIX_X_NEXT2], h->U, h->V,
+            h->x[ADMIX_X_TMP], h->qn_partial, h->qnp, h->sc, h->sms, h->st);
     if (e == cudaSuccess) e = enq_loglik(h, ADMIX_X_TMP, &h->sc->ll_qn, true);
     if (e == cudaSuccess) e = launch_accept(nx, h->x[ADMIX_X_TMP], h->x[ADMIX_X_NEXT2], h->x[ADMIX_X], h->sc, h->sms, h->st);
     return e;
@@ -741,6 +744,20 @@ int admix_set_fixed(admix_ctx *h, int32_t fix_q, int32_t fix_p)
         if (h->iter_graph) { cudaGraphExecDestroy(h->iter_graph); h->iter_graph = nullptr; }
         if (h->iter_graph_def) { cudaGraphDestroy(h->iter_graph_def); h->iter_graph_def = nullptr; }
         h->fix = fix;
+    }
+    return ADMIX_OK;
+}
+
+int admix_set_qn_mode(admix_ctx *h, int32_t mode)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (mode != ADMIX_QN_ZAL && mode != ADMIX_QN_LBQN)
+        return fail(h, ADMIX_ERR_ARG, "mode %d is neither ADMIX_QN_ZAL (0) nor ADMIX_QN_LBQN (1)", (int)mode);
+    if (mode != h->qn_mode) {
+        CK(h, cudaStreamSynchronize(h->st));
+        if (h->iter_graph) { cudaGraphExecDestroy(h->iter_graph); h->iter_graph = nullptr; }
+        if (h->iter_graph_def) { cudaGraphDestroy(h->iter_graph_def); h->iter_graph_def = nullptr; }
+        h->qn_mode = mode;
     }
     return ADMIX_OK;
 }

@@ -12,7 +12,8 @@
 struct DevScalars {
     double ll_new, ll_prev, ll_basic, ll_qn, reldiff;
     double ll_tmp;                 /* result slot of a stand-alone loglik */
-    double qn_cf[8];               /* inv(U'(U-V)) U'(x0 - x1) */
+    double qn_cf[8];               /* ZAL: inv(U'(U-V)) U'(x0 - x1); LBQN: the alpha_i of update_QN_LBQN! */
+    double qn_gamma;               /* LBQN: gamma_t = u'v / v'v */
     int32_t iter;                  /* iteration number i of the current QN step */
     int32_t accepted;
     int32_t fail_q, fail_p;

@@ -77,6 +77,9 @@ QNPlan plan_qn(int64_t n, int sms);
 cudaError_t launch_qn(int Q, int64_t I, int64_t J, int K, const double *x0, const double *x1,
                       const double *x2, double *U, double *V, double *x_tmp, double *partial,
                       const QNPlan &pl, DevScalars *sc, int sms, cudaStream_t st);
+cudaError_t launch_lbqn(int Q, int64_t I, int64_t J, int K, const double *x0, const double *x1,
+                        const double *x2, double *U, double *V, double *x_tmp, double *partial,
+                        const QNPlan &pl, DevScalars *sc, int sms, cudaStream_t st);
 cudaError_t launch_iter_begin(DevScalars *sc, cudaStream_t st);
 cudaError_t launch_accept(int64_t n, const double *x_tmp, const double *x_next2, double *x,
                           DevScalars *sc, int sms, cudaStream_t st);

@@ -15,9 +15,13 @@
  *
  * Host code cannot hand the array's name to a kernel (in host code it is only a stand-in
  * for the symbol, not a device address).  The first call on each device, with that device
- * current, looks the device address up with cudaGetSymbolAddress and caches it; make that
- * first call before any stream capture.
+ * current, looks the device address up with cudaGetSymbolAddress and caches it together with
+ * the device's current context; make that first call before any stream capture.  A device
+ * reset (cudaDeviceReset, or a host runtime that destroys and recreates the primary context)
+ * reloads the module and may move the array, so the address is looked up again whenever the
+ * current context is not the one it was cached under.
  */
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <mutex>
 #include <stdio.h>
@@ -30,6 +34,7 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void *g_scratch[kMaxDevices];
+CUcontext g_ctx[kMaxDevices];      /* the context each cached address belongs to */
 bool g_ready[kMaxDevices];
 thread_local char g_msg[256];
 
@@ -46,6 +51,7 @@ extern "C" int admix_loglik_dev_noalloc(const uint8_t *d_bed, int64_t I, int64_t
                                         const double *d_q, const double *d_p, double *d_out,
                                         void *stream)
 {
+    g_msg[0] = 0;   /* a successful call leaves no stale message behind */
     if (!d_bed || !d_q || !d_p || !d_out) return noalloc_fail(ADMIX_ERR_ARG, "NULL device pointer");
     if (I < 1 || J < 1) return noalloc_fail(ADMIX_ERR_ARG, "I and J must be >= 1");
     if (K < 1 || K > ADMIX_MAX_K) return noalloc_fail(ADMIX_ERR_UNSUPPORTED, "K outside [1, ADMIX_MAX_K]");
@@ -62,16 +68,33 @@ extern "C" int admix_loglik_dev_noalloc(const uint8_t *d_bed, int64_t I, int64_t
                  "(I up to about 33 million individuals)", (long long)nparts, ADMIX_NOALLOC_MAX_PARTIALS);
         return noalloc_fail(ADMIX_ERR_UNSUPPORTED, buf);
     }
+    /* the runtime call above made the device's primary context current; the driver's
+     * cuCtxGetCurrent is reached through the runtime, so the library needs no libcuda link */
+    CUcontext ctx = nullptr;
+    {
+        static CUresult (*get_ctx)(CUcontext *) = nullptr;
+        if (!get_ctx) {
+            void *fn = nullptr;
+            cudaDriverEntryPointQueryResult q;
+            if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+                q != cudaDriverEntryPointSuccess || !fn)
+                return noalloc_fail(ADMIX_ERR_CUDA, "cuCtxGetCurrent is not available");
+            get_ctx = (CUresult(*)(CUcontext *))fn;
+        }
+        if (get_ctx(&ctx) != CUDA_SUCCESS || ctx == nullptr)
+            return noalloc_fail(ADMIX_ERR_CUDA, "no current CUDA context");
+    }
     void *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_ready[dev]) {
+        if (!g_ready[dev] || g_ctx[dev] != ctx) {
             cudaError_t e = cudaGetSymbolAddress(&g_scratch[dev], g_loglik_scratch);
             if (e != cudaSuccess) {
                 char buf[200];
                 snprintf(buf, sizeof(buf), "cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
                 return noalloc_fail(ADMIX_ERR_CUDA, buf);
             }
+            g_ctx[dev] = ctx;
             g_ready[dev] = true;
         }
         scratch = g_scratch[dev];

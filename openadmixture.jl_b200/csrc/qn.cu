@@ -7,7 +7,8 @@
  *   project_p!(p_tmp), project_q!(q_tmp); accept x_tmp if ll_qn > ll_prev else x_next2.
  *
  * The iteration number i is read from DevScalars so one captured sequence of launches
- * serves every iteration.
+ * serves every iteration.  The LBQN mode of admixture_qn! (quasi_newton.jl:15-58) follows the
+ * ZAL kernels below.
  */
 #include "common.cuh"
 #include "kernels.h"
@@ -145,6 +146,130 @@ k_qn_extrap(int64_t I, int64_t J, const double *__restrict__ x1, const double *_
     }
 }
 
+/* ------------------------------------------------------------------------------------------
+ * LBQN mode (update_UV_LBQN!, quasi_newton.jl:15-23; update_QN_LBQN!, quasi_newton.jl:38-58):
+ *   shift the secant columns right, U[:,1] = x1 - x0, V[:,1] = (x2 - x1) - U[:,1];
+ *   gamma = u'v / v'v;  x_q = u;  for i = 1..m: alpha_i = (V_i' x_q) / (V_i' V_i), x_q -= alpha_i V_i;
+ *   x_tmp = x0 - (gamma x_q + sum_i alpha_i U_i)       (u = U[:,1], v = V[:,1], m = min(iter, Q))
+ * The column shift is an index change: logical column l (1 = newest) of iteration i is physical
+ * slot (i - l) mod Q.  Because x_q = u - sum_{l<i} alpha_l V_l, every dot product the loop takes is
+ * a combination of the Gram matrix V_l' V_l' and of V_l' u, so one pass over the vectors collects
+ * them all (per-block partials, reduced in a fixed order) and one thread runs the recurrence. */
+template <int Q>
+__global__ void __launch_bounds__(256)
+k_lbqn_dots(int64_t n, const double *__restrict__ x0, const double *__restrict__ x1,
+            const double *__restrict__ x2, double *__restrict__ U, double *__restrict__ V,
+            const DevScalars *__restrict__ sc, double *__restrict__ partial)
+{
+    __shared__ double red[8];
+    const int iter = sc->iter;
+    const int m = iter < Q ? iter : Q;
+    const int slot = (iter - 1) % Q;
+    double G[Q][Q], c[Q];
+#pragma unroll
+    for (int r = 0; r < Q; ++r) {
+        c[r] = 0.0;
+#pragma unroll
+        for (int t = 0; t < Q; ++t) G[r][t] = 0.0;
+    }
+    for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < n; a += (int64_t)gridDim.x * blockDim.x) {
+        const double xa1 = x1[a];
+        const double un = xa1 - x0[a];
+        const double vn = (x2[a] - xa1) - un;
+        U[a + n * slot] = un;
+        V[a + n * slot] = vn;
+        double v[Q];
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            v[l] = 0.0;
+            if (l < m) v[l] = (l == 0) ? vn : V[a + n * ((iter - 1 - l) % Q)];
+        }
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            c[l] = fma(v[l], un, c[l]);
+#pragma unroll
+            for (int t = 0; t < Q; ++t) G[l][t] = fma(v[l], v[t], G[l][t]);
+        }
+    }
+    constexpr int NV = Q * Q + Q;
+#pragma unroll
+    for (int w = 0; w < NV; ++w) {
+        const double val = (w < Q * Q) ? G[w / Q][w % Q] : c[w - Q * Q];
+        const double s = block_sum(val, red);
+        if (threadIdx.x == 0) partial[(size_t)blockIdx.x * NV + w] = s;
+    }
+}
+
+template <int Q>
+__global__ void k_lbqn_solve(int nblocks, const double *__restrict__ partial, DevScalars *__restrict__ sc)
+{
+    constexpr int NV = Q * Q + Q;
+    __shared__ double tot[NV];
+    for (int w = threadIdx.x; w < NV; w += blockDim.x) {
+        double s = 0.0;
+        for (int bl = 0; bl < nblocks; ++bl) s += partial[(size_t)bl * NV + w];
+        tot[w] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const int iter = sc->iter;
+    const int m = iter < Q ? iter : Q;
+    double alpha[Q];
+    for (int i = 0; i < m; ++i) {
+        double d = tot[Q * Q + i];                       /* V_i' x_q with x_q = u - sum_{l<i} alpha_l V_l */
+        for (int l = 0; l < i; ++l) d = __dsub_rn(d, __dmul_rn(alpha[l], tot[i * Q + l]));
+        const double rho = 1.0 / tot[i * Q + i];
+        alpha[i] = __dmul_rn(rho, d);
+    }
+    for (int r = 0; r < Q; ++r) sc->qn_cf[r] = r < m ? alpha[r] : 0.0;
+    sc->qn_gamma = tot[Q * Q] / tot[0];                 /* u'v / v'v, v = V_1 */
+    sc->qn_singular = (tot[0] == 0.0) ? 1 : 0;
+}
+
+/* x_tmp = x0 - (gamma (u - sum_l alpha_l V_l) + sum_l alpha_l U_l) in the reference's order of
+ * operations per element, then project_q! on Q columns and project_p! on P columns. */
+template <int K, int Q>
+__global__ void __launch_bounds__(256)
+k_lbqn_extrap(int64_t I, int64_t J, const double *__restrict__ x0, const double *__restrict__ U,
+              const double *__restrict__ V, const DevScalars *__restrict__ sc, double *__restrict__ x_tmp)
+{
+    const int64_t ncol = I + J, n = ncol * K;
+    const int iter = sc->iter;
+    const int m = iter < Q ? iter : Q;
+    const double gamma = sc->qn_gamma;
+    double al[Q];
+    int64_t off[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        al[l] = sc->qn_cf[l];
+        off[l] = n * (int64_t)((iter - 1 - (l < m ? l : 0)) % Q);
+    }
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncol; c += (int64_t)gridDim.x * blockDim.x) {
+        double b[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int64_t a = c * K + k;
+            double xq = U[a + off[0]];
+#pragma unroll
+            for (int l = 0; l < Q; ++l)
+                if (l < m) xq = __dsub_rn(xq, __dmul_rn(al[l], V[a + off[l]]));
+            double xr = __dmul_rn(gamma, xq);
+#pragma unroll
+            for (int l = 0; l < Q; ++l)
+                if (l < m) xr = __dadd_rn(xr, __dmul_rn(al[l], U[a + off[l]]));
+            b[k] = x0[a] - xr;
+        }
+        if (c < I) {
+            project_simplex_local<K>(b);
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) b[k] = fmin(fmax(b[k], 1e-5), 1.0 - 1e-5);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) x_tmp[c * K + k] = b[k];
+    }
+}
+
 __global__ void k_iter_begin(DevScalars *sc)
 {
     sc->ll_prev = sc->ll_new;
@@ -194,7 +319,38 @@ cudaError_t launch_qn_q(int64_t I, int64_t J, int K, const double *x0, const dou
     return e;
 }
 
+template <int Q>
+cudaError_t launch_lbqn_q(int64_t I, int64_t J, int K, const double *x0, const double *x1,
+                          const double *x2, double *U, double *V, double *x_tmp, double *partial,
+                          const QNPlan &pl, DevScalars *sc, int sms, cudaStream_t st)
+{
+    const int64_t n = (int64_t)K * (I + J);
+    k_lbqn_dots<Q><<<pl.blocks, 256, 0, st>>>(n, x0, x1, x2, U, V, sc, partial);
+    k_lbqn_solve<Q><<<1, 128, 0, st>>>(pl.blocks, partial, sc);
+    const int64_t ncol = I + J;
+    const int gb = (int)std::max<int64_t>(1, std::min<int64_t>((ncol + 255) / 256, (int64_t)sms * 16));
+    ADMIX_DISPATCH_K(K, (k_lbqn_extrap<KK, Q><<<gb, 256, 0, st>>>(I, J, x0, U, V, sc, x_tmp)));
+    return cudaGetLastError();
+}
+
 } // namespace
+
+cudaError_t launch_lbqn(int Q, int64_t I, int64_t J, int K, const double *x0, const double *x1,
+                        const double *x2, double *U, double *V, double *x_tmp, double *partial,
+                        const QNPlan &pl, DevScalars *sc, int sms, cudaStream_t st)
+{
+    switch (Q) {
+    case 1: return launch_lbqn_q<1>(I, J, K, x0, x1, x2, U, V, x_tmp, partial, pl, sc, sms, st);
+    case 2: return launch_lbqn_q<2>(I, J, K, x0, x1, x2, U, V, x_tmp, partial, pl, sc, sms, st);
+    case 3: return launch_lbqn_q<3>(I, J, K, x0, x1, x2, U, V, x_tmp, partial, pl, sc, sms, st);
+    case 4: return launch_lbqn_q<4>(I, J, K, x0, x1, x2, U, V, x_tmp, partial, pl, sc, sms, st);
+    case 5: return launch_lbqn_q<5>(I, J, K, x0, x1, x2, U, V, x_tmp, partial, pl, sc, sms, st);
+    case 6: return launch_lbqn_q<6>(I, J, K, x0, x1, x2, U, V, x_tmp, partial, pl, sc, sms, st);
+    case 7: return launch_lbqn_q<7>(I, J, K, x0, x1, x2, U, V, x_tmp, partial, pl, sc, sms, st);
+    case 8: return launch_lbqn_q<8>(I, J, K, x0, x1, x2, U, V, x_tmp, partial, pl, sc, sms, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 QNPlan plan_qn(int64_t n, int sms)
 {

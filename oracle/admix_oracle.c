@@ -486,12 +486,45 @@ typedef struct {
     double ll_prev, ll_new;
     int32_t mu_mode;
     int32_t fix;                                /* bit 0: fix_q, bit 1: fix_p (algorithms_outer.jl:98-116) */
+    int32_t mode;                               /* 0 = :ZAL, 1 = :LBQN (algorithms_outer.jl:126-137) */
+    double *x_q, *x_r;                          /* LBQN work vectors, K*(I+J) each (structs.jl x_qq, x_rr) */
 } orc_state;
 
 static double *Qof(orc_state *s, double *x) { (void)s; return x; }
 static double *Pof(orc_state *s, double *x) { return x + (size_t)s->K * s->I; }
 
 /* update_q! (algorithms_inner.jl:167-231), CPU branch. */
+/* The per-problem QP loop of update_q! / update_p! (algorithms_inner.jl:205-221, 281-298):
+ * for each of n problems, the tableau of (XtX, r = -Xtz, x) (simplex form for the Q block, box
+ * form for the P block) and quadratic_program!; delta (K x n) receives the steps and status (n,
+ * may be NULL) the return values.  Exported on its own so a test can run the QPs on sums that
+ * came from elsewhere (the engine's). */
+void orc_qp_batch(const double *XtX, const double *r, const double *x, const double *vt, int K, int64_t n,
+                  int simplex, int mu_mode, double *delta, int32_t *status)
+{
+    #pragma omp parallel
+    {
+        int m = simplex ? K + 2 : K + 1;
+        double *tab = (double *)malloc(sizeof(double) * m * m);
+        double *tk = (double *)malloc(sizeof(double) * (K + 2));
+        double *d = (double *)malloc(sizeof(double) * m);
+        double *tmp = (double *)malloc(sizeof(double) * m);
+        double *pmin = (double *)calloc(K, sizeof(double));
+        double *pmax = (double *)malloc(sizeof(double) * K);
+        int *swept = (int *)malloc(sizeof(int) * K);
+        for (int k = 0; k < K; ++k) pmax[k] = 1.0;
+        #pragma omp for schedule(dynamic, 64)
+        for (int64_t i = 0; i < n; ++i) {
+            orc_create_tableau(tab, XtX + (size_t)K * K * i, r + (size_t)K * i, x + (size_t)K * i, vt, K,
+                               simplex, mu_mode, tk);
+            int st = orc_quadratic_program(delta + (size_t)K * i, tab, x + (size_t)K * i, pmin, pmax, K,
+                                           simplex ? 1 : 0, d, tmp, swept);
+            if (status) status[i] = st;
+        }
+        free(tab); free(tk); free(d); free(tmp); free(pmin); free(pmax); free(swept);
+    }
+}
+
 void orc_update_q(orc_state *s, int update2, int32_t *status)
 {
     const int K = s->K;
@@ -503,27 +536,7 @@ void orc_update_q(orc_state *s, int update2, int32_t *status)
     s->ll_prev = s->ll_new;
     orc_grad_hess_q(s->bed, I, J, K, q, p, s->XtX_q, s->Xtz_q);
     for (int64_t a = 0; a < (int64_t)K * I; ++a) s->Xtz_q[a] *= -1.0;
-    #pragma omp parallel
-    {
-        int n = K + 2;
-        double *tab = (double *)malloc(sizeof(double) * n * n);
-        double *tk = (double *)malloc(sizeof(double) * (K + 2));
-        double *d = (double *)malloc(sizeof(double) * n);
-        double *tmp = (double *)malloc(sizeof(double) * n);
-        double *pmin = (double *)calloc(K, sizeof(double));
-        double *pmax = (double *)malloc(sizeof(double) * K);
-        int *swept = (int *)malloc(sizeof(int) * K);
-        for (int k = 0; k < K; ++k) pmax[k] = 1.0;
-        #pragma omp for schedule(dynamic, 64)
-        for (int64_t i = 0; i < I; ++i) {
-            orc_create_tableau(tab, s->XtX_q + (size_t)K * K * i, s->Xtz_q + (size_t)K * i,
-                               q + (size_t)K * i, s->vt, K, 1, s->mu_mode, tk);
-            int st = orc_quadratic_program(qdiff + (size_t)K * i, tab, q + (size_t)K * i,
-                                           pmin, pmax, K, 1, d, tmp, swept);
-            if (status) status[i] = st;
-        }
-        free(tab); free(tk); free(d); free(tmp); free(pmin); free(pmax); free(swept);
-    }
+    orc_qp_batch(s->XtX_q, s->Xtz_q, q, s->vt, K, I, 1, s->mu_mode, qdiff, status);
     for (int64_t a = 0; a < (int64_t)K * I; ++a) q_next[a] = q[a] + qdiff[a];
     orc_project_q(q_next, I, K);
 }
@@ -540,27 +553,7 @@ void orc_update_p(orc_state *s, int update2, int32_t *status)
     s->ll_prev = s->ll_new;
     orc_grad_hess_p(s->bed, I, J, K, q, p, s->XtX_p, s->Xtz_p);
     for (int64_t a = 0; a < (int64_t)K * J; ++a) s->Xtz_p[a] *= -1.0;
-    #pragma omp parallel
-    {
-        int n = K + 1;
-        double *tab = (double *)malloc(sizeof(double) * n * n);
-        double *tk = (double *)malloc(sizeof(double) * (K + 2));
-        double *d = (double *)malloc(sizeof(double) * n);
-        double *tmp = (double *)malloc(sizeof(double) * n);
-        double *pmin = (double *)calloc(K, sizeof(double));
-        double *pmax = (double *)malloc(sizeof(double) * K);
-        int *swept = (int *)malloc(sizeof(int) * K);
-        for (int k = 0; k < K; ++k) pmax[k] = 1.0;
-        #pragma omp for schedule(dynamic, 256)
-        for (int64_t j = 0; j < J; ++j) {
-            orc_create_tableau(tab, s->XtX_p + (size_t)K * K * j, s->Xtz_p + (size_t)K * j,
-                               p + (size_t)K * j, s->vt, K, 0, s->mu_mode, tk);
-            int st = orc_quadratic_program(pdiff + (size_t)K * j, tab, p + (size_t)K * j,
-                                           pmin, pmax, K, 0, d, tmp, swept);
-            if (status) status[j] = st;
-        }
-        free(tab); free(tk); free(d); free(tmp); free(pmin); free(pmax); free(swept);
-    }
+    orc_qp_batch(s->XtX_p, s->Xtz_p, p, s->vt, K, J, 0, s->mu_mode, pdiff, status);
     for (int64_t a = 0; a < (int64_t)K * J; ++a) p_next[a] = p[a] + pdiff[a];
     orc_project_p(p_next, (int64_t)K * J);
 }
@@ -658,7 +651,46 @@ void orc_qn_step(orc_state *s, int iter)
     }
 }
 
-/* One iteration of admixture_qn! (algorithms_outer.jl:92-159), mode = :ZAL.  With fix_q / fix_p
+/* update_UV_LBQN! (quasi_newton.jl:15-23) then update_QN_LBQN! (quasi_newton.jl:38-58) on the
+ * first m = min(iter, Q) columns, written out as the reference's vector operations. */
+static double orc_dot(const double *a, const double *b, int64_t n)
+{
+    double acc = 0.0;
+    for (int64_t t = 0; t < n; ++t) acc += a[t] * b[t];
+    return acc;
+}
+
+void orc_qn_step_lbqn(orc_state *s, int iter)
+{
+    const int64_t n = (int64_t)s->K * (s->I + s->J);
+    const int Q = s->Q;
+    double *U = s->U, *V = s->V;
+    for (int c = (iter < Q ? iter : Q) - 1; c >= 1; --c) {          /* for i in min(iter, Q):-1:2 */
+        memcpy(U + n * c, U + n * (c - 1), sizeof(double) * (size_t)n);
+        memcpy(V + n * c, V + n * (c - 1), sizeof(double) * (size_t)n);
+    }
+    for (int64_t a = 0; a < n; ++a) {
+        U[a] = s->x_next[a] - s->x[a];
+        V[a] = s->x_next2[a] - s->x_next[a];
+        V[a] = V[a] - U[a];                                           /* x2 - 2x1 + x0 */
+    }
+    const int m = iter < Q ? iter : Q;
+    const double gamma = orc_dot(U, V, n) / orc_dot(V, V, n);
+    double alpha[8];
+    memcpy(s->x_q, U, sizeof(double) * (size_t)n);
+    for (int i = 0; i < m; ++i) {
+        const double *Vi = V + n * i;
+        const double rho = 1.0 / orc_dot(Vi, Vi, n);
+        alpha[i] = rho * orc_dot(Vi, s->x_q, n);
+        for (int64_t a = 0; a < n; ++a) s->x_q[a] = s->x_q[a] - alpha[i] * Vi[a];
+    }
+    for (int64_t a = 0; a < n; ++a) s->x_r[a] = gamma * s->x_q[a];
+    for (int i = 0; i < m; ++i)
+        for (int64_t a = 0; a < n; ++a) s->x_r[a] = s->x_r[a] + alpha[i] * U[a + n * i];
+    for (int64_t a = 0; a < n; ++a) s->x_tmp[a] = s->x[a] - s->x_r[a];
+}
+
+/* One iteration of admixture_qn! (algorithms_outer.jl:92-159), mode = :ZAL or :LBQN (s->mode).  With fix_q / fix_p
  * (s->fix bits 0 / 1) the block is copied instead of updated: q_next .= q, q_next2 .= q
  * (algorithms_outer.jl:98-116), likewise p.  info[0..4] = (prev, basic, qn, new, reldiff).
  * Returns 1 when reldiff < rtol. */
@@ -676,7 +708,7 @@ int orc_qn_iteration(orc_state *s, int iter, double rtol, double *info,
     if (s->fix & 2) memcpy(Pof(s, s->x_next2), Pof(s, s->x), np); else orc_update_p(s, 1, st_p);
     s->ll_prev = ll_prev;
     double ll_basic = orc_loglik_x(s, s->x_next2);
-    orc_qn_step(s, iter);
+    if (s->mode == 1) orc_qn_step_lbqn(s, iter); else orc_qn_step(s, iter);
     orc_project_p(Pof(s, s->x_tmp), (int64_t)K * J);
     orc_project_q(Qof(s, s->x_tmp), I, K);
     double ll_qn = orc_loglik_x(s, s->x_tmp);

@@ -33,6 +33,7 @@ class OrcState(C.Structure):
         ("U", _D), ("V", _D), ("vt", _D),
         ("ll_prev", C.c_double), ("ll_new", C.c_double),
         ("mu_mode", C.c_int32), ("fix", C.c_int32),
+        ("mode", C.c_int32), ("x_q", _D), ("x_r", _D),
     ]
 
 
@@ -66,6 +67,7 @@ def lib() -> C.CDLL:
             "orc_project_q1": (None, [_D, C.c_int, C.c_double]),
             "orc_project_q": (None, [_D, C.c_int64, C.c_int]),
             "orc_project_p": (None, [_D, C.c_int64]),
+            "orc_qp_batch": (None, [_D, _D, _D, _D, C.c_int, C.c_int64, C.c_int, C.c_int, _D, _I32]),
             "orc_update_q": (None, [C.POINTER(OrcState), C.c_int, _I32]),
             "orc_update_p": (None, [C.POINTER(OrcState), C.c_int, _I32]),
             "orc_loglik_x": (C.c_double, [C.POINTER(OrcState), _D]),
@@ -154,6 +156,20 @@ def quadratic_program(tab, par, p: int, c: int):
     return it, delta, tab
 
 
+def qp_batch(XtX, Xtz, x, simplex: bool, mu_mode: int = MU_AS_EXECUTED):
+    """The QPs of update_q! (simplex=True) or update_p! (simplex=False) on given sums: XtX (n, K, K),
+    Xtz (n, K) as the sweep returns them (negated here, as algorithms_inner.jl:196,272 does), x (n, K)
+    the current block.  Returns (status (n,) int32, delta (n, K))."""
+    n, K = x.shape
+    r = np.ascontiguousarray(-np.asarray(Xtz, dtype=np.float64))
+    H = np.ascontiguousarray(XtX, dtype=np.float64)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    st = np.empty(n, np.int32); delta = np.empty((n, K))
+    lib().orc_qp_batch(_d(H), _d(r), _d(xx), _d(np.ascontiguousarray(vt_ones(K))), K, n, int(simplex), mu_mode,
+                       _d(delta), st.ctypes.data_as(_I32))
+    return st, delta
+
+
 def project_q1(b, pseudocount=1e-5):
     b = np.ascontiguousarray(b, dtype=np.float64).copy()
     lib().orc_project_q1(_d(b), len(b), pseudocount)
@@ -170,7 +186,7 @@ class OracleRun:
     """Oracle mirror of AdmixData + the outer loop (structs.jl, algorithms_outer.jl)."""
 
     def __init__(self, bed: np.ndarray, I: int, J: int, K: int, Q: int, x0: np.ndarray,
-                 mu_mode: int = MU_AS_EXECUTED, fix_q: bool = False, fix_p: bool = False):
+                 mu_mode: int = MU_AS_EXECUTED, fix_q: bool = False, fix_p: bool = False, mode: str = "ZAL"):
         self.bed = np.ascontiguousarray(bed)
         self.I, self.J, self.K, self.Q = I, J, K, Q
         n = I + J
@@ -189,6 +205,11 @@ class OracleRun:
         s.ll_prev = math.nan; s.ll_new = math.nan
         s.mu_mode = mu_mode
         s.fix = (1 if fix_q else 0) | (2 if fix_p else 0)
+        if mode not in ("ZAL", "LBQN"):
+            raise ValueError(f"Invalid mode {mode!r}")
+        s.mode = 1 if mode == "LBQN" else 0
+        self.x_q = np.zeros(n * K); self.x_r = np.zeros(n * K)
+        s.x_q, s.x_r = _d(self.x_q), _d(self.x_r)
         self.s = s
 
     @property

@@ -277,3 +277,72 @@ def test_oracle_fix_p_keeps_p_and_raises_loglik(oa, orc):
     assert np.all(np.diff(lls) >= -1e-9 * abs(lls[0]))
     assert np.max(np.abs(r.x[g.I:] - np.clip(p, 1e-5, 1 - 1e-5))) < 1e-12
     assert np.max(np.abs(r.x[: g.I] - x0[: g.I])) > 1e-2
+
+
+def test_qp_batch_reproduces_update_q_and_update_p(oa, orc):
+    """oracle.qp_batch (the QP loop of update_q! / update_p! on given sums) returns the statuses
+    and steps of the oracle's own updates when given the oracle's own sums."""
+    spec = oa.COHORTS["c1"].scaled(I=120, J=700, K=4, seed=5)
+    g, _, _ = oa.make_cohort(spec)
+    x0 = oa.init_x(g.I, g.J, 4, 9)
+    r = orc.OracleRun(g.data, g.I, g.J, 4, 3, x0)
+    r.init_em(2)
+    q, p = np.ascontiguousarray(r.x[: g.I]), np.ascontiguousarray(r.x[g.I:])
+    st = r.update_q(False)
+    H, z = orc.grad_hess_q(g.data, g.I, g.J, 4, q, p)
+    st2, dq = orc.qp_batch(H, z, q, True)
+    assert np.array_equal(st, st2)
+    assert np.array_equal(dq, r.x_tmp[: g.I])
+    st = r.update_p(False)
+    qn = np.ascontiguousarray(r.x_next[: g.I])
+    H, z = orc.grad_hess_p(g.data, g.I, g.J, 4, qn, p)
+    st2, dp = orc.qp_batch(H, z, p, False)
+    assert np.array_equal(st, st2)
+    assert np.array_equal(dp, r.x_tmp[g.I:])
+
+
+def _lbqn_numpy(U, V, x, x1, x2, it, Q):
+    """update_UV_LBQN! + update_QN_LBQN! (quasi_newton.jl:15-58) in numpy, columns of U, V as rows."""
+    for i in range(min(it, Q) - 1, 0, -1):
+        U[i] = U[i - 1]; V[i] = V[i - 1]
+    U[0] = x1 - x
+    V[0] = (x2 - x1) - U[0]
+    m = min(it, Q)
+    u, v = U[0], V[0]
+    gamma = np.dot(u, v) / np.dot(v, v)
+    xq = u.copy()
+    alpha = np.zeros(m)
+    for i in range(m):
+        rho = 1.0 / np.dot(V[i], V[i])
+        alpha[i] = rho * np.dot(V[i], xq)
+        xq = xq - alpha[i] * V[i]
+    xr = gamma * xq
+    for i in range(m):
+        xr = xr + alpha[i] * U[i]
+    return x - xr
+
+
+def test_lbqn_step_matches_numpy_restatement_and_converges(oa, orc):
+    """mode = :LBQN in the oracle: each iteration's QN point (before projection) is the numpy
+    restatement's, and the run reaches the :ZAL run's optimum."""
+    spec = oa.COHORTS["c1"].scaled(I=150, J=800, K=3, seed=12)
+    g, _, _ = oa.make_cohort(spec)
+    x0 = oa.init_x(g.I, g.J, 3, 4)
+    Q = 3
+    r = orc.OracleRun(g.data, g.I, g.J, 3, Q, x0, mode="LBQN")
+    r.init_em(3)
+    n = (g.I + g.J) * 3
+    U = np.zeros((Q, n)); V = np.zeros((Q, n))
+    for it in range(1, 7):
+        xb = r.x.copy().ravel()
+        r.qn_iteration(it)
+        want = _lbqn_numpy(U, V, xb, r.x_next.ravel(), r.x_next2.ravel(), it, Q).reshape(-1, 3)
+        want[: g.I] = np.array([orc.project_q1(row) for row in want[: g.I]])
+        want[g.I:] = orc.project_p(want[g.I:])
+        assert np.max(np.abs(r.x_tmp - want)) < 1e-12, it
+    hist, conv = r.admixture_qn(1000, 1e-7, iter_offset=6)
+    assert conv
+    rz = orc.OracleRun(g.data, g.I, g.J, 3, Q, x0)
+    rz.init_em(3)
+    hz, cz = rz.admixture_qn(1000, 1e-7)
+    assert cz and abs(r.ll_new - rz.ll_new) < 1e-6 * abs(rz.ll_new)
