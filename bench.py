@@ -321,10 +321,11 @@ def ttc_legs(oa, g, spec, rank, world, mixed: bool, plain: bool) -> dict:
     flags = oa.ADMIX_FLAG_MIXED if mixed else 0
     legs = {}
     model = ws.load_default(K) if mixed else None
+    ws_info = {}
     if model is not None:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        start = ws.learned_start(g, K, model)
+        start = ws.learned_start(g, K, model, info=ws_info)
         t_pred = time.perf_counter() - t0
         if start is not None:
             r = ws.run_to_target(g, K, flags=flags, start=start, rng=seed)
@@ -338,6 +339,7 @@ def ttc_legs(oa, g, spec, rank, world, mixed: bool, plain: bool) -> dict:
     chosen = "chosen_learned" if "chosen_learned" in legs else "chosen_random_em5"
     out = {"criterion": "reldiff < 1e-7; seconds from the start of initialisation (wall clock, device "
                         "synchronised at both ends)",
+           "warm_start_check": ws_info,
            "chosen": chosen, "form": ("mixed" if mixed else "plain-fp64")
            + (" + learned warm start" if chosen == "chosen_learned" else " + random start, 5 EM")}
     ref = legs.get("plain_fp64_random_em5")

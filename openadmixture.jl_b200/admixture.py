@@ -385,14 +385,15 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
     try:
         if warm_start is not None and (init_q is None or init_p is None):
             from . import warmstart
-            start = warmstart.learned_start(g, K, None if warm_start == "learned" else warm_start)
+            info = {}
+            start = warmstart.learned_start(g, K, None if warm_start == "learned" else warm_start, info=info)
             if start is not None:
                 if not quiet:
                     print("Starting from the learned warm start")
                 init_q = start[0].T if init_q is None else init_q
                 init_p = start[1].T if init_p is None else init_p
             elif not quiet:
-                print(f"No warm-start model applies to K={K}, J={g.J}; random start + EM")
+                print(f"No warm start ({info.get('fallback')}); random start + EM")
         if init_q is None or init_p is None:
             init_em(d, g, admix_n_em_iters, d_cu=d_cu, g_cu=g_cu, quiet=quiet)
         if init_q is not None:

@@ -2,12 +2,17 @@
 start on a held-out cohort of the same ancestral populations.
 
     python openadmixture.jl_b200/train_warmstart.py [--cohorts 50] [--I 20000] [--J 100000] [--K 8]
-        [--alpha 0.2] [--world 777] [--eval c5|held-out] [--out models/warmstart_k8.npz]
+        [--alpha 0.2] [--world 777] [--eval c5|held-out|other-world] [--out models/warmstart_k8.npz]
+    python openadmixture.jl_b200/train_warmstart.py --add-freq models/warmstart_k8.npz   (CPU only)
 
 Training cohorts and the evaluation cohort share their ancestral allele frequencies SNP by SNP
 (CohortSpec.p_seed = --world); individuals and admixture proportions differ.  Each training
 cohort is solved by the plain FP64 engine (5 EM iterations + quasi-Newton to rtol 1e-7); its
-converged Q, relabelled to the populations' order, is the target.  The evaluation reports, for
+converged Q, relabelled to the populations' order, is the target.  The model file also records the
+training cohorts' allele frequencies at the sketch SNPs; a cohort whose frequencies do not
+correlate with them (other ancestral populations) gets the random start instead
+(warmstart.learned_start).  --add-freq computes that record for an existing model file from the
+training cohorts' genotypes, drawn on the host.  The evaluation reports, for
 the random start (+ 5 EM iterations) and for the learned start, the iterations and seconds the
 chosen (mixed) form needs to reach a log-likelihood within 1e-6 relative of the plain FP64
 solution.  One JSON line is printed at the end.
@@ -30,6 +35,34 @@ def log(msg):
     print(msg, flush=True)
 
 
+def host_sketch_freq(g, snps: np.ndarray) -> np.ndarray:
+    """Allele frequency of each sketch SNP from host genotypes, as the sketch kernel computes it:
+    sum of dosages over non-missing individuals / (2 x their count)."""
+    cols = g.data[snps]                                       # (S, ceil(I/4)) bytes
+    codes = np.stack([(cols >> (2 * s)) & 3 for s in range(4)], axis=2).reshape(len(snps), -1)[:, : g.I]
+    dose = np.where(codes == 3, 2, np.where(codes == 2, 1, 0)).astype(np.float64)
+    nm = (codes != 1)
+    n = 2.0 * nm.sum(1)
+    return np.where(n > 0, (dose * nm).sum(1) / np.maximum(n, 1), 0.5).astype(np.float32)
+
+
+def add_freq(path: str, cohorts: int, I: int, J: int, K: int, alpha: float, world: int) -> None:
+    """Record the training world's sketch-SNP allele frequencies (mean over `cohorts` training
+    cohorts, drawn on the host) in an existing model file."""
+    import openadmixture_b200 as oa
+    z = dict(np.load(path))
+    snps = z["snps"]
+    acc = np.zeros(len(snps))
+    for c in range(cohorts):
+        spec = oa.CohortSpec(f"train{c}", I, J, K, alpha=alpha, miss=0.01, seed=1000 + c, p_seed=world)
+        g, _, _ = oa.make_cohort(spec)
+        acc += host_sketch_freq(g, snps)
+        log(f"cohort {c}: sketch frequencies")
+    z["freq"] = (acc / cohorts).astype(np.float32)
+    np.savez_compressed(path, **z)
+    log(f"wrote freq ({len(snps)} SNPs) into {path}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cohorts", type=int, default=50)
@@ -43,7 +76,15 @@ def main():
     ap.add_argument("--out", default=str(HERE / "models" / "warmstart_k8.npz"))
     ap.add_argument("--max-iter", type=int, default=100, help="QN iteration cap of each evaluation run")
     ap.add_argument("--model", default=None, help="skip training and evaluate this model file")
+    ap.add_argument("--add-freq", default=None, metavar="MODEL",
+                    help="record the training world's sketch-SNP frequencies in MODEL (host only) and exit")
+    ap.add_argument("--freq-cohorts", type=int, default=4)
     args = ap.parse_args()
+    if args.add_freq:
+        from openadmixture_b200.synth import WARMSTART_WORLD
+        add_freq(args.add_freq, args.freq_cohorts, args.I, args.J, args.K, args.alpha,
+                 WARMSTART_WORLD if args.world is None else args.world)
+        return
 
     import torch
     import openadmixture_b200 as oa
@@ -73,7 +114,8 @@ def main():
             log(f"cohort {c}: plain solve {r['iterations']} iterations, {r['seconds']:.1f} s, ll {r['ll']:.6e}")
             del g
         report["solve_seconds"] = time.perf_counter() - t_solve
-        model = ws.WarmStartMLP(len(snps), 32, args.K, seed=0, snps=snps)
+        freq = np.mean([sk.freq.detach().cpu().numpy() for sk, _ in data], axis=0)
+        model = ws.WarmStartMLP(len(snps), 32, args.K, seed=0, snps=snps, freq=freq)
         t_train = time.perf_counter()
         hist = ws.train(model, data, epochs=args.epochs, log=log)
         report["train_seconds"] = time.perf_counter() - t_train
@@ -85,6 +127,8 @@ def main():
 
     if args.eval == "c5":
         spec = oa.COHORTS["c5"].scaled(p_seed=args.world, seed=5)
+    elif args.eval == "other-world":     # populations the model was not trained on
+        spec = oa.COHORTS["c5"].scaled(p_seed=args.world + 1, seed=5)
     else:
         spec = oa.CohortSpec("held-out", args.I, args.J, args.K, alpha=args.alpha, miss=0.01, seed=999,
                              p_seed=args.world)
@@ -100,7 +144,11 @@ def main():
     rand = ws.run_to_target(g, spec.K, flags=oa.ADMIX_FLAG_MIXED, rng=1, target=target, max_iter=args.max_iter)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    start = ws.predict_start(model, g)
+    check = {}
+    start = ws.predict_start(model, g, info=check, check=True)
+    report["warm_start_check"] = dict(check)
+    if start is None:     # the run_admixture path falls back; time the refused start anyway
+        start = ws.predict_start(model, g)
     t_pred = time.perf_counter() - t0
     learned = ws.run_to_target(g, spec.K, flags=oa.ADMIX_FLAG_MIXED, rng=1, start=start, target=target,
                                max_iter=args.max_iter)

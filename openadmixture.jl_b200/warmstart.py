@@ -80,10 +80,12 @@ class WarmStartMLP:
     NAMES = ("w1", "b1", "w2", "b2", "w3", "b3")
 
     def __init__(self, S: int, R: int, K: int, H: int = 256, seed: int = 0, params: dict | None = None,
-                 snps: np.ndarray | None = None):
+                 snps: np.ndarray | None = None, freq: np.ndarray | None = None):
         torch = _torch()
         self.S, self.R, self.K, self.H = S, R, K, H
         self.snps = None if snps is None else np.ascontiguousarray(snps, dtype=np.int32)
+        # allele frequencies of the training cohorts at the sketch SNPs: the populations the model knows
+        self.freq = None if freq is None else np.ascontiguousarray(freq, dtype=np.float32)
         if self.snps is not None and len(self.snps) != S:
             raise ValueError(f"{len(self.snps)} sketch SNPs for an input of S={S}")
         dev = torch.device("cuda", torch.cuda.current_device())
@@ -106,6 +108,8 @@ class WarmStartMLP:
     def save(self, path) -> None:
         """FP16 weights on disk (the deployed precision); the sketch definition alongside."""
         extra = {} if self.snps is None else {"snps": np.ascontiguousarray(self.snps, dtype=np.int32)}
+        if self.freq is not None:
+            extra["freq"] = np.ascontiguousarray(self.freq, dtype=np.float32)
         np.savez_compressed(path, S=self.S, R=self.R, K=self.K, H=self.H, **extra,
                             **{k: v.detach().cpu().numpy().astype(np.float16) for k, v in self.p.items()})
 
@@ -114,7 +118,8 @@ class WarmStartMLP:
         z = np.load(path)
         params = {k: z[k].astype(np.float32) for k in cls.NAMES}
         return cls(int(z["S"]), int(z["R"]), int(z["K"]), int(z["H"]), params=params,
-                   snps=z["snps"] if "snps" in z.files else None)
+                   snps=z["snps"] if "snps" in z.files else None,
+                   freq=z["freq"] if "freq" in z.files else None)
 
     def forward(self, sk: Sketch, batch: int = 65536):
         """Class probabilities (n x K) of every individual of the sketch, as a device tensor."""
@@ -220,15 +225,45 @@ def warm_p(g, q: np.ndarray) -> np.ndarray:
     return dp.cpu().numpy()
 
 
-def predict_start(model: WarmStartMLP, g, snps: np.ndarray | None = None, R: int = 32, seed: int = 7):
+# a cohort whose sketch-SNP allele frequencies correlate less than this with the training
+# cohorts' comes from other ancestral populations than the model was trained on
+MIN_FREQ_CORR = 0.9
+
+
+def freq_corr(model: WarmStartMLP, sk: Sketch) -> float | None:
+    """Pearson correlation of the cohort's sketch-SNP allele frequencies with the training
+    cohorts' (None when the model does not record them)."""
+    if model.freq is None:
+        return None
+    a = sk.freq.detach().cpu().numpy().astype(np.float64)
+    b = model.freq.astype(np.float64)
+    a, b = a - a.mean(), b - b.mean()
+    den = np.sqrt((a * a).sum() * (b * b).sum())
+    return float((a * b).sum() / den) if den > 0 else 0.0
+
+
+def predict_start(model: WarmStartMLP, g, snps: np.ndarray | None = None, R: int = 32, seed: int = 7,
+                  info: dict | None = None, check: bool = False):
     """(q, p) starting point for run_admixture's init_q / init_p: Q (I, K) from the encoder (rows
     floored at the projection's pseudocount 1e-5 and renormalised), P (J, K) from the closed-form
-    step.  snps defaults to the sketch stored with the model."""
+    step.  snps defaults to the sketch stored with the model.  With check=True the start is
+    refused (None) when the cohort's sketch-SNP allele frequencies correlate less than
+    MIN_FREQ_CORR with the training cohorts' (populations the model was not trained on); `info`
+    receives the correlation and the decision."""
     if snps is None:
         snps = model.snps
     if snps is None:
         raise ValueError("the model carries no sketch SNP list; pass snps")
     sk = sketch(g, snps, R, seed)
+    corr = freq_corr(model, sk)
+    if info is not None:
+        info["freq_corr"] = corr
+        info["fallback"] = None
+    if check and corr is not None and corr < MIN_FREQ_CORR:
+        if info is not None:
+            info["fallback"] = (f"sketch allele frequencies correlate {corr:.3f} with the training cohorts' "
+                                f"(< {MIN_FREQ_CORR}): other ancestral populations")
+        return None
     q = model.forward(sk).cpu().numpy().astype(np.float64)
     q = np.maximum(q, 1e-5)
     q /= q.sum(1, keepdims=True)
@@ -245,17 +280,25 @@ def load_default(K: int) -> WarmStartMLP | None:
     return WarmStartMLP.load(path) if path.exists() else None
 
 
-def learned_start(g, K: int, model=None):
-    """(q, p) from the learned encoder, or None when no model applies (none for K, or the cohort
-    has fewer SNPs than the sketch reaches): the caller then falls back to the random start + EM.
-    `model` is a WarmStartMLP, a path to one, or None for the shipped model of K."""
+def learned_start(g, K: int, model=None, info: dict | None = None):
+    """(q, p) from the learned encoder, or None when no model applies -- none for K, the cohort
+    has fewer SNPs than the sketch reaches, or its sketch-SNP allele frequencies do not match the
+    populations the model was trained on: the caller then falls back to the random start + EM.
+    `model` is a WarmStartMLP, a path to one, or None for the shipped model of K; `info` (a dict)
+    receives the reason for a fallback and the frequency correlation."""
+    if info is None:
+        info = {}
     if model is None:
         model = load_default(K)
     elif not isinstance(model, WarmStartMLP):
         model = WarmStartMLP.load(model)
-    if model is None or model.K != K or model.snps is None or int(model.snps.max()) >= g.J:
+    if model is None or model.K != K:
+        info["fallback"] = f"no model for K={K}"
         return None
-    return predict_start(model, g)
+    if model.snps is None or int(model.snps.max()) >= g.J:
+        info["fallback"] = f"the model's sketch reaches beyond the cohort's {g.J} SNPs"
+        return None
+    return predict_start(model, g, info=info, check=True)
 
 
 def run_to_target(g, K: int, *, flags: int = 0, start=None, em: int = 5, rtol: float = 1e-7, target=None,
