@@ -42,12 +42,29 @@ extern "C" {
 /* admix_create flags */
 #define ADMIX_FLAG_MU_GERSHGORIN  1u  /* simplex tableau adds the Gerschgorin mu of qp.jl:54-58
                                           (default: mu = 0, what the aliased mul! yields) */
+/* ADMIX_FLAG_MIXED is also what the host API maps the reference's T = Float32 to
+ * (run_admixture(...; T=Float32), AdmixData{Float32}): a deliberate change of meaning.  The
+ * reference then keeps every array and every sum in Float32; this engine keeps Q, P and the sums
+ * in FP64 and runs the mixed form, so a T = Float32 run here is more accurate than the
+ * reference's (it reaches the FP64 optimum) and returns Float32 copies of Q and P.  Callers who
+ * need the reference's Float32 rounding itself get no bit-for-bit reproduction of it. */
 #define ADMIX_FLAG_MIXED          2u  /* mixed-precision form: the iteration's Q/P gradient / Hessian
                                           sweeps (tcgen05 BF16 Hessians, FP32 gradient cells, FP64
                                           sums), its log-likelihoods (FP32 cells, FP64 reduction) and
                                           admix_init_em's EM sums; admix_loglik, admix_em_q/_p, the
                                           QPs and the QN step stay FP64.  A mixed call whose
                                           tensor-core pipeline wait runs out returns ADMIX_ERR_CUDA. */
+
+#define ADMIX_FLAG_MEAN_IMPUTE    4u  /* AdmixData(...; skipmissing=false) (structs.jl:105): the loops
+                                          that impute a missing genotype by its SNP's mean dosage g.mu
+                                          (loglikelihood_loop, em_q_loop!, em_p_loop!, update_q_loop!,
+                                          update_p_loop!; loops.jl:493-514,589-608,679-698,840-865,
+                                          896-921) instead of skipping it.  g.mu is computed once at
+                                          creation from the genotypes (mean over non-missing
+                                          individuals).  FP64 form of a device-resident handle only:
+                                          with ADMIX_FLAG_MIXED or admix_create_streamed the call
+                                          returns ADMIX_ERR_UNSUPPORTED (the reference's own GPU path
+                                          asserts skipmissing, algorithms_inner.jl:191,267). */
 
 #define ADMIX_MAX_K 16
 #define ADMIX_MAX_Q 8

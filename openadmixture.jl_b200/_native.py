@@ -22,6 +22,7 @@ ADMIX_ERR_STATE = 5
 ADMIX_X, ADMIX_X_NEXT, ADMIX_X_NEXT2, ADMIX_X_TMP = 0, 1, 2, 3
 ADMIX_FLAG_MU_GERSHGORIN = 1
 ADMIX_FLAG_MIXED = 2
+ADMIX_FLAG_MEAN_IMPUTE = 4
 ADMIX_MAX_K = 16
 ADMIX_MAX_Q = 8
 

@@ -39,11 +39,9 @@ class AdmixData:
     """
 
     def __init__(self, I: int, J: int, K: int, Q: int = 3, *, skipmissing: bool = True, rng: int = 0):
-        if not skipmissing:
-            raise NotImplementedError("skipmissing=False (mean imputation) is not part of the GPU path "
-                                      "(the reference's GPU path asserts skipmissing, algorithms_inner.jl:191)")
         self.I, self.J, self.K, self.Q = int(I), int(J), int(K), int(Q)
-        self.skipmissing = True
+        # skipmissing=False: the mean-imputed loops (ADMIX_FLAG_MEAN_IMPUTE on the handle)
+        self.skipmissing = bool(skipmissing)
         self.x = init_x(self.I, self.J, self.K, int(rng))
         self.x_next = np.zeros_like(self.x)
         self.x_next2 = np.zeros_like(self.x)
@@ -80,6 +78,8 @@ class CuAdmixData:
         blocks of that many SNPs (a multiple of 32) -- for cohorts larger than device memory."""
         if (g.I, g.J) != (d.I, d.J):
             raise ValueError(f"genotypes are {g.I} x {g.J}, AdmixData is {d.I} x {d.J}")
+        if not d.skipmissing:      # AdmixData(...; skipmissing=false): the mean-imputed loops
+            flags |= N.ADMIX_FLAG_MEAN_IMPUTE
         lib = N.admix_lib()
         h = C.c_void_p()
         self._host_bed = None

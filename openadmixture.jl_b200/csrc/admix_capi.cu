@@ -47,6 +47,7 @@ struct admix_ctx {
     double *U = nullptr, *V = nullptr, *vt = nullptr;
     int32_t *status_q = nullptr, *status_p = nullptr;
     uint8_t *pkg = nullptr;          /* mixed sweeps: per-chunk packages of the fixed block */
+    double *mu = nullptr;            /* ADMIX_FLAG_MEAN_IMPUTE: the SNP means g.mu (J) */
     double *ll_partial = nullptr, *qn_partial = nullptr;
     DevScalars *sc = nullptr;
     DevScalars *sc_host = nullptr;   /* pinned mirror */
@@ -135,7 +136,7 @@ static void release(admix_ctx *h)
     if (h->cst) { cudaStreamSynchronize(h->cst); cudaStreamDestroy(h->cst); }
     if (h->host_registered) cudaHostUnregister((void *)h->host_bed);
     void *dps[] = {h->pkg, h->xbuf, h->parts_q, h->parts_p, h->U, h->V, h->vt, h->status_q,
-                   h->status_p, h->ll_partial, h->qn_partial, h->sc, h->counts};
+                   h->status_p, h->ll_partial, h->qn_partial, h->sc, h->counts, h->mu};
     for (void *p : dps)
         if (p) cudaFree(p);
     if (h->sc_host) cudaFreeHost(h->sc_host);
@@ -174,8 +175,11 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     if (K < 1 || K > ADMIX_MAX_K) return fail(nullptr, ADMIX_ERR_UNSUPPORTED, "K=%d outside [1, %d]", K, ADMIX_MAX_K);
     if (Q < 1 || Q > ADMIX_MAX_Q) return fail(nullptr, ADMIX_ERR_UNSUPPORTED, "Q=%d outside [1, %d]", Q, ADMIX_MAX_Q);
     if (!bed) return fail(nullptr, ADMIX_ERR_ARG, "bed is NULL");
-    if (flags & ~(ADMIX_FLAG_MU_GERSHGORIN | ADMIX_FLAG_MIXED))
+    if (flags & ~(ADMIX_FLAG_MU_GERSHGORIN | ADMIX_FLAG_MIXED | ADMIX_FLAG_MEAN_IMPUTE))
         return fail(nullptr, ADMIX_ERR_ARG, "unknown flags 0x%x", flags);
+    if ((flags & ADMIX_FLAG_MEAN_IMPUTE) && ((flags & ADMIX_FLAG_MIXED) || stream_blk > 0))
+        return fail(nullptr, ADMIX_ERR_UNSUPPORTED, "the mean-imputed loops run in the FP64 form of a device-resident "
+                    "handle only (not with ADMIX_FLAG_MIXED or a streamed handle)");
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
     if (ce != cudaSuccess || ndev == 0)
@@ -262,6 +266,10 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     TRYC(cudaMallocHost((void **)&h->iter_host, sizeof(int32_t)));
 
     if (!shared_bed && !h->streamed) TRYC(upload_genotypes(h->bed, h->pitch, bed, src_pitch, I, J, on_device, h->sms, h->st));
+    if (flags & ADMIX_FLAG_MEAN_IMPUTE) {
+        TRY(dalloc(h, &h->mu, (size_t)J));
+        TRYC(launch_snp_means(h->bed, J, h->pitch, h->mu, h->st));
+    }
     TRYC(cudaMemsetAsync(h->xbuf, 0, sizeof(double) * 4 * nx, h->st));
     TRYC(cudaMemsetAsync(h->U, 0, sizeof(double) * nx * Q, h->st));
     TRYC(cudaMemsetAsync(h->V, 0, sizeof(double) * nx * Q, h->st));
@@ -417,7 +425,7 @@ static cudaError_t enq_loglik(admix_ctx *h, int which, double *dst, bool fast = 
                                        &h->sc->tc_err, h->pkg, h->st);
         }
         const LoglikPlan pl = h->streamed ? plan_loglik(h->I, nj, h->sms) : h->llp;
-        return launch_loglik_f64(h->K, bed, h->I, nj, h->pitch, Qof(h, which), P, pl, h->ll_partial, o, h->st);
+        return launch_loglik_f64(h->K, bed, h->I, nj, h->pitch, Qof(h, which), P, pl, h->ll_partial, o, h->st, h->mu);
     };
     cudaError_t e = for_blocks(h, one);
     if (e == cudaSuccess && h->streamed) e = launch_sum_doubles(h->ll_blk, h->nblk, dst, h->st);
@@ -441,7 +449,7 @@ static cudaError_t enq_sweep_q_mode(admix_ctx *h, int mode, int wq, int wp, int 
                                         h->pkg, h->st);
         }
         const SweepPlan pl = h->streamed ? block_plan(h->sq, nj) : h->sq;
-        return launch_sweep_q_f64(h->K, mode, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, h->st);
+        return launch_sweep_q_f64(h->K, mode, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, h->st, h->mu);
     });
 }
 
@@ -465,7 +473,7 @@ static cudaError_t enq_sweep_p_mode(admix_ctx *h, int mode, int wq, int wp, int 
                                         &h->sc->tc_err, h->pkg, h->st);
         }
         const SweepPlan pl = h->streamed ? block_plan(plan_sweep_p(h->K, h->I, nj, h->sms), (h->I + 3) / 4 * 4) : h->sp;
-        return launch_sweep_p_f64(h->K, mode, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, h->st);
+        return launch_sweep_p_f64(h->K, mode, bed, h->I, nj, h->pitch, Qof(h, wq), P, pl, out, h->st, h->mu);
     });
 }
 
@@ -1085,7 +1093,8 @@ static int batch_create_common(int64_t I, int64_t J, const uint8_t *bed, bool on
         if (Ks[t] < 1 || Ks[t] > ADMIX_MAX_K)
             return bfail(nullptr, ADMIX_ERR_UNSUPPORTED, "member %d: K=%d outside [1, %d]", t, Ks[t], ADMIX_MAX_K);
     if (Q < 1 || Q > ADMIX_MAX_Q) return bfail(nullptr, ADMIX_ERR_UNSUPPORTED, "Q=%d outside [1, %d]", Q, ADMIX_MAX_Q);
-    if (flags & ~(ADMIX_FLAG_MU_GERSHGORIN | ADMIX_FLAG_MIXED)) return bfail(nullptr, ADMIX_ERR_ARG, "unknown flags 0x%x", flags);
+    if (flags & ~(ADMIX_FLAG_MU_GERSHGORIN | ADMIX_FLAG_MIXED | ADMIX_FLAG_MEAN_IMPUTE))
+        return bfail(nullptr, ADMIX_ERR_ARG, "unknown flags 0x%x", flags);
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
     if (ce != cudaSuccess || ndev == 0) return bfail(nullptr, ADMIX_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(ce));

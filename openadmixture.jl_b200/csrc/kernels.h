@@ -16,15 +16,18 @@ SweepPlan plan_sweep_p(int K, int64_t I, int64_t J, int sms);
 
 /* FP64 sweeps (sweeps_f64.cu) */
 cudaError_t prepare_sweeps(int K);
+/* mu (J doubles, the SNP means) != nullptr selects the reference's non-skipmissing loops */
 cudaError_t launch_loglik_f64(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                               const double *p, const LoglikPlan &pl, double *partial, double *out,
-                              cudaStream_t st);
+                              cudaStream_t st, const double *mu = nullptr);
 cudaError_t launch_sweep_q_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                const double *q, const double *p, const SweepPlan &pl, double *out,
-                               cudaStream_t st);
+                               cudaStream_t st, const double *mu = nullptr);
 cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                const double *q, const double *p, const SweepPlan &pl, double *out,
-                               cudaStream_t st);
+                               cudaStream_t st, const double *mu = nullptr);
+/* g.mu of the SnpLinAlg: mean non-missing dosage per SNP of the padded device genotypes */
+cudaError_t launch_snp_means(const uint8_t *bed, int64_t J, int64_t pitch, double *mu, cudaStream_t st);
 /* fixed-order FP64 sum of n doubles into *dst (one block) */
 cudaError_t launch_sum_doubles(const double *src, int64_t n, double *dst, cudaStream_t st);
 cudaError_t launch_emq_finalize(int64_t I, int K, int64_t J, int S, const double *parts,

@@ -14,7 +14,9 @@
 /* ===================================================================== loglik */
 
 /* loglikelihood_kernel (cuda/kernels.jl:2-32) / loglikelihood_loop_skipmissing
- * (loops.jl:517-539).  Thread = one genotype byte (4 individuals) of a column range;
+ * (loops.jl:517-539); with mu != NULL the non-skipmissing loglikelihood_loop (loops.jl:493-514),
+ * whose missing cells count with the SNP's mean dosage mu_j.  Thread = one genotype byte (4
+ * individuals) of a column range;
  * q of its 4 individuals lives in registers, p of a 64-SNP chunk in shared memory.
  * Each cell adds nm * log(qp^g (1-qp)^(2-g)): one log per cell instead of two (equal to
  * the reference's g log qp + (2-g) log(1-qp) up to rounding). */
@@ -22,7 +24,7 @@ template <int K>
 __global__ void __launch_bounds__(256)
 k_loglik_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib, int64_t pitch,
              const double *__restrict__ q, const double *__restrict__ p,
-             int64_t jslice, double *__restrict__ partial)
+             int64_t jslice, double *__restrict__ partial, const double *__restrict__ mu)
 {
     constexpr int JC = 64;
     __shared__ double ps[JC * K];
@@ -56,9 +58,15 @@ k_loglik_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t Ib, 
 #pragma unroll
                     for (int k = 0; k < K; ++k) qp = fma(qr[s][k], ps[jj * K + k], qp);
                     const double om = 1.0 - qp;
-                    const double arg = (c == 3) ? qp * qp : ((c == 2) ? qp * om : om * om);
-                    const double v = log(arg);
-                    acc += (valid[s] && c != 1) ? v : 0.0;
+                    double v = 0.0;
+                    if (c != 1) {
+                        const double arg = (c == 3) ? qp * qp : ((c == 2) ? qp * om : om * om);
+                        v = log(arg);
+                    } else if (mu) {   /* loglikelihood_loop: the missing dosage imputed by mu_j */
+                        const double gm = __ldg(mu + jc + jj);
+                        v = gm * log(qp) + (2.0 - gm) * log(om);
+                    }
+                    acc += valid[s] ? v : 0.0;
                 }
             }
         }
@@ -80,7 +88,11 @@ k_sum_partials(const double *__restrict__ partial, int64_t n, double *__restrict
 
 /* ===================================================================== Q side */
 
-/* Per-individual accumulators over SNPs j.  MODE 0 (update_q_loop_skipmissing!,
+/* With mu != NULL every kernel below runs the reference's non-skipmissing twin (update_q_loop!,
+ * em_q_loop!, update_p_loop!, em_p_loop!, loops.jl:589-608,679-698,840-865,896-921): a missing
+ * cell counts with g = mu_j, the SNP's mean dosage, and weight 1.
+ *
+ * Per-individual accumulators over SNPs j.  MODE 0 (update_q_loop_skipmissing!,
  * loops.jl:867-894; update_q_kernel!, cuda/kernels.jl:102-137): entries e < T are the
  * packed upper triangle of XtX_q (T = K(K+1)/2), entries T..T+K-1 are Xtz_q.
  * MODE 1 (em_q_loop_skipmissing!, loops.jl:610-632): E = K entries sum_j (z1 p_k + z2 (1-p_k)),
@@ -105,7 +117,7 @@ template <int K, int MODE>
 __global__ void __launch_bounds__(128)
 k_sweep_q_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
               const double *__restrict__ q, const double *__restrict__ p,
-              int64_t jslice, double *__restrict__ out)
+              int64_t jslice, double *__restrict__ out, const double *__restrict__ mu)
 {
     using C = QSide<K, MODE>;
     constexpr int T = C::T, E = C::E, NS = C::NS, L = C::L, JC = C::JC;
@@ -154,8 +166,9 @@ k_sweep_q_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pit
             double qp = 0.0;
 #pragma unroll
             for (int k = 0; k < K; ++k) qp = fma(qi[k], P[jj * K + k], qp);
-            const double g = gval(c);
-            const bool nm = (c != 1);
+            double g = gval(c);
+            bool nm = (c != 1);
+            if (!nm && mu && valid) { g = __ldg(mu + jc + jj); nm = true; }   /* mean-imputed loops */
             const double r1 = 1.0 / qp, r2 = 1.0 / (1.0 - qp);
             const double z1 = (nm && g != 0.0) ? g * r1 : 0.0;
             const double z2 = (nm && g != 2.0) ? (2.0 - g) * r2 : 0.0;
@@ -223,7 +236,7 @@ template <int K, int MODE>
 __global__ void __launch_bounds__(128)
 k_sweep_p_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
               const double *__restrict__ q, const double *__restrict__ p,
-              int64_t islice, double *__restrict__ out)
+              int64_t islice, double *__restrict__ out, const double *__restrict__ mu)
 {
     using C = PSide<K, MODE>;
     constexpr int T = C::T, E = C::E, NS = C::NS, L = C::L, IC = C::IC;
@@ -237,6 +250,7 @@ k_sweep_p_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pit
     double pj[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) pj[k] = valid ? p[(size_t)K * j + k] : 0.5;
+    const double muj = (mu && valid) ? mu[j] : 0.0;
     double acc[L];
 #pragma unroll
     for (int l = 0; l < L; ++l) acc[l] = 0.0;
@@ -269,8 +283,9 @@ k_sweep_p_f64(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pit
                 double qp = 0.0;
 #pragma unroll
                 for (int k = 0; k < K; ++k) qp = fma(qq[k], pj[k], qp);
-                const double g = gval(c);
-                const bool nm = (c != 1);
+                double g = gval(c);
+                bool nm = (c != 1);
+                if (!nm && mu && valid) { g = muj; nm = true; }   /* mean-imputed loops */
                 const double r1 = 1.0 / qp, r2 = 1.0 / (1.0 - qp);
                 const double z1 = (nm && g != 0.0) ? g * r1 : 0.0;
                 const double z2 = (nm && g != 2.0) ? (2.0 - g) * r2 : 0.0;
@@ -379,16 +394,47 @@ k_decode_counts(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t I
         }
 }
 
+/* ===================================================================== SNP means */
+
+/* g.mu of the SnpLinAlg (additive model): per SNP the mean dosage over its non-missing
+ * individuals, NaN when all are missing.  One block per SNP over its padded column (padding is
+ * coded missing, so it never counts).  Per byte: codes 10 and 11 have the high bit, 11 also the
+ * low bit, so sum g = popc(hi) + popc(hi & lo) and the missing count is popc(lo & ~hi). */
+__global__ void __launch_bounds__(256)
+k_snp_means(const uint8_t *__restrict__ bed, int64_t J, int64_t pitch, double *__restrict__ mu)
+{
+    __shared__ double red[8];
+    const int64_t j = blockIdx.x;
+    if (j >= J) return;
+    const uint8_t *col = bed + (size_t)j * pitch;
+    long long gs = 0, nn = 0;
+    for (int64_t b = threadIdx.x; b < pitch; b += blockDim.x) {
+        const unsigned v = col[b];
+        const unsigned lo = v & 0x55u, hi = (v >> 1) & 0x55u;
+        gs += __popc(hi) + __popc(hi & lo);
+        nn += 4 - __popc(lo & ~hi);
+    }
+    const double sg = block_sum((double)gs, red);
+    const double sn = block_sum((double)nn, red);
+    if (threadIdx.x == 0) mu[j] = sn > 0.0 ? sg / sn : __longlong_as_double(0x7ff8000000000000LL);
+}
+
+cudaError_t launch_snp_means(const uint8_t *bed, int64_t J, int64_t pitch, double *mu, cudaStream_t st)
+{
+    k_snp_means<<<(unsigned)J, 256, 0, st>>>(bed, J, pitch, mu);
+    return cudaGetLastError();
+}
+
 /* ===================================================================== launchers */
 
 template <int K>
 static cudaError_t launch_loglik_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                                    const double *p, const LoglikPlan &pl, double *partial, double *out,
-                                   cudaStream_t st)
+                                   cudaStream_t st, const double *mu)
 {
     const int64_t Ib = (I + 3) / 4;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.gy);
-    k_loglik_f64<K><<<grid, 256, 0, st>>>(bed, I, J, Ib, pitch, q, p, pl.jslice, partial);
+    k_loglik_f64<K><<<grid, 256, 0, st>>>(bed, I, J, Ib, pitch, q, p, pl.jslice, partial, mu);
     k_sum_partials<<<1, 1024, 0, st>>>(partial, (int64_t)pl.gx * pl.gy, out);
     return cudaGetLastError();
 }
@@ -409,10 +455,10 @@ LoglikPlan plan_loglik(int64_t I, int64_t J, int sms)
 
 cudaError_t launch_loglik_f64(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
                               const double *p, const LoglikPlan &pl, double *partial, double *out,
-                              cudaStream_t st)
+                              cudaStream_t st, const double *mu)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    ADMIX_DISPATCH_K(K, e = launch_loglik_t<KK>(bed, I, J, pitch, q, p, pl, partial, out, st));
+    ADMIX_DISPATCH_K(K, e = launch_loglik_t<KK>(bed, I, J, pitch, q, p, pl, partial, out, st, mu));
     return e;
 }
 
@@ -448,41 +494,43 @@ SweepPlan plan_sweep_p(int K, int64_t I, int64_t J, int sms)
 
 template <int K, int MODE>
 static cudaError_t launch_sweep_q_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                                    const double *p, const SweepPlan &pl, double *out, cudaStream_t st)
+                                    const double *p, const SweepPlan &pl, double *out, cudaStream_t st,
+                                    const double *mu)
 {
     using C = QSide<K, MODE>;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_q_f64<K, MODE><<<grid, 128, C::smem, st>>>(bed, I, J, pitch, q, p, pl.slice, out);
+    k_sweep_q_f64<K, MODE><<<grid, 128, C::smem, st>>>(bed, I, J, pitch, q, p, pl.slice, out, mu);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sweep_q_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                const double *q, const double *p, const SweepPlan &pl, double *out,
-                               cudaStream_t st)
+                               cudaStream_t st, const double *mu)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    if (mode == 0) { ADMIX_DISPATCH_K(K, (e = launch_sweep_q_t<KK, 0>(bed, I, J, pitch, q, p, pl, out, st))); }
-    else { ADMIX_DISPATCH_K(K, (e = launch_sweep_q_t<KK, 1>(bed, I, J, pitch, q, p, pl, out, st))); }
+    if (mode == 0) { ADMIX_DISPATCH_K(K, (e = launch_sweep_q_t<KK, 0>(bed, I, J, pitch, q, p, pl, out, st, mu))); }
+    else { ADMIX_DISPATCH_K(K, (e = launch_sweep_q_t<KK, 1>(bed, I, J, pitch, q, p, pl, out, st, mu))); }
     return e;
 }
 
 template <int K, int MODE>
 static cudaError_t launch_sweep_p_t(const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
-                                    const double *p, const SweepPlan &pl, double *out, cudaStream_t st)
+                                    const double *p, const SweepPlan &pl, double *out, cudaStream_t st,
+                                    const double *mu)
 {
     using C = PSide<K, MODE>;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_sweep_p_f64<K, MODE><<<grid, 128, C::smem, st>>>(bed, I, J, pitch, q, p, pl.slice, out);
+    k_sweep_p_f64<K, MODE><<<grid, 128, C::smem, st>>>(bed, I, J, pitch, q, p, pl.slice, out, mu);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch,
                                const double *q, const double *p, const SweepPlan &pl, double *out,
-                               cudaStream_t st)
+                               cudaStream_t st, const double *mu)
 {
     cudaError_t e = cudaErrorInvalidValue;
-    if (mode == 0) { ADMIX_DISPATCH_K(K, (e = launch_sweep_p_t<KK, 0>(bed, I, J, pitch, q, p, pl, out, st))); }
-    else { ADMIX_DISPATCH_K(K, (e = launch_sweep_p_t<KK, 1>(bed, I, J, pitch, q, p, pl, out, st))); }
+    if (mode == 0) { ADMIX_DISPATCH_K(K, (e = launch_sweep_p_t<KK, 0>(bed, I, J, pitch, q, p, pl, out, st, mu))); }
+    else { ADMIX_DISPATCH_K(K, (e = launch_sweep_p_t<KK, 1>(bed, I, J, pitch, q, p, pl, out, st, mu))); }
     return e;
 }
 

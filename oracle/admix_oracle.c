@@ -36,6 +36,40 @@
 static const double G_MAP[4]  = {0.0, 0.0, 1.0, 2.0};
 static const double NM_MAP[4] = {1.0, 0.0, 1.0, 1.0};
 
+/* The non-skipmissing loops (AdmixData(...; skipmissing=false): loglikelihood_loop,
+ * em_q_loop!, em_p_loop!, update_q_loop!, update_p_loop!, loops.jl:365-383,493-514,589-608,
+ * 679-698,840-865,896-921) use gij = g_map[code] + (code == 01) mu_j -- the missing genotype
+ * imputed by the SNP's mean dosage g.mu[j] of the SnpLinAlg -- and no non-missing factor.
+ * g_mu = NULL selects the skipmissing loops (the driver's choice, driver.jl:149). */
+static const double *g_mu = NULL;
+
+void orc_set_mean_impute(const double *mu) { g_mu = mu; }
+
+/* g.mu of a SnpLinAlg with the additive model: the mean dosage over the non-missing
+ * individuals of each SNP (NaN when every genotype is missing, the mean of nothing). */
+void orc_snp_means(const uint8_t *bed, int64_t I, int64_t J, double *mu)
+{
+    const int64_t Ib = (I + 3) / 4;
+    #pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < J; ++j) {
+        double s = 0.0;
+        int64_t n = 0;
+        for (int64_t i = 0; i < I; ++i) {
+            const uint8_t blk = bed[j * Ib + (i >> 2)];
+            const int c = (blk >> ((i & 3) << 1)) & 3;
+            if (c != 1) { s += G_MAP[c]; ++n; }
+        }
+        mu[j] = n > 0 ? s / (double)n : NAN;
+    }
+}
+
+/* genotype value and non-missing weight of a cell (both loop families) */
+static inline void cell_gnm(int c, int64_t j, double *g, double *nm)
+{
+    if (g_mu) { *g = G_MAP[c] + (c == 1 ? g_mu[j] : 0.0); *nm = 1.0; }
+    else { *g = G_MAP[c]; *nm = NM_MAP[c]; }
+}
+
 static inline int code_at(const uint8_t *bed, int64_t Ib, int64_t i, int64_t j)
 {
     /* loops.jl:529-532: blk = gmat[(i-1)>>2+1, j]; re = (i-1)%4; (blk >> (re<<1)) & 3 */
@@ -88,7 +122,8 @@ static double loglik_tile(const uint8_t *bed, int64_t Ib, const double *q, const
         const double *pj = p + (size_t)K * j;
         for (int64_t i = i0; i < i1; ++i) {
             int c = code_at(bed, Ib, i, j);
-            double g = G_MAP[c], nm = NM_MAP[c];
+            double g, nm;
+            cell_gnm(c, j, &g, &nm);
             double qp = qp_cell(q + (size_t)K * i, pj, K);
             r += nm * ((g * log(qp)) + ((2.0 - g) * log(1.0 - qp)));
         }
@@ -184,7 +219,8 @@ void orc_em_q(const uint8_t *bed, int64_t I, int64_t J, int K,
         for (int64_t j = 0; j < J; ++j) {
             const double *pj = p + (size_t)K * j;
             int c = code_at(bed, Ib, i, j);
-            double g = G_MAP[c], nm = NM_MAP[c];
+            double g, nm;
+            cell_gnm(c, j, &g, &nm);
             double qp = qp_cell(qi, pj, K);
             for (int k = 0; k < K; ++k) {
                 double tmp = (g * qi[k] * pj[k] / qp + (2.0 - g) * qi[k] * (1.0 - pj[k]) / (1.0 - qp));
@@ -212,7 +248,8 @@ void orc_em_p(const uint8_t *bed, int64_t I, int64_t J, int K,
             for (int64_t i = 0; i < I; ++i) {
                 const double *qi = q + (size_t)K * i;
                 int c = code_at(bed, Ib, i, j);
-                double g = G_MAP[c], nm = NM_MAP[c];
+                double g, nm;
+                cell_gnm(c, j, &g, &nm);
                 double qp = qp_cell(qi, pj, K);
                 for (int k = 0; k < K; ++k) {
                     A[k] += nm * (g * qi[k] * pj[k] / qp);
@@ -243,7 +280,8 @@ void orc_grad_hess_q(const uint8_t *bed, int64_t I, int64_t J, int K,
         for (int64_t j = 0; j < J; ++j) {
             const double *pj = p + (size_t)K * j;
             int c = code_at(bed, Ib, i, j);
-            double g = G_MAP[c], nm = NM_MAP[c];
+            double g, nm;
+            cell_gnm(c, j, &g, &nm);
             double qp = qp_cell(qi, pj, K);
             double oq = 1.0 - qp;
             for (int k = 0; k < K; ++k) {
@@ -271,7 +309,8 @@ void orc_grad_hess_p(const uint8_t *bed, int64_t I, int64_t J, int K,
         for (int64_t i = 0; i < I; ++i) {
             const double *qi = q + (size_t)K * i;
             int c = code_at(bed, Ib, i, j);
-            double g = G_MAP[c], nm = NM_MAP[c];
+            double g, nm;
+            cell_gnm(c, j, &g, &nm);
             double qp = qp_cell(qi, pj, K);
             double oq = 1.0 - qp;
             for (int k = 0; k < K; ++k) {

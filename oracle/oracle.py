@@ -76,6 +76,8 @@ def lib() -> C.CDLL:
             "orc_qn_iteration": (C.c_int, [C.POINTER(OrcState), C.c_int, C.c_double, _D, _I32, _I32]),
             "orc_admixture_qn": (C.c_int, [C.POINTER(OrcState), C.c_int, C.c_double, C.c_int, _D, C.POINTER(C.c_int)]),
             "orc_num_threads": (C.c_int, []),
+            "orc_set_mean_impute": (None, [_D]),
+            "orc_snp_means": (None, [_U8, C.c_int64, C.c_int64, _D]),
         }
         for fn, (res, args) in sig.items():
             f = getattr(L, fn)
@@ -101,32 +103,64 @@ def _u8(a):
 # Arrays follow the numpy mirror of Julia's column-major layout: q is (I, K), p is (J, K),
 # XtX_q is (I, K, K) with XtX[i, k, k2] = Julia XtX_q[k2, k, i].
 
+class _impute:
+    """Selects the non-skipmissing (mean-imputed) loops for the calls inside the block when mu
+    (the SNP means, length J) is given; the skipmissing loops otherwise."""
+
+    def __init__(self, mu):
+        self.mu = None if mu is None else np.ascontiguousarray(mu, dtype=np.float64)
+
+    def __enter__(self):
+        lib().orc_set_mean_impute(_d(self.mu) if self.mu is not None else None)
+
+    def __exit__(self, *a):
+        lib().orc_set_mean_impute(None)
+
+
+def snp_means(bed: np.ndarray, I: int, J: int) -> np.ndarray:
+    """g.mu of the SnpLinAlg (additive model): mean dosage over the non-missing individuals."""
+    mu = np.empty(J)
+    lib().orc_snp_means(_u8(bed), I, J, _d(mu))
+    return mu
+
+
 def decode_counts(bed: np.ndarray, I: int, J: int):
     snp = np.zeros(J, np.int64); ind = np.zeros(I, np.int64)
     lib().orc_decode_counts(_u8(bed), I, J, snp.ctypes.data_as(_I64), ind.ctypes.data_as(_I64))
     return snp, ind
 
 
-def loglik(bed, I, J, K, q, p) -> float:
-    return lib().orc_loglik(_u8(bed), I, J, K, _d(q), _d(p))
+def loglik(bed, I, J, K, q, p, mu=None) -> float:
+    with _impute(mu):
+        return lib().orc_loglik(_u8(bed), I, J, K, _d(q), _d(p))
 
 
-def em_q(bed, I, J, K, q, p):
-    out = np.empty((I, K)); lib().orc_em_q(_u8(bed), I, J, K, _d(q), _d(p), _d(out)); return out
+def em_q(bed, I, J, K, q, p, mu=None):
+    out = np.empty((I, K))
+    with _impute(mu):
+        lib().orc_em_q(_u8(bed), I, J, K, _d(q), _d(p), _d(out))
+    return out
 
 
-def em_p(bed, I, J, K, q, p):
-    out = np.empty((J, K)); lib().orc_em_p(_u8(bed), I, J, K, _d(q), _d(p), _d(out)); return out
+def em_p(bed, I, J, K, q, p, mu=None):
+    out = np.empty((J, K))
+    with _impute(mu):
+        lib().orc_em_p(_u8(bed), I, J, K, _d(q), _d(p), _d(out))
+    return out
 
 
-def grad_hess_q(bed, I, J, K, q, p):
+def grad_hess_q(bed, I, J, K, q, p, mu=None):
     H = np.empty((I, K, K)); z = np.empty((I, K))
-    lib().orc_grad_hess_q(_u8(bed), I, J, K, _d(q), _d(p), _d(H), _d(z)); return H, z
+    with _impute(mu):
+        lib().orc_grad_hess_q(_u8(bed), I, J, K, _d(q), _d(p), _d(H), _d(z))
+    return H, z
 
 
-def grad_hess_p(bed, I, J, K, q, p):
+def grad_hess_p(bed, I, J, K, q, p, mu=None):
     H = np.empty((J, K, K)); z = np.empty((J, K))
-    lib().orc_grad_hess_p(_u8(bed), I, J, K, _d(q), _d(p), _d(H), _d(z)); return H, z
+    with _impute(mu):
+        lib().orc_grad_hess_p(_u8(bed), I, J, K, _d(q), _d(p), _d(H), _d(z))
+    return H, z
 
 
 def vt_ones(K: int) -> np.ndarray:
@@ -186,7 +220,8 @@ class OracleRun:
     """Oracle mirror of AdmixData + the outer loop (structs.jl, algorithms_outer.jl)."""
 
     def __init__(self, bed: np.ndarray, I: int, J: int, K: int, Q: int, x0: np.ndarray,
-                 mu_mode: int = MU_AS_EXECUTED, fix_q: bool = False, fix_p: bool = False, mode: str = "ZAL"):
+                 mu_mode: int = MU_AS_EXECUTED, fix_q: bool = False, fix_p: bool = False, mode: str = "ZAL",
+                 skipmissing: bool = True):
         self.bed = np.ascontiguousarray(bed)
         self.I, self.J, self.K, self.Q = I, J, K, Q
         n = I + J
@@ -208,6 +243,8 @@ class OracleRun:
         if mode not in ("ZAL", "LBQN"):
             raise ValueError(f"Invalid mode {mode!r}")
         s.mode = 1 if mode == "LBQN" else 0
+        # AdmixData(...; skipmissing=false): the mean-imputed loops with the SNP means g.mu
+        self.mu = None if skipmissing else snp_means(self.bed, I, J)
         self.x_q = np.zeros(n * K); self.x_r = np.zeros(n * K)
         s.x_q, s.x_r = _d(self.x_q), _d(self.x_r)
         self.s = s
@@ -222,33 +259,39 @@ class OracleRun:
 
     def loglik(self, x: np.ndarray) -> float:
         x = np.ascontiguousarray(x)
-        return lib().orc_loglik_x(C.byref(self.s), _d(x))
+        with _impute(self.mu):
+            return lib().orc_loglik_x(C.byref(self.s), _d(x))
 
     def init_em(self, iters: int) -> list[float]:
         hist = np.empty(max(iters, 1))
-        lib().orc_init_em(C.byref(self.s), iters, _d(hist))
+        with _impute(self.mu):
+            lib().orc_init_em(C.byref(self.s), iters, _d(hist))
         return list(hist[:iters])
 
     def update_q(self, update2: bool) -> np.ndarray:
         st = np.empty(self.I, np.int32)
-        lib().orc_update_q(C.byref(self.s), int(update2), st.ctypes.data_as(_I32))
+        with _impute(self.mu):
+            lib().orc_update_q(C.byref(self.s), int(update2), st.ctypes.data_as(_I32))
         return st
 
     def update_p(self, update2: bool) -> np.ndarray:
         st = np.empty(self.J, np.int32)
-        lib().orc_update_p(C.byref(self.s), int(update2), st.ctypes.data_as(_I32))
+        with _impute(self.mu):
+            lib().orc_update_p(C.byref(self.s), int(update2), st.ctypes.data_as(_I32))
         return st
 
     def qn_iteration(self, it: int, rtol: float = 1e-7) -> dict:
         info = np.empty(5)
-        stop = lib().orc_qn_iteration(C.byref(self.s), it, rtol, _d(info), None, None)
+        with _impute(self.mu):
+            stop = lib().orc_qn_iteration(C.byref(self.s), it, rtol, _d(info), None, None)
         return dict(ll_prev=info[0], ll_basic=info[1], ll_qn=info[2], ll_new=info[3], reldiff=info[4],
                     stop=bool(stop))
 
     def admixture_qn(self, n_iter: int = 1000, rtol: float = 1e-7, iter_offset: int = 0):
         hist = np.empty((max(n_iter, 1), 5))
         conv = C.c_int(0)
-        n = lib().orc_admixture_qn(C.byref(self.s), n_iter, rtol, iter_offset, _d(hist), C.byref(conv))
+        with _impute(self.mu):
+            n = lib().orc_admixture_qn(C.byref(self.s), n_iter, rtol, iter_offset, _d(hist), C.byref(conv))
         return hist[:n], bool(conv.value)
 
 

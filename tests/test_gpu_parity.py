@@ -418,3 +418,45 @@ def test_run_admixture_streamed(oa, flags):
     d0, _, _ = oa.run_admixture(g, 3, rng=5, quiet=True)
     d1, _, _ = oa.run_admixture(g, 3, rng=5, quiet=True, stream_block=512, flags=flags)
     assert rel_err(d1.ll_new, d0.ll_new) < (1e-9 if flags == 0 else 1e-6)
+
+
+@pytest.mark.parametrize("K", [2, 5, 12])
+def test_mean_imputed_loops_match_oracle(oa, orc, K):
+    """AdmixData(...; skipmissing=false) (ADMIX_FLAG_MEAN_IMPUTE): every pass of the FP64 form with
+    missing genotypes imputed by their SNP's mean dosage (loops.jl:493-514,589-608,679-698,
+    840-865,896-921) against the oracle's mean-imputed loops, then EM and QN iterations; the
+    flag is refused with the mixed form and with a streamed handle."""
+    g = _cohort(oa, I=411, J=1703, K=K, seed=150 + K, miss=0.05)
+    d = oa.AdmixData(g.I, g.J, K, 3, rng=K, skipmissing=False)
+    I, J = g.I, g.J
+    mu = orc.snp_means(g.data, I, J)
+    q, p = np.ascontiguousarray(d.x[:I]), np.ascontiguousarray(d.x[I:])
+    with oa.CuAdmixData(d, g) as h:
+        h.upload(oa.X, d.x)
+        assert rel_err(h.loglik(oa.X), orc.loglik(g.data, I, J, K, q, p, mu=mu)) < FP64_TOL
+        assert rel_err(h.loglik(oa.X), orc.loglik(g.data, I, J, K, q, p)) > 1e-6     # not the skipmissing value
+        H, z = h.grad_hess_q(oa.X, oa.X)
+        Ho, zo = orc.grad_hess_q(g.data, I, J, K, q, p, mu=mu)
+        assert _row_rel(H, Ho) < FP64_TOL and _row_rel(z, zo) < FP64_TOL
+        H, z = h.grad_hess_p(oa.X, oa.X)
+        Ho, zo = orc.grad_hess_p(g.data, I, J, K, q, p, mu=mu)
+        assert _row_rel(H, Ho) < FP64_TOL and _row_rel(z, zo) < FP64_TOL
+        oa.em_q(h); oa.em_p(h)
+        xn = h.download(oa.X_NEXT)
+        assert rel_err(xn[:I], orc.em_q(g.data, I, J, K, q, p, mu=mu)) < FP64_TOL
+        assert rel_err(xn[I:], orc.em_p(g.data, I, J, K, q, p, mu=mu)) < FP64_TOL
+        r = orc.OracleRun(g.data, I, J, K, 3, d.x, skipmissing=False)
+        ll_o = r.init_em(3)
+        ll_g = oa.init_em(d, g, 3, d_cu=h, quiet=True)
+        assert rel_err(np.array(ll_g), np.array(ll_o)) < 1e-9
+        d.x[:] = r.x
+        d.ll_new = r.ll_new
+        recs = oa.admixture_qn(d, g, 4, 0.0, d_cu=h, quiet=True)
+        for it, rec in enumerate(recs, start=1):
+            o = r.qn_iteration(it)
+            for k in ("ll_prev", "ll_basic", "ll_qn", "ll_new"):
+                assert rel_err(rec[k], o[k]) < 1e-8, (it, k, rec[k], o[k])
+    with pytest.raises(oa.AdmixError):
+        oa.CuAdmixData(d, g, flags=oa.ADMIX_FLAG_MIXED)
+    with pytest.raises(oa.AdmixError):
+        oa.CuAdmixData(d, g, stream_block=512)

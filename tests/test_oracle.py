@@ -346,3 +346,46 @@ def test_lbqn_step_matches_numpy_restatement_and_converges(oa, orc):
     rz.init_em(3)
     hz, cz = rz.admixture_qn(1000, 1e-7)
     assert cz and abs(r.ll_new - rz.ll_new) < 1e-6 * abs(rz.ll_new)
+
+
+def test_mean_imputed_loops(oa, orc):
+    """AdmixData(...; skipmissing=false): the missing genotype is the SNP's mean dosage g.mu[j]
+    (loops.jl:365-383,589-608,679-698,840-865,896-921).  Known answers: mu is the mean over the
+    non-missing genotypes; without missing genotypes the two loop families agree; the imputed
+    loglik equals the plain formula evaluated on the imputed dosage matrix; Xtz_p / XtX_p are its
+    first / negated second p-derivatives; EM stays monotone."""
+    g, x = _tiny(oa)
+    I, J, K = g.I, g.J, 3
+    q, p = _qp_split(x, I)
+    codes = np.stack([(g.data >> (2 * s)) & 3 for s in range(4)], axis=2).reshape(J, -1)[:, :I]
+    dose = np.where(codes == 3, 2.0, np.where(codes == 2, 1.0, 0.0))
+    nm = codes != 1
+    mu = orc.snp_means(g.data, I, J)
+    assert np.allclose(mu, (dose * nm).sum(1) / nm.sum(1), rtol=1e-14)
+    gi = np.where(nm, dose, mu[:, None])                      # (J, I) imputed dosages
+    qp = p @ q.T                                              # (J, I)
+    want = float(np.sum(gi * np.log(qp) + (2 - gi) * np.log(1 - qp)))
+    assert rel_err(orc.loglik(g.data, I, J, K, q, p, mu=mu), want) < 1e-11
+    full = g.data.copy()                                      # every missing code 01 replaced by 00
+    for s in range(4):
+        c = (full >> (2 * s)) & 3
+        full = np.where(c == 1, full & ~np.uint8(3 << (2 * s)), full).astype(np.uint8)
+    mu_f = orc.snp_means(full, I, J)
+    assert rel_err(orc.loglik(full, I, J, K, q, p, mu=mu_f), orc.loglik(full, I, J, K, q, p)) < 1e-13
+    H0, z0 = orc.grad_hess_q(full, I, J, K, q, p)
+    H1, z1 = orc.grad_hess_q(full, I, J, K, q, p, mu=mu_f)
+    assert np.array_equal(H0, H1) and np.array_equal(z0, z1)
+    p2 = np.clip(p, 0.1, 0.9)
+    H, z = orc.grad_hess_p(g.data, I, J, K, q, p2, mu=mu)
+    h = 1e-6
+    for j, k in [(0, 0), (5, 2), (40, 1)]:
+        pp, pm = p2.copy(), p2.copy()
+        pp[j, k] += h; pm[j, k] -= h
+        fd = (orc.loglik(g.data, I, J, K, q, pp, mu=mu) - orc.loglik(g.data, I, J, K, q, pm, mu=mu)) / (2 * h)
+        assert abs(fd - z[j, k]) < 1e-5 * max(1.0, abs(z[j, k]))
+        _, zp = orc.grad_hess_p(g.data, I, J, K, q, pp, mu=mu)
+        _, zm = orc.grad_hess_p(g.data, I, J, K, q, pm, mu=mu)
+        assert np.allclose(-(zp[j] - zm[j]) / (2 * h), H[j, :, k], rtol=1e-5, atol=1e-5)
+    r = orc.OracleRun(g.data, I, J, K, 3, x, skipmissing=False)
+    hist = [r.loglik(r.x)] + r.init_em(5)
+    assert all(b > a for a, b in zip(hist, hist[1:]))
