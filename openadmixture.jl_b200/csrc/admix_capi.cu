@@ -246,7 +246,8 @@ static int create_common(int64_t I, int64_t J, int32_t K, int32_t Q, const uint8
     TRY(dalloc(h, &h->vt, (size_t)K * K));
     TRY(dalloc(h, &h->status_q, (size_t)I));
     if (flags & ADMIX_FLAG_MIXED)
-        TRY(dalloc(h, &h->pkg, std::max(sweep_q_mixed_pkg_bytes(K, J), sweep_p_mixed_pkg_bytes(K, I))));
+        TRY(dalloc(h, &h->pkg, std::max({sweep_q_mixed_pkg_bytes(K, J), sweep_p_mixed_pkg_bytes(K, I),
+                                          loglik_mixed_pkg_bytes(K, I)})));
     TRY(dalloc(h, &h->status_p, (size_t)J));
     /* per-CTA log-likelihood partials: the resident plans, and for a streamed handle the plans of
      * a full block and of the last block (the mixed plan's count can grow as its SNP range shrinks) */

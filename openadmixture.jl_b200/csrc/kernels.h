@@ -58,6 +58,8 @@ cudaError_t launch_sweep_p_mixed(int K, int mode, const uint8_t *bed, int64_t I,
                                  const double *q, const double *p, const SweepPlan &pl, double *out, int *err,
                                  uint8_t *pkg, cudaStream_t st);
 size_t sweep_p_mixed_pkg_bytes(int K, int64_t I);
+/* The mixed log-likelihood first builds its per-chunk Q limb packages in pkg (this many bytes). */
+size_t loglik_mixed_pkg_bytes(int K, int64_t I);
 /* one CTA whose bounded wait on an mbarrier nothing completes runs out and sets *err */
 cudaError_t launch_wait_probe(int *err, uint32_t polls, cudaStream_t st);
 SweepPlan plan_loglik_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax = INT64_MAX);

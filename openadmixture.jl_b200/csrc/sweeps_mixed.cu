@@ -78,22 +78,46 @@ __device__ __forceinline__ uint4 interleave8(uint2 a, uint2 b)
 
 /* ===================================================================== Q side
  *
- * Per 32-SNP chunk, two tensor-core products:
+ * Per 32-SNP chunk, three tensor-core products:
  *   qp / om    D[128 x 64] = Qtile * [p ; 1-p]^T in TF32 split form (hi*hi + lo*hi + hi*lo, about
  *              2^-21 relative): the K-term dot products of every (individual, SNP) cell;
- *   Hessian    D[128 x N] += [w1 | w2] * [PP ; PbarPbar]^T in BF16 (FP32 accumulation);
- * and on the CUDA cores, per cell: the code lookup, one reciprocal, z1, z2, w1, w2 and the FP32
- * gradient sum_j (z1 - z2) p_k + z2 (= sum_j z1 p_k + z2 (1 - p_k)), added into FP64 per chunk.
+ *   Hessian    D[128 x N] += [w1 | w2] * [PP ; PbarPbar]^T in BF16 (FP32 accumulation), drained
+ *              into FP64 every MX_HBLOCK chunks;
+ *   diag/grad  D[128 x NDG] = [w1 | w2] * [p^2 ; (1-p)^2]^T (the Hessian diagonal) and
+ *              [dz_hi | dz_lo | dz_hi] * [p_hi ; p_hi ; p_lo]^T (the gradient sum_j dz p_k with
+ *              dz = z1 - z2 and both factors split into two BF16 parts, about 2^-17 relative), a
+ *              fresh FP32 sum every chunk that the producers add into FP64;
+ * and on the CUDA cores, per cell: the code lookup, one reciprocal, z1, z2, w1, w2, dz and its
+ * split, and sum_j z2 (FP32 per chunk, FP64 across chunks).  The gradient is
+ * sum_j (z1 - z2) p_k + z2 (= sum_j z1 p_k + z2 (1 - p_k)).
+ *
+ * The diagonal's per-chunk sum is the compensated correction of the BF16 Hessian: the tensor
+ * core's FP32 accumulation rounds toward zero, so a sum carried over many chunks drifts low
+ * (about 5e-5 relative over 256 chunks); restarted every chunk and carried in FP64, the
+ * diagonal drifts only by what one chunk's four accumulations lose.  The off-diagonal entries
+ * keep the MX_HBLOCK drains.
  *
  * Everything that depends on P alone -- the BF16 pair-product tiles, the TF32 hi / lo split of
- * [p ; 1-p] and p in FP32 -- is built once per sweep by k_q_pack, one "package" per chunk laid
- * out exactly as the sweep's shared memory wants it, and fetched by each CTA with one bulk
- * asynchronous copy (three package buffers in flight).  The qp MMA of chunk c+1 runs while the
- * CUDA cores work on chunk c. */
+ * [p ; 1-p], the diagonal and gradient B blocks -- is built once per sweep by k_q_pack, one
+ * "package" per chunk laid out exactly as the sweep's shared memory wants it, and fetched by
+ * each CTA with one bulk asynchronous copy.  The qp MMA of chunk c+1 runs while the CUDA cores
+ * work on chunk c. */
 
 constexpr int MQ_JC = 32;          /* SNPs per chunk = 2 BF16 MMA K-steps */
 constexpr int MQ_THREADS = 128;    /* one thread per individual = accumulator row */
-constexpr int MQ_NPKG = 3;         /* package buffers */
+#ifndef ADMIX_MQ_NPKG
+#define ADMIX_MQ_NPKG 2
+#endif
+constexpr int MQ_NPKG = ADMIX_MQ_NPKG;   /* package buffers */
+
+/* The [diagonal | gradient] accumulator of a chunk: N = NDG columns, the Hessian diagonal
+ * sum_j w1 p_k^2 + w2 (1-p_k)^2 in columns 0..K-1 and the gradient sum_j (z1 - z2) p_k in columns
+ * GOFF..GOFF+K-1.  It starts afresh every chunk and the producers add it into FP64, so no FP32
+ * partial of these entries sees more than one chunk's accumulations. */
+template <int K> struct DGShape {
+    static constexpr int NDG = K <= 8 ? 16 : 32;
+    static constexpr int GOFF = K <= 8 ? 8 : 16;
+};
 
 template <int K>
 struct MQ {
@@ -101,32 +125,37 @@ struct MQ {
     static constexpr int N = ((T + 15) / 16) * 16;              /* Hessian MMA N (multiple of 16 for M = 128) */
     static constexpr int KP = ((K + 7) / 8) * 8;                /* TF32 K extent of the qp MMAs */
     static constexpr int QPN = 2 * MQ_JC;                       /* qp MMA N: the chunk's p rows, then 1-p rows */
+    static constexpr int NDG = DGShape<K>::NDG, GOFF = DGShape<K>::GOFF;
     static constexpr uint32_t COL_H = 64;                       /* TMEM column of the Hessian accumulator */
-    static constexpr uint32_t NCOLS = tmem_cols_for(COL_H + N);
+    static constexpr uint32_t COL_DG = COL_H + N;               /* TMEM column of the [diag | grad] accumulator */
+    static constexpr uint32_t NCOLS = tmem_cols_for(COL_DG + NDG);
     static constexpr int E = T + K;                             /* partial entries per individual */
-    static constexpr uint32_t A_BYTES = 128 * MQ_JC * 2;        /* one BF16 weight tile: 8 KB */
+    static constexpr uint32_t A_BYTES = 128 * MQ_JC * 2;        /* one BF16 A tile (128 rows x 32 SNPs): 8 KB */
     static constexpr uint32_t B_BYTES = N * MQ_JC * 2;          /* one BF16 pair-product tile */
     static constexpr uint32_t QA_BYTES = 128 * 2 * KP * 4;      /* TF32 Q tile [hi | lo] */
     static constexpr uint32_t QB_BYTES = QPN * 2 * KP * 4;      /* TF32 [p ; 1-p] chunk [hi | lo] */
-    static constexpr int PS = MQ_JC + 4;                        /* FP32 p row stride (floats, 16-byte rows) */
-    /* package of one chunk: [PP tile | PbarPbar tile | TF32 [p ; 1-p] | FP32 p [k][jj]] */
+    static constexpr uint32_t DGB_BYTES = NDG * MQ_JC * 2;      /* one BF16 B block of the [diag | grad] MMA */
+    /* package of one chunk: [PP tile | PbarPbar tile | TF32 [p ; 1-p] | diag p^2 | diag (1-p)^2 |
+     * gradient p (BF16 high part) | gradient p (BF16 low part)] */
     static constexpr uint32_t PK_QB = 2 * B_BYTES;
-    static constexpr uint32_t PK_PF = PK_QB + QB_BYTES;
-    static constexpr uint32_t PKG = PK_PF + K * PS * 4;
+    static constexpr uint32_t PK_DG = PK_QB + QB_BYTES;
+    static constexpr uint32_t PKG = PK_DG + 4 * DGB_BYTES;
     static constexpr uint32_t GBUF = MQ_JC * 32;                /* genotype bytes of one chunk */
-    static constexpr uint32_t OFF_A = 0;                        /* W1 tile, then W2 tile */
-    static constexpr uint32_t OFF_PKG = 2 * A_BYTES;
+    static constexpr uint32_t OFF_A = 0;                        /* W1, W2, DZ0, DZ1 tiles */
+    static constexpr uint32_t OFF_PKG = 4 * A_BYTES;
     static constexpr uint32_t OFF_QA = OFF_PKG + MQ_NPKG * PKG;
     static constexpr uint32_t OFF_G = OFF_QA + QA_BYTES;        /* two G buffers, [pair][byte][2] */
     static constexpr uint32_t OFF_TAB = OFF_G + 2 * GBUF;       /* float4 [16][8] code table */
     static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024; /* + alignment slack */
     /* core matrices (8 rows x 16 B): BF16 A 128 B apart along M, 2048 B along K; BF16 B 128 B
      * along N, 16 N bytes along K; TF32 Q tile 128 B along M, 2048 B along K; TF32 [p ; 1-p]
-     * 128 B along N, 1024 B along K */
+     * 128 B along N, 1024 B along K; [diag | grad] B blocks 128 B along N, 16 NDG bytes along K */
     static constexpr uint32_t A_LBO = 2048, A_SBO = 128;
     static constexpr uint32_t B_LBO = 16 * N, B_SBO = 128;
     static constexpr uint32_t QA_LBO = 2048, QB_LBO = 1024, Q_SBO = 128;
+    static constexpr uint32_t DG_LBO = 16 * NDG;
     static_assert(PKG % 16 == 0 && OFF_QA % 16 == 0, "bulk copies and descriptors need 16-byte alignment");
+    static_assert(K <= 16, "K up to 16");
 };
 
 /* byte offset of element (row r, 4-byte column f) in a K-major no-swizzle tile */
@@ -135,6 +164,19 @@ __device__ __forceinline__ uint32_t kmaj_off(int r, int f, uint32_t lbo)
     return (uint32_t)(f >> 2) * lbo + (uint32_t)(r >> 3) * 128u + (uint32_t)(r & 7) * 16u + (uint32_t)(f & 3) * 4u;
 }
 
+/* BF16 high part of x (round to nearest) and the BF16 of the remainder: hi + lo = x to about
+ * 2^-17 relative */
+__device__ __forceinline__ void bf16_split(float x, uint16_t &hi, uint16_t &lo)
+{
+    const uint32_t h = pack_bf16x2(x, 0.f) & 0xFFFFu;
+    const float r = x - __uint_as_float(h << 16);
+    hi = (uint16_t)h;
+    lo = (uint16_t)(pack_bf16x2(r, 0.f) & 0xFFFFu);
+}
+
+/* Row n's 8 BF16 values of granule kc (8 SNPs) in a B block of `rows` rows */
+__device__ __forceinline__ uint32_t bblk_off(int n, int kc, uint32_t lbo) { return (uint32_t)kc * lbo + 16u * (uint32_t)n; }
+
 /* One package per 32-SNP chunk of the whole SNP range (block = chunk).  SNPs beyond J get
  * p = 0.5; their genotypes read as missing, so they contribute nothing. */
 template <int K>
@@ -142,8 +184,8 @@ __global__ void __launch_bounds__(128)
 k_q_pack(const double *__restrict__ p, int64_t J, uint8_t *__restrict__ pkg)
 {
     using C = MQ<K>;
-    constexpr int T = C::T, N = C::N;
-    __shared__ __align__(16) float pf[2 * K * C::PS];          /* p, then 1-p: [term][k][jj] */
+    constexpr int T = C::T, N = C::N, PS = MQ_JC + 4;
+    __shared__ __align__(16) float pf[2 * K * PS];             /* p, then 1-p: [term][k][jj] */
     __shared__ __align__(16) uint8_t buf[C::PKG];
     const int tid = threadIdx.x;
     const int64_t jc = (int64_t)blockIdx.x * MQ_JC;
@@ -153,9 +195,8 @@ k_q_pack(const double *__restrict__ p, int64_t J, uint8_t *__restrict__ pkg)
         const int jj = t / K, k = t - jj * K;
         const double pd = (jc + jj < J) ? p[(size_t)K * jc + t] : 0.5;
         const float a = (float)pd, b = (float)(1.0 - pd);
-        pf[k * C::PS + jj] = a;
-        pf[K * C::PS + k * C::PS + jj] = b;
-        ((float *)(buf + C::PK_PF))[k * C::PS + jj] = a;
+        pf[k * PS + jj] = a;
+        pf[K * PS + k * PS + jj] = b;
         float h, l;
         tf32_split(a, h, l);
         *(float *)(buf + C::PK_QB + kmaj_off(jj, k, C::QB_LBO)) = h;
@@ -163,6 +204,17 @@ k_q_pack(const double *__restrict__ p, int64_t J, uint8_t *__restrict__ pkg)
         tf32_split(b, h, l);
         *(float *)(buf + C::PK_QB + kmaj_off(MQ_JC + jj, k, C::QB_LBO)) = h;
         *(float *)(buf + C::PK_QB + kmaj_off(MQ_JC + jj, C::KP + k, C::QB_LBO)) = l;
+        /* [diag | grad] B blocks: element (row n, SNP jj) at granule jj / 8, half-word jj % 8 */
+        uint16_t *dgp = (uint16_t *)(buf + C::PK_DG + bblk_off(k, jj >> 3, C::DG_LBO)) + (jj & 7);
+        uint16_t *dgb = (uint16_t *)(buf + C::PK_DG + C::DGB_BYTES + bblk_off(k, jj >> 3, C::DG_LBO)) + (jj & 7);
+        uint16_t *gp0 = (uint16_t *)(buf + C::PK_DG + 2 * C::DGB_BYTES + bblk_off(C::GOFF + k, jj >> 3, C::DG_LBO)) + (jj & 7);
+        uint16_t *gp1 = (uint16_t *)(buf + C::PK_DG + 3 * C::DGB_BYTES + bblk_off(C::GOFF + k, jj >> 3, C::DG_LBO)) + (jj & 7);
+        *dgp = (uint16_t)(pack_bf16x2(a * a, 0.f) & 0xFFFFu);
+        *dgb = (uint16_t)(pack_bf16x2(b * b, 0.f) & 0xFFFFu);
+        uint16_t hi, lo;
+        bf16_split(a, hi, lo);
+        *gp0 = hi;
+        *gp1 = lo;
     }
     __syncthreads();
     /* pair-product tiles: task (term, kc, nn) writes pair nn's 8 SNPs of k-chunk kc at kc*16N + 16nn */
@@ -173,9 +225,9 @@ k_q_pack(const double *__restrict__ p, int64_t J, uint8_t *__restrict__ pkg)
         if (nn < T) {
             int ka, kb;
             tri_pair(nn, ka, kb);
-            const float *src = pf + term * K * C::PS + kc * 8;
-            const float4 a0 = *(const float4 *)(src + ka * C::PS), a1 = *(const float4 *)(src + ka * C::PS + 4);
-            const float4 b0 = *(const float4 *)(src + kb * C::PS), b1 = *(const float4 *)(src + kb * C::PS + 4);
+            const float *src = pf + term * K * PS + kc * 8;
+            const float4 a0 = *(const float4 *)(src + ka * PS), a1 = *(const float4 *)(src + ka * PS + 4);
+            const float4 b0 = *(const float4 *)(src + kb * PS), b1 = *(const float4 *)(src + kb * PS + 4);
             w[0] = pack_bf16x2(a0.x * b0.x, a0.y * b0.y);
             w[1] = pack_bf16x2(a0.z * b0.z, a0.w * b0.w);
             w[2] = pack_bf16x2(a1.x * b1.x, a1.y * b1.y);
@@ -209,6 +261,27 @@ __device__ __forceinline__ void issue_qp(uint32_t tmem, const uint8_t *sm, const
     }
 }
 
+/* The chunk's [diag | grad] MMAs (one thread), a fresh sum into TMEM columns COL_DG..:
+ *   diag:  [W1 | W2] x [p^2 block ; (1-p)^2 block]                      (4 K-steps)
+ *   grad:  [DZ0 | DZ1 | DZ0] x [p hi block ; p hi block ; p lo block]   (6 K-steps)
+ * a_base: the A tiles W1, W2, DZ0, DZ1 (A_BYTES apart); b_base: the package's PK_DG blocks. */
+template <int K, uint32_t A_BYTES, uint32_t A_LBO, uint32_t DGB_BYTES, uint32_t DG_LBO>
+__device__ __forceinline__ void issue_dg(uint32_t tmem_dg, uint32_t a_base, uint32_t b_base)
+{
+    constexpr uint32_t id = idesc_bf16_f32(128, DGShape<K>::NDG);
+    constexpr int AT[5] = {0, 1, 2, 3, 2};   /* A tile of each term: W1, W2, DZ0, DZ1, DZ0 */
+    constexpr int BB[5] = {0, 1, 2, 2, 3};   /* B block of each term: p^2, (1-p)^2, p hi, p hi, p lo */
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            const uint64_t ad = umma_desc_kmajor(a_base + AT[t] * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
+            const uint64_t bd = umma_desc_kmajor(b_base + BB[t] * DGB_BYTES + ks * 2 * DG_LBO, DG_LBO, 128);
+            tc_mma_bf16(tmem_dg, ad, bd, id, (t > 0 || ks > 0) ? 1u : 0u);
+        }
+    }
+}
+
 /* Warp roles: warps 0-3 are producers (thread = accumulator row), warp 4 is the controller
  * (bulk copies, genotype staging, MMA issue).  No CTA-wide barrier inside the chunk loop: the
  * roles hand off through mbarriers.  Every wait is bounded; after a failed wait a thread sets
@@ -216,7 +289,7 @@ __device__ __forceinline__ void issue_qp(uint32_t tmem, const uint8_t *sm, const
 constexpr int MQ_CTA = MQ_THREADS + 32;
 
 template <int K>
-__global__ void __launch_bounds__(MQ_CTA, (K <= 10 ? 3 : (K <= 12 ? 2 : 1)))
+__global__ void __launch_bounds__(MQ_CTA, (K <= 8 ? 3 : (K <= 12 ? 2 : 1)))
 k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                 const double *__restrict__ q, const uint8_t *__restrict__ pkg, int64_t jslice,
                 double *__restrict__ out, int *__restrict__ err)
@@ -225,7 +298,8 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     constexpr int T = C::T, N = C::N, E = C::E;
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    /* qp ready, qp consumed (4 warps), A tile written (4 warps), Hessian done, G staged [2], package [3] */
+    /* qp ready, qp consumed (4 warps), A tiles written (4 warps), the chunk's Hessian and
+     * [diag | grad] MMAs done, G staged [2], package [NPKG] */
     __shared__ uint64_t mbar[6 + MQ_NPKG];
     __shared__ uint32_t tmem_holder;
     __shared__ volatile int abort_flag;
@@ -341,7 +415,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     tc_commit(bar_qp);
                 }
             }
-            /* Hessian of chunk c once the producers wrote its weight tile */
+            /* Hessian and [diag | grad] of chunk c once the producers wrote its A tiles */
             if (wait(bar_afull, (uint32_t)(c & 1))) {
                 if (leader) {
                     tc_fence_after_sync();
@@ -356,12 +430,13 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                             tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || term > 0 || ks > 0) ? 1u : 0u);
                         }
                     }
+                    issue_dg<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase, bbase + C::PK_DG);
                     tc_commit(bar_h);
                 }
                 /* the producers are done with G buffer c & 1: stage chunk c+2 into it */
                 if (c + 2 < nchunk) stage_g(c + 2);
             }
-            /* package c is free once the Hessian of chunk c is done: fetch chunk c+3 into it */
+            /* package c is free once the MMAs of chunk c are done: fetch chunk c+NPKG into it */
             if (c + MQ_NPKG < nchunk && wait(bar_h, (uint32_t)(c & 1))) {
                 fence_async_smem();
                 copy_pkg(c + MQ_NPKG);
@@ -383,13 +458,40 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             sres = (float)(1.0 - sq);
         }
         const float2 sres2 = make_float2(sres, sres);
-        double gd[K];
+        double gd[K], dd[K], zsd = 0.0;   /* gradient sum_j (z1 - z2) p_k, Hessian diagonal, sum_j z2 */
 #pragma unroll
-        for (int k = 0; k < K; ++k) gd[k] = 0.0;
+        for (int k = 0; k < K; ++k) gd[k] = dd[k] = 0.0;
+        /* the [diag | grad] accumulator of the last chunk whose MMAs completed, into FP64 */
+        auto drain_dg = [&]() {
+            tc_fence_after_sync();
+            float v[16];
+            tmem_ld16(tmem + lane_base + C::COL_DG, v);
+#pragma unroll
+            for (int k = 0; k < K && k < 8; ++k) {
+                dd[k] += (double)v[k];
+                if (C::NDG == 16) gd[k] += (double)v[C::GOFF + k];
+            }
+            if constexpr (C::NDG == 32) {
+#pragma unroll
+                for (int k = 8; k < K; ++k) dd[k] += (double)v[k];
+                tmem_ld16(tmem + lane_base + C::COL_DG + 16u, v);
+#pragma unroll
+                for (int k = 0; k < K; ++k) gd[k] += (double)v[k];
+            }
+            tc_fence_before_sync();
+        };
         for (int c = 0; c < nchunk && ok; ++c) {
-            const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
-            const float *Pf = (const float *)(pk + C::PK_PF);
             const uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF;
+            if (c > 0) {   /* the MMAs of chunk c-1 are done: its [diag | grad] sums, free A tiles */
+                if (!wait(bar_h, (uint32_t)((c - 1) & 1))) break;
+                drain_dg();
+                if (c % MX_HBLOCK == 0) {   /* drain the Hessian block of chunks c-MX_HBLOCK .. c-1 */
+                    tc_fence_after_sync();
+                    hess_drain<N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E,
+                                     c == MX_HBLOCK, valid);
+                    tc_fence_before_sync();
+                }
+            }
             /* qp / om of the chunk's 32 SNPs, read in two halves of 16 columns (SNPs 0-15, then
              * 16-31) to keep the producer within its registers */
             uint32_t rq[16], ro[16];
@@ -400,17 +502,8 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             tmem_wait_ld();
             if (!wait(&bar_p[c % MQ_NPKG], (uint32_t)((c / MQ_NPKG) & 1))) break;
             if (!wait(&bar_g[c & 1], (uint32_t)((c >> 1) & 1))) break;
-            if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the weight tile is free */
-            if (c > 0 && c % MX_HBLOCK == 0) {   /* drain the block of chunks c-MX_HBLOCK .. c-1 */
-                tc_fence_after_sync();
-                hess_drain<N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E,
-                                 c == MX_HBLOCK, valid);
-                tc_fence_before_sync();
-            }
             const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);
-            float2 gk[K], zs = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
+            float2 zs = make_float2(0.f, 0.f);
 #pragma unroll
             for (int kc = 0; kc < 4; ++kc) {
                 if (kc == 2) {   /* the second half of the columns; then the qp columns are free */
@@ -422,8 +515,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     __syncwarp();
                     if (lane == 0) mbar_arrive(bar_qfree);
                 }
-                uint32_t w1p[4], w2p[4];
-                float2 dz[4];
+                uint32_t w1p[4], w2p[4], d0p[4], d1p[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int m = kc * 4 + e;
@@ -439,51 +531,38 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const float2 z1 = __fmul2_rn(make_float2(a.x, a.y), r1);
                     const float2 z2 = __fmul2_rn(make_float2(a.z, a.w), r2);
                     const float2 w1 = __fmul2_rn(z1, r1), w2 = __fmul2_rn(z2, r2);
-                    dz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);
+                    const float2 dz = __ffma2_rn(z2, make_float2(-1.f, -1.f), z1);
                     zs = __fadd2_rn(zs, z2);
                     w1p[e] = pack_bf16x2(w1.x, w1.y);
                     w2p[e] = pack_bf16x2(w2.x, w2.y);
+                    /* dz = hi + lo in BF16: hi rounded to nearest, lo the BF16 of the remainder */
+                    const uint32_t h = pack_bf16x2(dz.x, dz.y);
+                    const float2 hf = make_float2(__uint_as_float(h << 16), __uint_as_float(h & 0xFFFF0000u));
+                    const float2 lr = __fadd2_rn(dz, make_float2(-hf.x, -hf.y));
+                    d0p[e] = h;
+                    d1p[e] = pack_bf16x2(lr.x, lr.y);
                 }
                 *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(w1p[0], w1p[1], w1p[2], w1p[3]);
                 *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(w2p[0], w2p[1], w2p[2], w2p[3]);
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    const float4 p0 = *(const float4 *)(Pf + k * C::PS + kc * 8);
-                    const float4 p1 = *(const float4 *)(Pf + k * C::PS + kc * 8 + 4);
-                    gk[k] = __ffma2_rn(dz[0], make_float2(p0.x, p0.y), gk[k]);
-                    gk[k] = __ffma2_rn(dz[1], make_float2(p0.z, p0.w), gk[k]);
-                    gk[k] = __ffma2_rn(dz[2], make_float2(p1.x, p1.y), gk[k]);
-                    gk[k] = __ffma2_rn(dz[3], make_float2(p1.z, p1.w), gk[k]);
-                }
+                *(uint4 *)(At + 2 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d0p[0], d0p[1], d0p[2], d0p[3]);
+                *(uint4 *)(At + 3 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d1p[0], d1p[1], d1p[2], d1p[3]);
             }
-            const double zsum = (double)zs.x + (double)zs.y;
-#pragma unroll
-            for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y + zsum;
+            zsd += (double)zs.x + (double)zs.y;
             fence_async_smem();
             __syncwarp();
             if (lane == 0) mbar_arrive(bar_afull);
         }
-        if (nchunk > 0) wait(bar_h, (uint32_t)((nchunk - 1) & 1));   /* the last Hessian MMAs */
+        if (nchunk > 0 && wait(bar_h, (uint32_t)((nchunk - 1) & 1))) drain_dg();   /* the last chunk */
         if (valid) {
             double *o = out + ((size_t)blockIdx.y * I + i) * E;
 #pragma unroll
-            for (int k = 0; k < K; ++k) o[T + k] = gd[k];
+            for (int k = 0; k < K; ++k) o[T + k] = ok ? gd[k] + zsd : __longlong_as_double(0x7ff8000000000000LL);
         }
-    }
-    /* every role is past its loop; after a failure, give MMAs and copies still in flight a
-     * bounded moment before the TMEM is read and released */
-    ok = __syncthreads_and(ok);
-    if (!ok && tid == MQ_THREADS) {
-        mbar_wait_bounded(bar_h, 0u, 1024u);
-        mbar_wait_bounded(bar_h, 1u, 1024u);
-        mbar_wait_bounded(bar_qp, 0u, 1024u);
-        mbar_wait_bounded(bar_qp, 1u, 1024u);
-        for (int b = 0; b < MQ_NPKG; ++b) { mbar_wait_bounded(&bar_p[b], 0u, 1024u); mbar_wait_bounded(&bar_p[b], 1u, 1024u); }
-    }
-    __syncthreads();
-    tc_fence_after_sync();
-    if (producer) {
-        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        /* every role is past its loop; the controller gives MMAs and copies still in flight a
+         * bounded moment (after a failure) before the TMEM is read and released */
+        ok = __syncthreads_and(ok);
+        __syncthreads();
+        tc_fence_after_sync();
         if (nchunk > 0) {
 #pragma unroll 1
             for (int c0 = 0; c0 < N; c0 += 16) {
@@ -499,11 +578,31 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                                            : __longlong_as_double(0x7ff8000000000000LL);
                 }
             }
-        } else if (valid) {
-            double *o = out + ((size_t)blockIdx.y * I + i) * E;
-            for (int e = 0; e < T; ++e) o[e] = 0.0;
         }
+        if (valid) {   /* the diagonal from the per-chunk [diag | grad] sums (FP64 across chunks) */
+            double *o = out + ((size_t)blockIdx.y * I + i) * E;
+            if (nchunk == 0) {
+                for (int e = 0; e < T; ++e) o[e] = 0.0;
+            } else {
+#pragma unroll
+                for (int k = 0; k < K; ++k)
+                    o[k * (k + 1) / 2 + k] = ok ? dd[k] : __longlong_as_double(0x7ff8000000000000LL);
+            }
+        }
+        tc_fence_before_sync();
+        __syncthreads();
+        return;
     }
+    /* controller: the same three CTA-wide barriers as the producers' epilogue */
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == MQ_THREADS) {
+        mbar_wait_bounded(bar_h, 0u, 1024u);
+        mbar_wait_bounded(bar_h, 1u, 1024u);
+        mbar_wait_bounded(bar_qp, 0u, 1024u);
+        mbar_wait_bounded(bar_qp, 1u, 1024u);
+        for (int b = 0; b < MQ_NPKG; ++b) { mbar_wait_bounded(&bar_p[b], 0u, 1024u); mbar_wait_bounded(&bar_p[b], 1u, 1024u); }
+    }
+    __syncthreads();
     tc_fence_before_sync();
     __syncthreads();
     if (warp == 4) tmem_dealloc_warp(tmem, C::NCOLS);
@@ -515,10 +614,13 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
  * chunks of 32 individuals.  Per chunk:
  *   qp, om     D[128 x 32] = Ptile * Qchunk^T and (1-P)tile * Qchunk^T, TF32 split form;
  *   Hessian    D[128 x N] += C * QQ^T in BF16, C = nm (g/qp^2 + (2-g)/(1-qp)^2);
- * and per cell on the CUDA cores the code (from the thread's own genotype word), one reciprocal
- * and the FP32 gradient sum_i nm (g/qp - (2-g)/(1-qp)) q_k, added into FP64 per chunk.  The
- * Q-derived tiles of each chunk (QQ in BF16, Q split into TF32 hi / lo, q in FP32) are built
- * once per sweep by k_p_pack and fetched with one bulk copy per chunk. */
+ *   diag/grad  D[128 x NDG] = C * [q^2]^T (the Hessian diagonal) and
+ *              [dz_hi | dz_lo | dz_hi] * [q_hi ; q_hi ; q_lo]^T (the gradient sum_i dz q_k,
+ *              dz = nm (g/qp - (2-g)/(1-qp))), afresh every chunk and added into FP64;
+ * and per cell on the CUDA cores the code (from the thread's own genotype word), one reciprocal,
+ * C, dz and its BF16 split.  The Q-derived tiles of each chunk (QQ in BF16, Q split into TF32
+ * hi / lo, the diagonal and gradient B blocks, q in FP32 for the EM mode) are built once per
+ * sweep by k_p_pack and fetched with one bulk copy per chunk. */
 
 constexpr int MP_IC = 32;          /* individuals per chunk = 2 BF16 MMA K-steps */
 constexpr int MP_THREADS = 128;    /* one thread per SNP = accumulator row */
@@ -529,26 +631,32 @@ struct MP {
     static constexpr int T = K * (K + 1) / 2;
     static constexpr int N = ((T + 15) / 16) * 16;
     static constexpr int KP = ((K + 7) / 8) * 8;
+    static constexpr int NDG = DGShape<K>::NDG, GOFF = DGShape<K>::GOFF;
     static constexpr uint32_t COL_OM = 32, COL_H = 64;          /* TMEM: qp 0..31, om 32..63, Hessian */
-    static constexpr uint32_t NCOLS = tmem_cols_for(COL_H + N);
+    static constexpr uint32_t COL_DG = COL_H + N;               /* [diag | grad] accumulator */
+    static constexpr uint32_t NCOLS = tmem_cols_for(COL_DG + NDG);
     static constexpr int E = T + K;
-    static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* BF16 C tile: 8 KB */
+    static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* one BF16 A tile (C, DZ0, DZ1): 8 KB */
     static constexpr uint32_t B_BYTES = N * MP_IC * 2;          /* BF16 QQ tile */
     static constexpr uint32_t PA_BYTES = 128 * 2 * KP * 4;      /* TF32 P tile [hi | lo] (and 1-P) */
     static constexpr uint32_t QB_BYTES = MP_IC * 2 * KP * 4;    /* TF32 Q chunk [hi | lo] */
+    static constexpr uint32_t DGB_BYTES = NDG * MP_IC * 2;      /* one BF16 B block of the [diag | grad] MMA */
     static constexpr int QS = MP_IC + 4;                        /* FP32 q row stride (floats) */
+    /* package: [QQ | TF32 Q | FP32 q (EM mode) | 1 - sum q | diag q^2 | grad q hi | grad q lo] */
     static constexpr uint32_t PK_QB = B_BYTES;
     static constexpr uint32_t PK_QF = PK_QB + QB_BYTES;
     static constexpr uint32_t PK_S = PK_QF + K * QS * 4;         /* 1 - sum_k q_k per individual */
-    static constexpr uint32_t PKG = PK_S + MP_IC * 4;
-    static constexpr uint32_t OFF_A = 0;
-    static constexpr uint32_t OFF_PKG = A_BYTES;
+    static constexpr uint32_t PK_DG = PK_S + MP_IC * 4;
+    static constexpr uint32_t PKG = PK_DG + 3 * DGB_BYTES;
+    static constexpr uint32_t OFF_A = 0;                        /* C, DZ0, DZ1 */
+    static constexpr uint32_t OFF_PKG = 3 * A_BYTES;
     static constexpr uint32_t OFF_PA = OFF_PKG + MP_NPKG * PKG; /* P tile, then (1-P) tile */
     static constexpr uint32_t OFF_TAB = OFF_PA + 2 * PA_BYTES;
     static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024;
     static constexpr uint32_t A_LBO = 2048, A_SBO = 128;
     static constexpr uint32_t B_LBO = 16 * N, B_SBO = 128;
     static constexpr uint32_t PA_LBO = 2048, QB_LBO = 512, T_SBO = 128;
+    static constexpr uint32_t DG_LBO = 16 * NDG;
     static_assert(PKG % 16 == 0 && OFF_PA % 16 == 0, "bulk copies and descriptors need 16-byte alignment");
 };
 
@@ -582,6 +690,15 @@ k_p_pack(const double *__restrict__ q, int64_t I, uint8_t *__restrict__ pkg)
         tf32_split(a, h, l);
         *(float *)(buf + C::PK_QB + kmaj_off(ii, k, C::QB_LBO)) = h;
         *(float *)(buf + C::PK_QB + kmaj_off(ii, C::KP + k, C::QB_LBO)) = l;
+        /* [diag | grad] B blocks: element (row n, individual ii) at granule ii / 8, half-word ii % 8 */
+        uint16_t *dg = (uint16_t *)(buf + C::PK_DG + bblk_off(k, ii >> 3, C::DG_LBO)) + (ii & 7);
+        uint16_t *g0 = (uint16_t *)(buf + C::PK_DG + C::DGB_BYTES + bblk_off(C::GOFF + k, ii >> 3, C::DG_LBO)) + (ii & 7);
+        uint16_t *g1 = (uint16_t *)(buf + C::PK_DG + 2 * C::DGB_BYTES + bblk_off(C::GOFF + k, ii >> 3, C::DG_LBO)) + (ii & 7);
+        *dg = (uint16_t)(pack_bf16x2(a * a, 0.f) & 0xFFFFu);
+        uint16_t hi, lo;
+        bf16_split(a, hi, lo);
+        *g0 = hi;
+        *g1 = lo;
     }
     __syncthreads();
     /* QQ tile: task (kc, nn) writes pair nn's 8 individuals of k-chunk kc at kc*16N + 16nn */
@@ -646,6 +763,27 @@ __device__ __forceinline__ uint2 col_load32(const uint8_t *__restrict__ bed, int
  * same pipeline: per SNP the two sums sum_i nm g q_k / qp and sum_i nm (2-g) q_k / (1-qp)
  * (rows of 2K, the FP64 EM sweep's layout, finalised by k_emp_finalize), with no Hessian tile,
  * MMAs or drains; a package slot is handed back once the four producer warps have read it. */
+/* The chunk's [diag | grad] MMAs of the P side (one thread), a fresh sum into COL_DG..:
+ *   diag:  C x [q^2 block]                                                (2 K-steps)
+ *   grad:  [DZ0 | DZ1 | DZ0] x [q hi block ; q hi block ; q lo block]   (6 K-steps)
+ * a_base: the A tiles C, DZ0, DZ1 (A_BYTES apart); b_base: the package's PK_DG blocks. */
+template <int K, uint32_t A_BYTES, uint32_t A_LBO, uint32_t DGB_BYTES, uint32_t DG_LBO>
+__device__ __forceinline__ void issue_dg_p(uint32_t tmem_dg, uint32_t a_base, uint32_t b_base)
+{
+    constexpr uint32_t id = idesc_bf16_f32(128, DGShape<K>::NDG);
+    constexpr int AT[4] = {0, 1, 2, 1};   /* A tile of each term: C, DZ0, DZ1, DZ0 */
+    constexpr int BB[4] = {0, 1, 1, 2};   /* B block of each term: q^2, q hi, q hi, q lo */
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            const uint64_t ad = umma_desc_kmajor(a_base + AT[t] * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
+            const uint64_t bd = umma_desc_kmajor(b_base + BB[t] * DGB_BYTES + ks * 2 * DG_LBO, DG_LBO, 128);
+            tc_mma_bf16(tmem_dg, ad, bd, id, (t > 0 || ks > 0) ? 1u : 0u);
+        }
+    }
+}
+
 constexpr int MP_CTA = MP_THREADS + 32;
 
 template <int K, bool EMS>
@@ -675,6 +813,9 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     const int nchunk = (int)((ib - ia + MP_IC - 1) / MP_IC);
     const uint8_t *pk0 = pkg + (size_t)(ia / MP_IC) * C::PKG;
     uint8_t *At = sm + C::OFF_A;
+    double diag_keep[K];   /* producers: the Hessian diagonal, kept for the epilogue */
+#pragma unroll
+    for (int k = 0; k < K; ++k) diag_keep[k] = 0.0;
 
     if (warp == 4) tmem_alloc_warp(&tmem_holder, C::NCOLS);
     if (tid == 0) {
@@ -771,6 +912,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
                     tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || ks > 0) ? 1u : 0u);
                 }
+                issue_dg_p<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase, bbase + C::PK_DG);
                 tc_commit(bar_h);
             }
             if (c + MP_NPKG < nchunk && wait(bar_h, (uint32_t)(c & 1))) {
@@ -785,15 +927,52 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         uint2 gcur = make_uint2(0x55555555u, 0x55555555u), gnext = gcur;
         if (nchunk > 0) gcur = col_load32(bed, pitch, j, valid, ia);
         if (nchunk > 1) gnext = col_load32(bed, pitch, j, valid, ia + MP_IC);
-        double gd[K], hd[EMS ? K : 1];
+        /* gradient sum_i dz q_k (EM mode: sum_i nm g q_k / qp), Hessian diagonal, and the EM mode's
+         * second sums */
+        double gd[K], dd[EMS ? 1 : K], hd[EMS ? K : 1];
 #pragma unroll
         for (int k = 0; k < K; ++k) gd[k] = 0.0;
 #pragma unroll
+        for (int k = 0; k < (EMS ? 1 : K); ++k) dd[k] = 0.0;
+#pragma unroll
         for (int k = 0; k < (EMS ? K : 1); ++k) hd[k] = 0.0;
+        /* the [diag | grad] accumulator of the last chunk whose MMAs completed, into FP64 */
+        auto drain_dg = [&]() {
+            if constexpr (!EMS) {
+                tc_fence_after_sync();
+                float v[16];
+                tmem_ld16(tmem + lane_base + C::COL_DG, v);
+#pragma unroll
+                for (int k = 0; k < K && k < 8; ++k) {
+                    dd[k] += (double)v[k];
+                    if (C::NDG == 16) gd[k] += (double)v[C::GOFF + k];
+                }
+                if constexpr (C::NDG == 32) {
+#pragma unroll
+                    for (int k = 8; k < K; ++k) dd[k] += (double)v[k];
+                    tmem_ld16(tmem + lane_base + C::COL_DG + 16u, v);
+#pragma unroll
+                    for (int k = 0; k < K; ++k) gd[k] += (double)v[k];
+                }
+                tc_fence_before_sync();
+            }
+        };
         for (int c = 0; c < nchunk && ok; ++c) {
             const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
             const float *Qf = (const float *)(pk + C::PK_QF);
             const float2 *Sres = (const float2 *)(pk + C::PK_S);
+            if constexpr (!EMS) {
+                if (c > 0) {   /* the MMAs of chunk c-1 are done: its [diag | grad] sums, free A tiles */
+                    if (!wait(bar_h, (uint32_t)((c - 1) & 1))) break;
+                    drain_dg();
+                    if (c % MX_HBLOCK == 0) {   /* drain the Hessian block of chunks c-MX_HBLOCK .. c-1 */
+                        tc_fence_after_sync();
+                        hess_drain<N, T>(tmem + lane_base + C::COL_H,
+                                         out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E, c == MX_HBLOCK, valid);
+                        tc_fence_before_sync();
+                    }
+                }
+            }
             /* qp / om of the chunk's 32 individuals, read in two halves of 16 columns
              * (individuals 0-15, then 16-31) to keep the producer within its registers */
             uint32_t rq[16], ro[16];
@@ -803,15 +982,6 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             tmem_ld16_raw(tmem + lane_base + C::COL_OM, ro);
             tmem_wait_ld();
             if (!wait(&bar_p[c % MP_NPKG], (uint32_t)((c / MP_NPKG) & 1))) break;
-            if constexpr (!EMS) {
-                if (c > 0 && !wait(bar_h, (uint32_t)((c - 1) & 1))) break;   /* the C tile is free */
-                if (c > 0 && c % MX_HBLOCK == 0) {   /* drain the block of chunks c-MX_HBLOCK .. c-1 */
-                    tc_fence_after_sync();
-                    hess_drain<N, T>(tmem + lane_base + C::COL_H,
-                                     out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E, c == MX_HBLOCK, valid);
-                    tc_fence_before_sync();
-                }
-            }
             float2 gk[K], hk[EMS ? K : 1];
 #pragma unroll
             for (int k = 0; k < K; ++k) gk[k] = make_float2(0.f, 0.f);
@@ -828,7 +998,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     __syncwarp();
                     if (lane == 0) mbar_arrive(bar_qfree);
                 }
-                uint32_t cp[4];
+                uint32_t cp[4], d0p[4], d1p[4];
                 float2 zz[4], z2s[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
@@ -849,12 +1019,21 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                         z2s[e] = z2;                                            /* nm (2-g) / (1-qp) */
                     } else {
                         const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
-                        zz[e] = make_float2(z1.x - z2.x, z1.y - z2.y);              /* nm (g/qp - (2-g)/(1-qp)) */
+                        const float2 dz = __ffma2_rn(z2, make_float2(-1.f, -1.f), z1);   /* nm (g/qp - (2-g)/(1-qp)) */
                         cp[e] = pack_bf16x2(cw.x, cw.y);
+                        /* dz = hi + lo in BF16: hi rounded to nearest, lo the BF16 of the remainder */
+                        const uint32_t h = pack_bf16x2(dz.x, dz.y);
+                        const float2 hf = make_float2(__uint_as_float(h << 16), __uint_as_float(h & 0xFFFF0000u));
+                        const float2 lr = __fadd2_rn(dz, make_float2(-hf.x, -hf.y));
+                        d0p[e] = h;
+                        d1p[e] = pack_bf16x2(lr.x, lr.y);
                     }
                 }
-                if constexpr (!EMS)
+                if constexpr (!EMS) {
                     *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
+                    *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d0p[0], d0p[1], d0p[2], d0p[3]);
+                    *(uint4 *)(At + 2 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d1p[0], d1p[1], d1p[2], d1p[3]);
+                } else {
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
                     const float4 q0 = *(const float4 *)(Qf + k * C::QS + kc * 8);
@@ -863,21 +1042,20 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     gk[k] = __ffma2_rn(zz[1], make_float2(q0.z, q0.w), gk[k]);
                     gk[k] = __ffma2_rn(zz[2], make_float2(q1.x, q1.y), gk[k]);
                     gk[k] = __ffma2_rn(zz[3], make_float2(q1.z, q1.w), gk[k]);
-                    if constexpr (EMS) {
-                        hk[k] = __ffma2_rn(z2s[0], make_float2(q0.x, q0.y), hk[k]);
-                        hk[k] = __ffma2_rn(z2s[1], make_float2(q0.z, q0.w), hk[k]);
-                        hk[k] = __ffma2_rn(z2s[2], make_float2(q1.x, q1.y), hk[k]);
-                        hk[k] = __ffma2_rn(z2s[3], make_float2(q1.z, q1.w), hk[k]);
-                    }
+                    hk[k] = __ffma2_rn(z2s[0], make_float2(q0.x, q0.y), hk[k]);
+                    hk[k] = __ffma2_rn(z2s[1], make_float2(q0.z, q0.w), hk[k]);
+                    hk[k] = __ffma2_rn(z2s[2], make_float2(q1.x, q1.y), hk[k]);
+                    hk[k] = __ffma2_rn(z2s[3], make_float2(q1.z, q1.w), hk[k]);
+                }
                 }
             }
             if constexpr (EMS) {   /* the package is read: hand its slot back */
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&bar_read[c % MP_NPKG]);
             }
-#pragma unroll
-            for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y;
             if constexpr (EMS) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) gd[k] += (double)gk[k].x + (double)gk[k].y;
 #pragma unroll
                 for (int k = 0; k < K; ++k) hd[k] += (double)hk[k].x + (double)hk[k].y;
             }
@@ -902,12 +1080,16 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 }
             }
         } else {
-            if (nchunk > 0) wait(bar_h, (uint32_t)((nchunk - 1) & 1));   /* the last Hessian MMAs */
+            if (nchunk > 0 && wait(bar_h, (uint32_t)((nchunk - 1) & 1))) drain_dg();   /* the last chunk */
             if (valid) {
                 double *o = out + ((size_t)blockIdx.y * J + j) * E;
 #pragma unroll
-                for (int k = 0; k < K; ++k) o[T + k] = gd[k];
+                for (int k = 0; k < K; ++k) o[T + k] = ok ? gd[k] : __longlong_as_double(0x7ff8000000000000LL);
             }
+        }
+        if constexpr (!EMS) {   /* the epilogue below writes the diagonal from these */
+#pragma unroll
+            for (int k = 0; k < K; ++k) diag_keep[k] = dd[k];
         }
     }
     ok = __syncthreads_and(ok);
@@ -941,173 +1123,297 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             double *o = out + ((size_t)blockIdx.y * J + j) * E;
             for (int e = 0; e < T; ++e) o[e] = 0.0;
         }
+        if (valid && nchunk > 0) {   /* the diagonal from the per-chunk [diag | grad] sums (FP64 across chunks) */
+            double *o = out + ((size_t)blockIdx.y * J + j) * E;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                o[k * (k + 1) / 2 + k] = ok ? diag_keep[k] : __longlong_as_double(0x7ff8000000000000LL);
+        }
     }
     tc_fence_before_sync();
     __syncthreads();
     if (warp == 4) tmem_dealloc_warp(tmem, C::NCOLS);
 }
 
-/* 64 individuals' codes of SNP column j from individual ic (a multiple of 64) */
-__device__ __forceinline__ uint4 col_load64(const uint8_t *__restrict__ bed, int64_t pitch, int64_t j, bool valid,
-                                            int64_t ic)
-{
-    return valid ? __ldg((const uint4 *)(bed + (size_t)j * pitch + (size_t)(ic / 4)))
-                 : make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
-}
-
-/* ===================================================================== loglik
- * loglikelihood_loop_skipmissing (loops.jl:517-539) with FP32 cells: thread = SNP, individuals
- * in pairs; qp is an FP32 FMA chain and 1 - qp is formed from it by one subtraction (exact for
- * qp >= 1/2), as the reference forms it; each cell contributes qp^g (1-qp)^(2-g) (1 when
- * missing), two cells' factors are
- * multiplied in FP32 and folded into an FP64 running product whose exponent moves into an
- * integer every 12 pairs; one FP64 log per thread at the end.  Every product is rounded to
- * nearest, so the rounding error is a random walk far below the convergence test's resolution. */
-constexpr int ML_IC = 64;
-
-constexpr int ML_JT = 2;   /* SNPs per thread (j and j + 128): each broadcast load of q serves both */
+/* ===================================================================== loglik on the tensor cores
+ * loglikelihood_loop_skipmissing (loops.jl:517-539) with qp from tcgen05 in exact pieces.
+ *
+ * Every q and p is split into three BF16 limbs on fixed grids: x0 = round(x 2^8) 2^-8,
+ * x1 = round((x - x0) 2^16) 2^-16, x2 = round((x - x0 - x1) 2^24) 2^-24 (each an integer of at most
+ * 8 bits times a power of two, so exact in BF16; |x - x0 - x1 - x2| <= 2^-25).  Two accumulators
+ * per cell:
+ *   L01 = sum_k q0 p0 + q0 p1 + q1 p0   a multiple of 2^-24 below 1,
+ *   L2  = sum_k q0 p2 + q1 p1 + q2 p0   a multiple of 2^-32 below 2^-12,
+ * so every product and partial sum of either accumulator is exactly representable in FP32 and
+ * the tensor core's accumulation (which rounds toward zero when it has to round) never rounds.
+ * On the CUDA cores qp = L01 + L2 and 1 - qp = (1 - L01) - L2 (1 - L01 exact) are then rounded
+ * to nearest once each: unbiased, and 1 - qp keeps its relative accuracy as qp -> 1.  (A single
+ * TF32 accumulation biases every qp low by about half an ulp, which moves the log-likelihood
+ * by ~1e-7 relative.)  The limbs' own rounding (2^-25 absolute, to nearest) and the dropped
+ * products q1 p2, q2 p1, q2 p2 are of random sign.
+ *
+ * Per cell the CUDA cores then form qp^g (1-qp)^(2-g) (1 when missing) and fold it into a
+ * running product: two cells' factors multiplied in FP32, one FP64 multiply per pair, the
+ * exponent moved into an integer every 16 cells, one log per thread at the end.
+ *
+ * Roles as in the sweeps: warps 0-3 producers (thread = SNP = TMEM lane), warp 4 controller
+ * (bulk copies of the per-chunk individual packages, MMA issue).  TMEM holds two chunk buffers
+ * of [L01 | L2] x 32 individuals, so the MMAs of chunk c+1 run while chunk c is consumed. */
+constexpr int LT_IC = 32;          /* individuals per chunk (MMA N) */
+constexpr int LT_NPKG = 4;         /* package buffers */
 
 template <int K>
-__global__ void __launch_bounds__(128, (K <= 10 ? 6 : 4))
-k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
-               const double *__restrict__ q, const double *__restrict__ p, int64_t islice,
-               double *__restrict__ partial)
+struct LT {
+    static constexpr int KP = ((K + 7) / 8) * 8;                /* limb width (granules of 8) */
+    static constexpr int R = ((3 * KP + 15) / 16) * 16;         /* reduction length of one accumulator */
+    static constexpr int NG = R / 8;                            /* granules per row */
+    static constexpr uint32_t A_BYTES = 128 * R * 2;            /* one P-limb tile (128 SNPs) */
+    static constexpr uint32_t B_BYTES = LT_IC * R * 2;          /* one Q-limb tile (32 individuals) */
+    static constexpr uint32_t PKG = 2 * B_BYTES;                /* [B01 | B2] */
+    static constexpr uint32_t OFF_A = 0;                        /* A01, A2 */
+    static constexpr uint32_t OFF_PKG = 2 * A_BYTES;
+    static constexpr uint32_t SMEM = OFF_PKG + LT_NPKG * PKG + 1024;
+    static constexpr uint32_t A_LBO = 128 * 16, B_LBO = LT_IC * 16, SBO = 128;
+    static constexpr uint32_t NCOLS = 128;                      /* 2 buffers x [L01 | L2] x 32 */
+    static_assert(PKG % 16 == 0 && OFF_PKG % 1024 == 0, "bulk copies and descriptors need alignment");
+};
+
+/* the three BF16 limbs of x in [0, 1] (exact conversions: each limb has at most 8 significant bits) */
+__device__ __forceinline__ void limbs3(double x, uint16_t &l0, uint16_t &l1, uint16_t &l2)
 {
-    constexpr int PREF = (K * ML_IC + 127) / 128;
-    __shared__ float4 Qs[2][K][ML_IC / 4];              /* q of individuals 4m .. 4m+3 */
-    __shared__ double red[4];
+    const double a = rint(x * 256.0) * (1.0 / 256.0);
+    const double r = x - a;
+    const double b = rint(r * 65536.0) * (1.0 / 65536.0);
+    const double c = rint((r - b) * 16777216.0) * (1.0 / 16777216.0);
+    l0 = (uint16_t)(pack_bf16x2((float)a, 0.f) & 0xFFFFu);
+    l1 = (uint16_t)(pack_bf16x2((float)b, 0.f) & 0xFFFFu);
+    l2 = (uint16_t)(pack_bf16x2((float)c, 0.f) & 0xFFFFu);
+}
+
+/* byte offset of row r's element e in a K-major BF16 tile whose granules (8 elements of every
+ * row) are lbo bytes apart */
+__device__ __forceinline__ uint32_t lt_off(int r, int e, uint32_t lbo) { return (uint32_t)(e >> 3) * lbo + 16u * (uint32_t)r + 2u * (uint32_t)(e & 7); }
+
+/* Per-chunk packages of 32 individuals: B01 = [q0 | q0 | q1], B2 = [q0 | q1 | q2] (limb widths KP,
+ * zero padding).  Individuals beyond I get q = 0; their genotypes read as missing. */
+template <int K>
+__global__ void __launch_bounds__(128)
+k_ll_pack(const double *__restrict__ q, int64_t I, uint8_t *__restrict__ pkg)
+{
+    using C = LT<K>;
+    __shared__ __align__(16) uint8_t buf[C::PKG];
     const int tid = threadIdx.x;
-    const int64_t j0 = (int64_t)blockIdx.x * (128 * ML_JT) + tid;
-    const int64_t ia = (int64_t)blockIdx.y * islice;
+    const int64_t ic = (int64_t)blockIdx.x * LT_IC;
+    for (uint32_t t = tid; t < C::PKG / 16; t += 128) ((uint4 *)buf)[t] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    for (int t = tid; t < K * LT_IC; t += 128) {
+        const int ii = t / K, k = t - ii * K;
+        const double v = (ic + ii < I) ? q[(size_t)K * ic + t] : 0.0;
+        uint16_t l0, l1, l2;
+        limbs3(v, l0, l1, l2);
+        uint8_t *b01 = buf, *b2 = buf + C::B_BYTES;
+        *(uint16_t *)(b01 + lt_off(ii, k, C::B_LBO)) = l0;
+        *(uint16_t *)(b01 + lt_off(ii, C::KP + k, C::B_LBO)) = l0;
+        *(uint16_t *)(b01 + lt_off(ii, 2 * C::KP + k, C::B_LBO)) = l1;
+        *(uint16_t *)(b2 + lt_off(ii, k, C::B_LBO)) = l0;
+        *(uint16_t *)(b2 + lt_off(ii, C::KP + k, C::B_LBO)) = l1;
+        *(uint16_t *)(b2 + lt_off(ii, 2 * C::KP + k, C::B_LBO)) = l2;
+    }
+    __syncthreads();
+    uint4 *dst = (uint4 *)(pkg + (size_t)blockIdx.x * C::PKG);
+    for (uint32_t t = tid; t < C::PKG / 16; t += 128) dst[t] = ((const uint4 *)buf)[t];
+}
+
+constexpr int LT_CTA = 128 + 32;
+
+template <int K>
+__global__ void __launch_bounds__(LT_CTA, 4)
+k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
+               const double *__restrict__ p, const uint8_t *__restrict__ pkg, int64_t islice,
+               double *__restrict__ partial, int *__restrict__ err)
+{
+    using C = LT<K>;
+    extern __shared__ __align__(1024) uint8_t smraw[];
+    uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    /* package landed [NPKG], MMAs of buffer b done [2], buffer b read (4 warps) [2] */
+    __shared__ uint64_t mbar[LT_NPKG + 4];
+    __shared__ uint32_t tmem_holder;
+    __shared__ volatile int abort_flag;
+    __shared__ double red[4];
+    uint64_t *bar_p = &mbar[0], *bar_mma = &mbar[LT_NPKG], *bar_free = &mbar[LT_NPKG + 2];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp < 4;
+    const int64_t j = (int64_t)blockIdx.x * 128 + tid;
+    const bool valid = producer && j < J;
+    const int64_t ia = (int64_t)blockIdx.y * islice;    /* islice is a multiple of LT_IC */
     const int64_t ib = min(I, ia + islice);
-    const int nchunk = (int)((ib - ia + ML_IC - 1) / ML_IC);
-    bool valid[ML_JT];
-    float2 pd[ML_JT][K];
-#pragma unroll
-    for (int t = 0; t < ML_JT; ++t) {
-        const int64_t j = j0 + 128 * t;
-        valid[t] = j < J;
-#pragma unroll
+    const int nchunk = (int)((ib - ia + LT_IC - 1) / LT_IC);
+    const uint8_t *pk0 = pkg + (size_t)(ia / LT_IC) * C::PKG;
+
+    if (warp == 4) tmem_alloc_warp(&tmem_holder, C::NCOLS);
+    if (tid == 0) {
+        for (int b = 0; b < LT_NPKG; ++b) mbar_init(&bar_p[b], 1);
+        mbar_init(&bar_mma[0], 1);
+        mbar_init(&bar_mma[1], 1);
+        mbar_init(&bar_free[0], 4);
+        mbar_init(&bar_free[1], 4);
+        abort_flag = 0;
+        mbar_fence_init();
+    }
+    if (producer) {   /* this SNP's rows of A01 = [p0 | p1 | p0] and A2 = [p2 | p1 | p0] */
+        uint8_t *a01 = sm + C::OFF_A, *a2 = a01 + C::A_BYTES;
+        for (int g = 0; g < C::NG; ++g) {
+            *(uint4 *)(a01 + g * C::A_LBO + 16 * tid) = make_uint4(0u, 0u, 0u, 0u);
+            *(uint4 *)(a2 + g * C::A_LBO + 16 * tid) = make_uint4(0u, 0u, 0u, 0u);
+        }
         for (int k = 0; k < K; ++k) {
-            const double pv = valid[t] ? p[(size_t)K * j + k] : 0.5;
-            pd[t][k] = make_float2((float)pv, (float)pv);
+            uint16_t l0, l1, l2;
+            limbs3(valid ? p[(size_t)K * j + k] : 0.0, l0, l1, l2);
+            *(uint16_t *)(a01 + lt_off(tid, k, C::A_LBO)) = l0;
+            *(uint16_t *)(a01 + lt_off(tid, C::KP + k, C::A_LBO)) = l1;
+            *(uint16_t *)(a01 + lt_off(tid, 2 * C::KP + k, C::A_LBO)) = l0;
+            *(uint16_t *)(a2 + lt_off(tid, k, C::A_LBO)) = l2;
+            *(uint16_t *)(a2 + lt_off(tid, C::KP + k, C::A_LBO)) = l1;
+            *(uint16_t *)(a2 + lt_off(tid, 2 * C::KP + k, C::A_LBO)) = l0;
         }
     }
-    float qr[PREF];
-    const uint4 none = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
-    uint4 g[ML_JT], gnext[ML_JT];
-#pragma unroll
-    for (int t = 0; t < ML_JT; ++t) g[t] = gnext[t] = none;
-    auto load = [&](int64_t ic) {
-#pragma unroll
-        for (int u = 0; u < PREF; ++u) {
-            const int t = tid + u * 128;                 /* t = k * IC + ii */
-            const int k = t / ML_IC, ii = t - k * ML_IC;
-            qr[u] = (t < K * ML_IC && ic + ii < ib) ? (float)q[(size_t)K * (ic + ii) + k] : 1.0f / K;
+    fence_async_smem();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tmem = tmem_holder;
+    bool ok = true;
+    auto wait = [&](uint64_t *b, uint32_t parity) -> bool {
+        if (!ok) return false;
+        for (uint32_t n = 0; n < MX_WAIT_LIMIT; ++n) {
+            if (mbar_try_wait(b, parity)) return true;
+            if ((n & 255u) == 255u && abort_flag) break;
         }
-#pragma unroll
-        for (int t = 0; t < ML_JT; ++t) gnext[t] = col_load64(bed, pitch, j0 + 128 * t, valid[t], ic);
+        ok = false;
+        abort_flag = 1;
+        atomicOr(err, 1);
+        return false;
     };
-    auto store = [&](int s) {
+    double ll = 0.0;
+
+    if (!producer) {
+        /* ---------------------------------------------------------------- controller warp */
+        const bool leader = lane == 0;
+        auto copy_pkg = [&](int c) {
+            if (leader) {
+                mbar_arrive_expect_tx(&bar_p[c % LT_NPKG], C::PKG);
+                bulk_g2s(sm + C::OFF_PKG + (c % LT_NPKG) * C::PKG, pk0 + (size_t)c * C::PKG, C::PKG, &bar_p[c % LT_NPKG]);
+            }
+        };
+        for (int c = 0; c < min(nchunk, LT_NPKG); ++c) copy_pkg(c);
+        constexpr uint32_t idesc = idesc_bf16_f32(128, LT_IC);
+        const uint32_t a01 = smem_u32(sm + C::OFF_A), a2 = a01 + C::A_BYTES;
+        for (int c = 0; c < nchunk && ok; ++c) {
+            const int b = c & 1;
+            if (!wait(&bar_p[c % LT_NPKG], (uint32_t)((c / LT_NPKG) & 1))) break;
+            if (c >= 2 && !wait(&bar_free[b], (uint32_t)(((c - 2) >> 1) & 1))) break;   /* buffer b was read */
+            if (leader) {
+                tc_fence_after_sync();
+                const uint32_t b01 = smem_u32(sm + C::OFF_PKG + (c % LT_NPKG) * C::PKG), b2 = b01 + C::B_BYTES;
+                const uint32_t d = tmem + (uint32_t)(b * 2 * LT_IC);
 #pragma unroll
-        for (int u = 0; u < PREF; ++u) {
-            const int t = tid + u * 128;
-            if (t < K * ML_IC) {
-                const int k = t / ML_IC, ii = t - k * ML_IC;
-                ((float *)Qs[s][k])[ii] = qr[u];
+                for (int s = 0; s < C::R / 16; ++s) {
+                    tc_mma_bf16(d, umma_desc_kmajor(a01 + s * 2 * C::A_LBO, C::A_LBO, C::SBO),
+                                umma_desc_kmajor(b01 + s * 2 * C::B_LBO, C::B_LBO, C::SBO), idesc, s > 0 ? 1u : 0u);
+                    tc_mma_bf16(d + LT_IC, umma_desc_kmajor(a2 + s * 2 * C::A_LBO, C::A_LBO, C::SBO),
+                                umma_desc_kmajor(b2 + s * 2 * C::B_LBO, C::B_LBO, C::SBO), idesc, s > 0 ? 1u : 0u);
+                }
+                tc_commit(&bar_mma[b]);
+            }
+            __syncwarp();
+            /* the previous chunk's MMAs are done with its package: refill that slot */
+            if (c >= 1 && c - 1 + LT_NPKG < nchunk) {
+                if (!wait(&bar_mma[(c - 1) & 1], (uint32_t)(((c - 1) >> 1) & 1))) break;
+                fence_async_smem();
+                copy_pkg(c - 1 + LT_NPKG);
             }
         }
-    };
-    auto fold = [&](double &prod, int64_t &ex) {   /* move the exponent into the integer */
-        const int64_t bits = __double_as_longlong(prod);
-        ex += ((bits >> 52) & 0x7FF) - 1023;
-        prod = __longlong_as_double((bits & ~(0x7FFLL << 52)) | (1023LL << 52));
-    };
-    if (nchunk > 0) {
-        load(ia);
-        store(0);
+    } else {
+        /* ---------------------------------------------------------------- producer warps */
+        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        auto gload = [&](int c) -> uint2 {
+            return valid ? __ldg((const uint2 *)(bed + (size_t)j * pitch + (size_t)((ia + (int64_t)c * LT_IC) / 4)))
+                         : make_uint2(0x55555555u, 0x55555555u);
+        };
+        uint2 gcur = make_uint2(0x55555555u, 0x55555555u), gnext = gcur;
+        if (nchunk > 0) gcur = gload(0);
+        if (nchunk > 1) gnext = gload(1);
+        double prod = 1.0;
+        int64_t ex = 0;
+        for (int c = 0; c < nchunk && ok; ++c) {
+            const int b = c & 1;
+            if (!wait(&bar_mma[b], (uint32_t)((c >> 1) & 1))) break;
+            tc_fence_after_sync();
 #pragma unroll
-        for (int t = 0; t < ML_JT; ++t) g[t] = gnext[t];
-    }
-    if (nchunk > 1) load(ia + ML_IC);
-    __syncthreads();
-    double prod[ML_JT];
-    int64_t ex[ML_JT];
-#pragma unroll
-    for (int t = 0; t < ML_JT; ++t) { prod[t] = 1.0; ex[t] = 0; }
-    for (int c = 0; c < nchunk; ++c) {
-        const int s = c & 1;
-        uint4 gw[ML_JT];   /* the chunk's 4 code words per SNP, consumed from .x and shifted down */
-#pragma unroll
-        for (int t = 0; t < ML_JT; ++t) gw[t] = g[t];
-#pragma unroll 1
-        for (int wd = 0; wd < 4; ++wd) {   /* 16 individuals per 32-bit code word */
-#pragma unroll
-            for (int m2l = 0; m2l < 4; ++m2l) {
-                const int m2 = 4 * wd + m2l;
-                /* qp of two individual pairs for both SNPs (one 16-byte broadcast load of q per k) */
-                float2 qpa[ML_JT], qpb[ML_JT];
-#pragma unroll
-                for (int t = 0; t < ML_JT; ++t) qpa[t] = qpb[t] = make_float2(0.f, 0.f);
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    const float4 qv = Qs[s][k][m2];
-#pragma unroll
-                    for (int t = 0; t < ML_JT; ++t) {
-                        qpa[t] = __ffma2_rn(make_float2(qv.x, qv.y), pd[t][k], qpa[t]);
-                        qpb[t] = __ffma2_rn(make_float2(qv.z, qv.w), pd[t][k], qpb[t]);
-                    }
+            for (int h = 0; h < 2; ++h) {   /* individuals 16h .. 16h+15 of the chunk */
+                uint32_t ra[16], rb[16];
+                tmem_ld16_raw(tmem + lane_base + (uint32_t)(b * 2 * LT_IC + 16 * h), ra);
+                tmem_ld16_raw(tmem + lane_base + (uint32_t)(b * 2 * LT_IC + LT_IC + 16 * h), rb);
+                tmem_wait_ld();
+                if (h == 1) {   /* buffer b is read: the controller may reuse it for chunk c+2 */
+                    tc_fence_before_sync();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bar_free[b]);
                 }
+                const uint32_t w = h ? gcur.y : gcur.x;   /* 16 individuals' codes, 2 bits each */
 #pragma unroll
-                for (int t = 0; t < ML_JT; ++t) {
-                    float2 fa, fb;   /* (first, second) cell factors of pair a (hm = 0) and pair b */
+                for (int m4 = 0; m4 < 4; ++m4) {   /* 4 cells per step: two pairs */
+                    float f[4];
 #pragma unroll
                     for (int hm = 0; hm < 2; ++hm) {
-                        /* the pair's 4 code bits, tested in place in their 32-bit word */
-                        const uint32_t w = gw[t].x;
-                        const int b = 4 * (2 * m2l + hm);
-                        const float2 qp = hm ? qpb[t] : qpa[t];
-                        /* 1 - qp as the reference forms it (one rounding), from the unbiased FP32 qp */
-                        const float2 om = __ffma2_rn(qp, make_float2(-1.f, -1.f), make_float2(1.f, 1.f));
-                        /* factor per code: 00 -> om^2, 01 -> 1 (missing), 10 -> qp om, 11 -> qp^2;
-                         * the three products are formed for both cells and one is selected */
+                        const int e = 4 * m4 + 2 * hm;   /* the pair's first individual in this half */
+                        const float2 l01 = make_float2(__uint_as_float(ra[e]), __uint_as_float(ra[e + 1]));
+                        const float2 l2 = make_float2(__uint_as_float(rb[e]), __uint_as_float(rb[e + 1]));
+                        const float2 qp = __fadd2_rn(l01, l2);
+                        const float2 om = __fadd2_rn(__ffma2_rn(l01, make_float2(-1.f, -1.f), make_float2(1.f, 1.f)),
+                                                     make_float2(-l2.x, -l2.y));
                         const float2 oo = __fmul2_rn(om, om), qo = __fmul2_rn(qp, om), qq = __fmul2_rn(qp, qp);
-                        const bool lo0 = (w >> b) & 1u, hi0 = (w >> (b + 1)) & 1u;
-                        const bool lo1 = (w >> (b + 2)) & 1u, hi1 = (w >> (b + 3)) & 1u;
-                        const float f0 = hi0 ? (lo0 ? qq.x : qo.x) : (lo0 ? 1.f : oo.x);
-                        const float f1 = hi1 ? (lo1 ? qq.y : qo.y) : (lo1 ? 1.f : oo.y);
-                        if (hm) fb = make_float2(f0, f1);
-                        else fa = make_float2(f0, f1);
+                        const int bp = 2 * e;   /* this pair's 4 code bits in w */
+                        const bool lo0 = (w >> bp) & 1u, hi0 = (w >> (bp + 1)) & 1u;
+                        const bool lo1 = (w >> (bp + 2)) & 1u, hi1 = (w >> (bp + 3)) & 1u;
+                        f[2 * hm] = hi0 ? (lo0 ? qq.x : qo.x) : (lo0 ? 1.f : oo.x);
+                        f[2 * hm + 1] = hi1 ? (lo1 ? qq.y : qo.y) : (lo1 ? 1.f : oo.y);
                     }
-                    /* the two pairs' products f0 f1 in one paired multiply, each into the FP64 product */
-                    const float2 ff = __fmul2_rn(make_float2(fa.x, fb.x), make_float2(fa.y, fb.y));
-                    prod[t] *= (double)ff.x;
-                    prod[t] *= (double)ff.y;
+                    /* each pair's product (factors >= 1e-10 inside the projections' bounds: >= 1e-20,
+                     * normal in FP32), then into the FP64 running product */
+                    const float2 ff = __fmul2_rn(make_float2(f[0], f[2]), make_float2(f[1], f[3]));
+                    prod *= (double)ff.x;
+                    prod *= (double)ff.y;
                 }
+                /* 16 cells: a product >= 1e-160 stays normal; move its exponent into the integer */
+                const int64_t bits = __double_as_longlong(prod);
+                ex += ((bits >> 52) & 0x7FF) - 1023;
+                prod = __longlong_as_double((bits & ~(0x7FFLL << 52)) | (1023LL << 52));
             }
-            /* 8 pairs per word: each pair's factor is >= 1e-20, so the product stays normal */
-#pragma unroll
-            for (int t = 0; t < ML_JT; ++t) {
-                fold(prod[t], ex[t]);
-                gw[t] = make_uint4(gw[t].y, gw[t].z, gw[t].w, 0u);
+            if (c + 1 < nchunk) {
+                gcur = gnext;
+                if (c + 2 < nchunk) gnext = gload(c + 2);
             }
         }
-        if (c + 1 < nchunk) {
-            store(s ^ 1);
-#pragma unroll
-            for (int t = 0; t < ML_JT; ++t) g[t] = gnext[t];
-            if (c + 2 < nchunk) load(ia + (int64_t)(c + 2) * ML_IC);
-        }
-        __syncthreads();
+        if (valid) ll = log(prod) + (double)ex * 0.69314718055994530942;
     }
-    double ll = 0.0;
-#pragma unroll
-    for (int t = 0; t < ML_JT; ++t)
-        if (valid[t]) ll += log(prod[t]) + (double)ex[t] * 0.69314718055994530942;
-    for (int o = 16; o > 0; o >>= 1) ll += __shfl_down_sync(0xffffffffu, ll, o);
-    if ((tid & 31) == 0) red[tid >> 5] = ll;
+    /* every role is past its loop; after a failure give MMAs and copies in flight a bounded moment */
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == 128) {
+        for (int b = 0; b < 2; ++b) { mbar_wait_bounded(&bar_mma[b], 0u, 1024u); mbar_wait_bounded(&bar_mma[b], 1u, 1024u); }
+        for (int b = 0; b < LT_NPKG; ++b) { mbar_wait_bounded(&bar_p[b], 0u, 1024u); mbar_wait_bounded(&bar_p[b], 1u, 1024u); }
+    }
+    if (producer) {
+        for (int o = 16; o > 0; o >>= 1) ll += __shfl_down_sync(0xffffffffu, ll, o);
+        if (lane == 0) red[warp] = ll;
+    }
+    tc_fence_before_sync();
     __syncthreads();
-    if (tid == 0) partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = red[0] + red[1] + red[2] + red[3];
+    if (tid == 0)
+        partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] =
+            ok ? (red[0] + red[1]) + (red[2] + red[3]) : __longlong_as_double(0x7ff8000000000000LL);
+    if (warp == 4) tmem_dealloc_warp(tmem, C::NCOLS);
 }
 
 /* A bounded mbarrier wait that nothing completes: it gives up after `polls` polls and raises the
@@ -1138,6 +1444,7 @@ cudaError_t prepare_mixed_t()
     cudaError_t e = cudaFuncSetAttribute(k_sweep_q_mixed<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MQ<K>::SMEM);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_sweep_p_mixed<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MP<K>::SMEM);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_sweep_p_mixed<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MP<K>::SMEM);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_loglik_mixed<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LT<K>::SMEM);
     return e;
 }
 
@@ -1187,12 +1494,21 @@ cudaError_t launch_ll_mixed_t(const uint8_t *bed, int64_t I, int64_t J, int64_t 
                               const double *p, const SweepPlan &pl, double *partial, double *out, int *err,
                               uint8_t *pkg, cudaStream_t st)
 {
-    (void)err;
-    (void)pkg;
+    k_ll_pack<K><<<(unsigned)((I + LT_IC - 1) / LT_IC), 128, 0, st>>>(q, I, pkg);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     dim3 grid((unsigned)pl.gx, (unsigned)pl.S);
-    k_loglik_mixed<K><<<grid, 128, 0, st>>>(bed, I, J, pitch, q, p, pl.slice, partial);
+    k_loglik_mixed<K><<<grid, LT_CTA, LT<K>::SMEM, st>>>(bed, I, J, pitch, p, pkg, pl.slice, partial, err);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     k_sum_partials_mixed<<<1, 1024, 0, st>>>(partial, (int64_t)pl.gx * pl.S, out);
     return cudaGetLastError();
+}
+
+template <int K>
+size_t ll_pkg_bytes_t(int64_t I)
+{
+    return (size_t)((I + LT_IC - 1) / LT_IC) * LT<K>::PKG;
 }
 
 /* Slices over the second axis for CTAs of 128 rows, `per_sm` of which are resident per SM.  CTAs
@@ -1235,7 +1551,7 @@ int resident_t(int kind)
     cudaError_t e;
     if (kind == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_q_mixed<K>, MQ_CTA, MQ<K>::SMEM);
     else if (kind == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_p_mixed<K, false>, MP_CTA, MP<K>::SMEM);
-    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_loglik_mixed<K>, 128, 0);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_loglik_mixed<K>, LT_CTA, LT<K>::SMEM);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -1278,10 +1594,10 @@ SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax)
     return plan_rows(J, I, sms, resident(1, K, 3), MP_IC, smax);
 }
 
+/* One CTA per 128 SNPs and individual slice (slices are multiples of 32 individuals). */
 SweepPlan plan_loglik_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax)
 {
-    /* CTAs of 128 threads x ML_JT SNPs */
-    return plan_rows((J + ML_JT - 1) / ML_JT, I, sms, resident(2, K, 4), ML_IC, smax);
+    return plan_rows(J, I, sms, resident(2, K, 4), LT_IC, smax);
 }
 
 cudaError_t launch_sweep_q_mixed(int K, const uint8_t *bed, int64_t I, int64_t J, int64_t pitch, const double *q,
@@ -1320,6 +1636,13 @@ size_t sweep_p_mixed_pkg_bytes(int K, int64_t I)
 {
     size_t b = 0;
     ADMIX_DISPATCH_K(K, b = p_pkg_bytes_t<KK>(I));
+    return b;
+}
+
+size_t loglik_mixed_pkg_bytes(int K, int64_t I)
+{
+    size_t b = 0;
+    ADMIX_DISPATCH_K(K, b = ll_pkg_bytes_t<KK>(I));
     return b;
 }
 

@@ -124,23 +124,20 @@ def test_init_em_and_sqp_updates_match_oracle(oa, orc, K, flags):
     st_qo = r.update_q(False)
     assert np.max(np.abs(d.x_next[: g.I] - r.x_next[: g.I])) < 1e-9
     # The device QPs are the oracle's QPs: run on the sums the device update used, the oracle's
-    # quadratic_program! returns the device's status for every problem.  A status can differ from
-    # the oracle's own run only where the two FP64 sweeps (different summation orders, equal to
-    # ~1e-15) put a problem on the other side of an active-set test; each such problem is
-    # accounted for by that check.
+    # quadratic_program! returns the device's status for every problem; and the statuses equal
+    # the oracle's own run (the two FP64 sweeps' sums differ only at ~1e-15, which moved no
+    # problem across an active-set test here).
     H, z = d_cu.grad_hess_q(oa.X, oa.X)
     st_chk, _ = orc.qp_batch(H, z, d.x[: g.I], True, mu_mode=flags & 1)
     assert np.array_equal(st_q, st_chk), np.flatnonzero(st_q != st_chk)
-    assert np.mean(st_q == st_qo) > 0.99
+    assert np.array_equal(st_q, st_qo), np.flatnonzero(st_q != st_qo)
     st_p = oa.update_p(d, g, False, d_cu=d_cu)
     st_po = r.update_p(False)
     assert np.max(np.abs(d.x_next[g.I:] - r.x_next[g.I:])) < 1e-9
     H, z = d_cu.grad_hess_p(oa.X_NEXT, oa.X)
     st_chk, _ = orc.qp_batch(H, z, d.x[g.I:], False, mu_mode=flags & 1)
     assert np.array_equal(st_p, st_chk), np.flatnonzero(st_p != st_chk)
-    assert np.mean(st_p == st_po) > 0.99
-    print(f"QP_STATUS K={K} flags={flags}: Q {int(np.sum(st_q != st_qo))}/{g.I} and "
-          f"P {int(np.sum(st_p != st_po))}/{g.J} statuses differ from the oracle's own run")
+    assert np.array_equal(st_p, st_po), np.flatnonzero(st_p != st_po)
     d_cu.close()
 
 

@@ -146,8 +146,8 @@ def _world(oa, name, I, J, K, seed, world):
 
 def test_learned_start_beats_random_start(oa, ws):
     """Train on 8 small cohorts of one world, then solve a held-out cohort of that world: the
-    learned start reaches within 1e-6 (relative) of the FP64 optimum in fewer iterations than
-    5 EM iterations + QN from the random start."""
+    learned start reaches within 1e-6 (relative) of the FP64 optimum with fewer genotype passes
+    than 5 EM iterations + QN from the random start."""
     import torch
     I, J, K, world = 3000, 4000, 3, 31
     snps = ws.sketch_snps(J, S=1024, seed=5)
@@ -177,9 +177,14 @@ def test_learned_start_beats_random_start(oa, ws):
     t_pred = time.perf_counter() - t0
     learned = ws.run_to_target(g, K, rng=1, start=start, target=target)
     assert rand["iterations_to_target"] is not None and learned["iterations_to_target"] is not None
-    # time to the target: the learned arm pays the sketch, the encoder and the P step, the random
-    # arm its 5 EM iterations (both inside seconds_to_target / predict time)
-    assert learned["seconds_to_target"] + t_pred < rand["seconds_to_target"], (learned, rand, t_pred)
+    # Work to the target in passes over the genotypes (at this size a QN iteration takes well under
+    # a millisecond, so wall time is launch noise; test_committed_model_gain compares seconds):
+    # a QN iteration is 6 passes (4 sweeps, 2 log-likelihoods), an EM iteration 3 (2 sweeps and
+    # its log-likelihood), the learned start 1 (the closed-form P step; sketch and encoder read
+    # 4096 SNPs).  The learned arm must need strictly fewer.
+    work_learned = 6 * learned["iterations_to_target"] + 1
+    work_rand = 3 * 5 + 6 * rand["iterations_to_target"]
+    assert work_learned < work_rand, (learned["iterations_to_target"], rand["iterations_to_target"], t_pred)
     # the learned start ends at the same optimum
     assert abs(learned["ll"] - plain["ll"]) <= 1e-6 * abs(plain["ll"])
 
