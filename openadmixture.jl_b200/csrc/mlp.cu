@@ -12,6 +12,14 @@
  * Network: x = [d - 2f | proj] (S + R) -> ReLU(W1 x + b1) (H) -> ReLU(W2 . + b2) (H) ->
  * softmax(W3 . + b3) (K).  Loss: cross-entropy against soft targets (aligned converged Q).
  * All matrices are row-major FP32 (W1: (S+R) x H, W2: H x H, W3: H x K).
+ *
+ * Every product of the forward and backward passes is one tensor-core GEMM (k_gemm_tc): a CTA
+ * owns a 128 x 64 tile of the output in TMEM; each 32-deep slice of the reduction is loaded by
+ * the CTA's threads through an operand functor (dense, transposed, or the network input built
+ * on the fly from the dosages), split into BF16 high and low parts, and multiplied as
+ * hi*hi + lo*hi + hi*lo by tcgen05 (about 2^-17 relative per product, FP32 accumulation).  The
+ * accumulator restarts every 128 of the reduction and the threads add it into FP32 registers,
+ * so no FP32 partial sees more than 24 of the tensor core's accumulations.
  */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -19,6 +27,7 @@
 #include "../../include/admix.h"
 #include "common.cuh"
 #include "synth.h"
+#include "tc05.cuh"
 
 namespace {
 
@@ -120,66 +129,184 @@ struct LoadXT {                    /* the input transposed: (k, m) */
     __device__ float operator()(int64_t k, int64_t m) const { return x(m, k); }
 };
 
-constexpr int GB_M = 64, GB_N = 64, GB_K = 16;
+constexpr int GT_M = 128, GT_N = 64, GT_K = 32;   /* output tile rows x columns, reduction slice */
+constexpr int GT_D = 4;                             /* slices per fresh accumulation */
+constexpr uint32_t GT_WAIT = 1u << 22;              /* polls of a bounded wait */
+/* one stage: A hi, A lo (128 x 32 BF16, K-major core matrices), B hi, B lo (64 x 32) */
+constexpr uint32_t GT_A = GT_M * GT_K * 2, GT_B = GT_N * GT_K * 2;
+constexpr uint32_t GT_STAGE = 2 * GT_A + 2 * GT_B;
+constexpr uint32_t GT_SMEM = 2 * GT_STAGE + 1024;
+constexpr uint32_t GT_A_LBO = GT_M * 16, GT_B_LBO = GT_N * 16;
+
+/* v = hi + lo, both BF16 (hi rounded to nearest, lo the BF16 of the remainder) */
+__device__ __forceinline__ void split_bf16(float v, uint32_t &hi, uint32_t &lo)
+{
+    hi = pack_bf16x2(v, 0.f) & 0xFFFFu;
+    lo = pack_bf16x2(v - __uint_as_float(hi << 16), 0.f) & 0xFFFFu;
+}
 
 /* C[m, n] = alpha * sum_k A(m, k) B(k, n) (+ bias[n]); relu if act; times [mask(m, n) > 0] if mask.
- * 256 threads, 64 x 64 tile, 4 x 4 outputs per thread, FP32 accumulation. */
+ * 128 threads, one 128 x 64 output tile per CTA (thread = output row = TMEM lane).  Two smem
+ * stages: the threads load slice c+1 while the tensor core multiplies slice c.  Every wait is
+ * bounded; a CTA whose wait runs out writes NaN into its tile (the failure shows in the loss). */
 template <class LA, class LB>
-__global__ void __launch_bounds__(256)
-k_gemm(LA A, LB B, int64_t M, int64_t N, int64_t Kd, float alpha, const float *__restrict__ bias, int act,
-       const float *__restrict__ mask, float *__restrict__ C, int64_t ldc)
+__global__ void __launch_bounds__(128)
+k_gemm_tc(LA A, LB B, int64_t M, int64_t N, int64_t Kd, float alpha, const float *__restrict__ bias, int act,
+          const float *__restrict__ mask, float *__restrict__ C, int64_t ldc)
 {
-    __shared__ float As[GB_K][GB_M + 4];
-    __shared__ float Bs[GB_K][GB_N + 4];
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const int64_t m0 = (int64_t)blockIdx.y * GB_M, n0 = (int64_t)blockIdx.x * GB_N;
-    float acc[4][4] = {};
-    for (int64_t k0 = 0; k0 < Kd; k0 += GB_K) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int e = tid + u * 256;              /* 1024 elements of each 64 x 16 tile */
-            const int am = e >> 4, ak = e & 15;
-            const int64_t gm = m0 + am, gk = k0 + ak;
-            As[ak][am] = (gm < M && gk < Kd) ? A(gm, gk) : 0.f;
-            const int bk = e >> 6, bn = e & 63;
-            const int64_t gk2 = k0 + bk, gn = n0 + bn;
-            Bs[bk][bn] = (gk2 < Kd && gn < N) ? B(gk2, gn) : 0.f;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < GB_K; ++kk) {
-            float a[4], b[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) { a[r] = As[kk][ty * 4 + r]; b[r] = Bs[kk][tx * 4 + r]; }
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a[r], b[c], acc[r][c]);
-        }
-        __syncthreads();
+    extern __shared__ __align__(1024) uint8_t smraw[];
+    uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    __shared__ uint64_t bar[2];          /* MMAs of the slice in stage s done */
+    __shared__ uint32_t tmem_holder;
+    __shared__ volatile int abort_flag;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int64_t m0 = (int64_t)blockIdx.y * GT_M, n0 = (int64_t)blockIdx.x * GT_N;
+    if (warp == 0) tmem_alloc_warp(&tmem_holder, GT_N);
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        abort_flag = 0;
+        mbar_fence_init();
     }
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tmem = tmem_holder;
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    bool ok = true;
+    auto wait = [&](uint64_t *b, uint32_t parity) {
+        if (!ok) return;
+        for (uint32_t n = 0; n < GT_WAIT; ++n) {
+            if (mbar_try_wait(b, parity)) return;
+            if ((n & 255u) == 255u && abort_flag) break;
+        }
+        ok = false;
+        abort_flag = 1;
+    };
+    float acc[GT_N];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const int64_t m = m0 + ty * 4 + r;
-        if (m >= M) continue;
+    for (int n = 0; n < GT_N; ++n) acc[n] = 0.f;
+    auto drain = [&]() {   /* the finished accumulation block into the FP32 registers */
+        tc_fence_after_sync();
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int64_t n = n0 + tx * 4 + c;
-            if (n >= N) continue;
-            float v = alpha * acc[r][c] + (bias ? bias[n] : 0.f);
+        for (int c0 = 0; c0 < GT_N; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + lane_base + (uint32_t)c0, v);
+#pragma unroll
+            for (int e = 0; e < 16; ++e) acc[c0 + e] += v[e];
+        }
+    };
+    const int nch = (int)((Kd + GT_K - 1) / GT_K);
+    constexpr uint32_t idesc = idesc_bf16_f32(GT_M, GT_N);
+    for (int c = 0; c < nch; ++c) {
+        const int st = c & 1;
+        uint8_t *Ah = sm + st * GT_STAGE, *Al = Ah + GT_A, *Bh = Al + GT_A, *Bl = Bh + GT_B;
+        if (c >= 2) wait(&bar[st], (uint32_t)(((c - 2) >> 1) & 1));   /* stage st is free again */
+        const int64_t k0 = (int64_t)c * GT_K;
+        /* A: thread t loads row m0 + t of the slice, 4 granules of 8 */
+        {
+            const int64_t m = m0 + tid;
+#pragma unroll
+            for (int gr = 0; gr < GT_K / 8; ++gr) {
+                uint32_t h[4], l[4];
+#pragma unroll
+                for (int e = 0; e < 8; e += 2) {
+                    const int64_t ka = k0 + 8 * gr + e;
+                    const float v0 = (m < M && ka < Kd) ? A(m, ka) : 0.f;
+                    const float v1 = (m < M && ka + 1 < Kd) ? A(m, ka + 1) : 0.f;
+                    uint32_t h0, l0, h1, l1;
+                    split_bf16(v0, h0, l0);
+                    split_bf16(v1, h1, l1);
+                    h[e / 2] = h0 | (h1 << 16);
+                    l[e / 2] = l0 | (l1 << 16);
+                }
+                *(uint4 *)(Ah + gr * GT_A_LBO + 16 * tid) = make_uint4(h[0], h[1], h[2], h[3]);
+                *(uint4 *)(Al + gr * GT_A_LBO + 16 * tid) = make_uint4(l[0], l[1], l[2], l[3]);
+            }
+        }
+        /* B: 64 columns x 4 granules = 256 tasks, two per thread; B row n holds B(k, n0 + n) */
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int task = tid + 128 * u;
+            const int n = task & (GT_N - 1), gr = task >> 6;
+            const int64_t col = n0 + n;
+            uint32_t h[4], l[4];
+#pragma unroll
+            for (int e = 0; e < 8; e += 2) {
+                const int64_t ka = k0 + 8 * gr + e;
+                const float v0 = (col < N && ka < Kd) ? B(ka, col) : 0.f;
+                const float v1 = (col < N && ka + 1 < Kd) ? B(ka + 1, col) : 0.f;
+                uint32_t h0, l0, h1, l1;
+                split_bf16(v0, h0, l0);
+                split_bf16(v1, h1, l1);
+                h[e / 2] = h0 | (h1 << 16);
+                l[e / 2] = l0 | (l1 << 16);
+            }
+            *(uint4 *)(Bh + gr * GT_B_LBO + 16 * n) = make_uint4(h[0], h[1], h[2], h[3]);
+            *(uint4 *)(Bl + gr * GT_B_LBO + 16 * n) = make_uint4(l[0], l[1], l[2], l[3]);
+        }
+        fence_async_smem();
+        if (c > 0 && c % GT_D == 0) {   /* the block ending at slice c-1: its MMAs done, into registers */
+            wait(&bar[(c - 1) & 1], (uint32_t)(((c - 1) >> 1) & 1));
+            if (ok) drain();
+        }
+        tc_fence_before_sync();
+        __syncthreads();
+        tc_fence_after_sync();
+        if (tid == 0 && ok) {
+            const uint32_t ah = smem_u32(Ah), al = smem_u32(Al), bh = smem_u32(Bh), bl = smem_u32(Bl);
+#pragma unroll
+            for (int ks = 0; ks < GT_K / 16; ++ks) {
+                const uint32_t ao = ks * 2 * GT_A_LBO, bo = ks * 2 * GT_B_LBO;
+                const uint32_t fresh = (c % GT_D == 0 && ks == 0) ? 0u : 1u;
+                tc_mma_bf16(tmem, umma_desc_kmajor(ah + ao, GT_A_LBO, 128), umma_desc_kmajor(bh + bo, GT_B_LBO, 128),
+                            idesc, fresh);
+                tc_mma_bf16(tmem, umma_desc_kmajor(al + ao, GT_A_LBO, 128), umma_desc_kmajor(bh + bo, GT_B_LBO, 128),
+                            idesc, 1u);
+                tc_mma_bf16(tmem, umma_desc_kmajor(ah + ao, GT_A_LBO, 128), umma_desc_kmajor(bl + bo, GT_B_LBO, 128),
+                            idesc, 1u);
+            }
+            tc_commit(&bar[st]);
+        }
+    }
+    if (nch > 0) {   /* the last block */
+        wait(&bar[(nch - 1) & 1], (uint32_t)(((nch - 1) >> 1) & 1));
+        if (ok) drain();
+    }
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == 0) {   /* give MMAs still in flight a bounded moment before the TMEM goes */
+        mbar_wait_bounded(&bar[0], 0u, 1024u); mbar_wait_bounded(&bar[0], 1u, 1024u);
+        mbar_wait_bounded(&bar[1], 0u, 1024u); mbar_wait_bounded(&bar[1], 1u, 1024u);
+    }
+    const int64_t m = m0 + tid;
+    if (m < M) {
+#pragma unroll
+        for (int n = 0; n < GT_N; ++n) {
+            const int64_t col = n0 + n;
+            if (col >= N) break;
+            float v = alpha * acc[n] + (bias ? bias[col] : 0.f);
             if (act) v = fmaxf(v, 0.f);
-            if (mask && !(mask[m * ldc + n] > 0.f)) v = 0.f;
-            C[m * ldc + n] = v;
+            if (mask && !(mask[m * ldc + col] > 0.f)) v = 0.f;
+            C[m * ldc + col] = ok ? v : __int_as_float(0x7fc00000);
         }
     }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc_warp(tmem, GT_N);
 }
 
 template <class LA, class LB>
 cudaError_t gemm(LA A, LB B, int64_t M, int64_t N, int64_t Kd, float alpha, const float *bias, int act,
                  const float *mask, float *C, int64_t ldc, cudaStream_t st)
 {
-    dim3 grid((unsigned)((N + GB_N - 1) / GB_N), (unsigned)((M + GB_M - 1) / GB_M));
-    k_gemm<LA, LB><<<grid, 256, 0, st>>>(A, B, M, N, Kd, alpha, bias, act, mask, C, ldc);
+    static bool ready = false;   /* the kernel's dynamic shared memory limit, set once per instantiation */
+    if (!ready) {
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<LA, LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GT_SMEM);
+        if (e != cudaSuccess) return e;
+        ready = true;
+    }
+    dim3 grid((unsigned)((N + GT_N - 1) / GT_N), (unsigned)((M + GT_M - 1) / GT_M));
+    k_gemm_tc<LA, LB><<<grid, 128, GT_SMEM, st>>>(A, B, M, N, Kd, alpha, bias, act, mask, C, ldc);
     return cudaGetLastError();
 }
 
