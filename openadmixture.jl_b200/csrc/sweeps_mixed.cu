@@ -614,9 +614,9 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
  * chunks of 32 individuals.  Per chunk:
  *   qp, om     D[128 x 32] = Ptile * Qchunk^T and (1-P)tile * Qchunk^T, TF32 split form;
  *   Hessian    D[128 x N] += C * QQ^T in BF16, C = nm (g/qp^2 + (2-g)/(1-qp)^2);
- *   diag/grad  D[128 x NDG] = C * [q^2]^T (the Hessian diagonal) and sum_{a+b<=2} DZa * [q_b]^T
- *              (the gradient sum_i dz q_k, dz = nm (g/qp - (2-g)/(1-qp)), both factors in three
- *              BF16 limbs because the sum cancels), afresh every chunk and added into FP64;
+ *   diag/grad  D[128 x NDG] = C * [q^2]^T (the Hessian diagonal) and
+ *              [dz_hi | dz_lo | dz_hi] * [q_hi ; q_hi ; q_lo]^T (the gradient sum_i dz q_k,
+ *              dz = nm (g/qp - (2-g)/(1-qp))), afresh every chunk and added into FP64;
  * and per cell on the CUDA cores the code (from the thread's own genotype word), one reciprocal,
  * C, dz and its BF16 split.  The Q-derived tiles of each chunk (QQ in BF16, Q split into TF32
  * hi / lo, the diagonal and gradient B blocks, q in FP32 for the EM mode) are built once per
@@ -624,7 +624,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
 
 constexpr int MP_IC = 32;          /* individuals per chunk = 2 BF16 MMA K-steps */
 constexpr int MP_THREADS = 128;    /* one thread per SNP = accumulator row */
-constexpr int MP_NPKG = 2;
+constexpr int MP_NPKG = 3;
 
 template <int K>
 struct MP {
@@ -636,20 +636,20 @@ struct MP {
     static constexpr uint32_t COL_DG = COL_H + N;               /* [diag | grad] accumulator */
     static constexpr uint32_t NCOLS = tmem_cols_for(COL_DG + NDG);
     static constexpr int E = T + K;
-    static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* one BF16 A tile (C, DZ0, DZ1, DZ2): 8 KB */
+    static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* one BF16 A tile (C, DZ0, DZ1): 8 KB */
     static constexpr uint32_t B_BYTES = N * MP_IC * 2;          /* BF16 QQ tile */
     static constexpr uint32_t PA_BYTES = 128 * 2 * KP * 4;      /* TF32 P tile [hi | lo] (and 1-P) */
     static constexpr uint32_t QB_BYTES = MP_IC * 2 * KP * 4;    /* TF32 Q chunk [hi | lo] */
     static constexpr uint32_t DGB_BYTES = NDG * MP_IC * 2;      /* one BF16 B block of the [diag | grad] MMA */
     static constexpr int QS = MP_IC + 4;                        /* FP32 q row stride (floats) */
-    /* package: [QQ | TF32 Q | FP32 q (EM mode) | 1 - sum q | diag q^2 | grad q limbs 0, 1, 2] */
+    /* package: [QQ | TF32 Q | FP32 q (EM mode) | 1 - sum q | diag q^2 | grad q hi | grad q lo] */
     static constexpr uint32_t PK_QB = B_BYTES;
     static constexpr uint32_t PK_QF = PK_QB + QB_BYTES;
     static constexpr uint32_t PK_S = PK_QF + K * QS * 4;         /* 1 - sum_k q_k per individual */
     static constexpr uint32_t PK_DG = PK_S + MP_IC * 4;
-    static constexpr uint32_t PKG = PK_DG + 4 * DGB_BYTES;
-    static constexpr uint32_t OFF_A = 0;                        /* C, DZ0, DZ1, DZ2 */
-    static constexpr uint32_t OFF_PKG = 4 * A_BYTES;
+    static constexpr uint32_t PKG = PK_DG + 3 * DGB_BYTES;
+    static constexpr uint32_t OFF_A = 0;                        /* C, DZ0, DZ1 */
+    static constexpr uint32_t OFF_PKG = 3 * A_BYTES;
     static constexpr uint32_t OFF_PA = OFF_PKG + MP_NPKG * PKG; /* P tile, then (1-P) tile */
     static constexpr uint32_t OFF_TAB = OFF_PA + 2 * PA_BYTES;
     static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024;
@@ -690,18 +690,15 @@ k_p_pack(const double *__restrict__ q, int64_t I, uint8_t *__restrict__ pkg)
         tf32_split(a, h, l);
         *(float *)(buf + C::PK_QB + kmaj_off(ii, k, C::QB_LBO)) = h;
         *(float *)(buf + C::PK_QB + kmaj_off(ii, C::KP + k, C::QB_LBO)) = l;
-        /* [diag | grad] B blocks: element (row n, individual ii) at granule ii / 8, half-word ii % 8;
-         * the gradient's q in three BF16 limbs split from the FP64 value (q to about 2^-25) */
+        /* [diag | grad] B blocks: element (row n, individual ii) at granule ii / 8, half-word ii % 8 */
         uint16_t *dg = (uint16_t *)(buf + C::PK_DG + bblk_off(k, ii >> 3, C::DG_LBO)) + (ii & 7);
+        uint16_t *g0 = (uint16_t *)(buf + C::PK_DG + C::DGB_BYTES + bblk_off(C::GOFF + k, ii >> 3, C::DG_LBO)) + (ii & 7);
+        uint16_t *g1 = (uint16_t *)(buf + C::PK_DG + 2 * C::DGB_BYTES + bblk_off(C::GOFF + k, ii >> 3, C::DG_LBO)) + (ii & 7);
         *dg = (uint16_t)(pack_bf16x2(a * a, 0.f) & 0xFFFFu);
-        double r = (ic + ii < I) ? q[(size_t)K * ic + t] : 1.0 / K;
-#pragma unroll
-        for (int l = 0; l < 3; ++l) {
-            const uint32_t h = pack_bf16x2((float)r, 0.f) & 0xFFFFu;
-            *((uint16_t *)(buf + C::PK_DG + (1 + l) * C::DGB_BYTES + bblk_off(C::GOFF + k, ii >> 3, C::DG_LBO)) + (ii & 7)) =
-                (uint16_t)h;
-            r -= (double)__uint_as_float(h << 16);
-        }
+        uint16_t hi, lo;
+        bf16_split(a, hi, lo);
+        *g0 = hi;
+        *g1 = lo;
     }
     __syncthreads();
     /* QQ tile: task (kc, nn) writes pair nn's 8 individuals of k-chunk kc at kc*16N + 16nn */
@@ -767,19 +764,17 @@ __device__ __forceinline__ uint2 col_load32(const uint8_t *__restrict__ bed, int
  * (rows of 2K, the FP64 EM sweep's layout, finalised by k_emp_finalize), with no Hessian tile,
  * MMAs or drains; a package slot is handed back once the four producer warps have read it. */
 /* The chunk's [diag | grad] MMAs of the P side (one thread), a fresh sum into COL_DG..:
- *   diag:  C x [q^2 block]                                                    (2 K-steps)
- *   grad:  sum over limb pairs (a, b) with a + b <= 2 of DZa x [q limb b]    (12 K-steps)
- * The P-side gradient sum_i dz q_k cancels (dz changes sign), so both factors carry three
- * BF16 limbs: the products kept are exact to about 2^-25 relative, like FP32 terms.
- * a_base: the A tiles C, DZ0, DZ1, DZ2 (A_BYTES apart); b_base: the package's PK_DG blocks. */
+ *   diag:  C x [q^2 block]                                                (2 K-steps)
+ *   grad:  [DZ0 | DZ1 | DZ0] x [q hi block ; q hi block ; q lo block]   (6 K-steps)
+ * a_base: the A tiles C, DZ0, DZ1 (A_BYTES apart); b_base: the package's PK_DG blocks. */
 template <int K, uint32_t A_BYTES, uint32_t A_LBO, uint32_t DGB_BYTES, uint32_t DG_LBO>
 __device__ __forceinline__ void issue_dg_p(uint32_t tmem_dg, uint32_t a_base, uint32_t b_base)
 {
     constexpr uint32_t id = idesc_bf16_f32(128, DGShape<K>::NDG);
-    constexpr int AT[7] = {0, 1, 2, 1, 3, 2, 1};   /* A tile of each term: C, DZ0, DZ1, DZ0, DZ2, DZ1, DZ0 */
-    constexpr int BB[7] = {0, 1, 1, 2, 1, 2, 3};   /* B block of each term: q^2, q0, q0, q1, q0, q1, q2 */
+    constexpr int AT[4] = {0, 1, 2, 1};   /* A tile of each term: C, DZ0, DZ1, DZ0 */
+    constexpr int BB[4] = {0, 1, 1, 2};   /* B block of each term: q^2, q hi, q hi, q lo */
 #pragma unroll
-    for (int t = 0; t < 7; ++t) {
+    for (int t = 0; t < 4; ++t) {
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
             const uint64_t ad = umma_desc_kmajor(a_base + AT[t] * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
@@ -1003,7 +998,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     __syncwarp();
                     if (lane == 0) mbar_arrive(bar_qfree);
                 }
-                uint32_t cp[4], d0p[4], d1p[4], d2p[4];
+                uint32_t cp[4], d0p[4], d1p[4];
                 float2 zz[4], z2s[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
@@ -1026,22 +1021,18 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                         const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
                         const float2 dz = __ffma2_rn(z2, make_float2(-1.f, -1.f), z1);   /* nm (g/qp - (2-g)/(1-qp)) */
                         cp[e] = pack_bf16x2(cw.x, cw.y);
-                        /* dz in three BF16 limbs, each the rounding of what the previous ones leave
-                         * (the remainders are exact in FP32) */
+                        /* dz = hi + lo in BF16: hi rounded to nearest, lo the BF16 of the remainder */
                         const uint32_t h = pack_bf16x2(dz.x, dz.y);
-                        const float2 r1 = __fadd2_rn(dz, make_float2(-__uint_as_float(h << 16), -__uint_as_float(h & 0xFFFF0000u)));
-                        const uint32_t m1 = pack_bf16x2(r1.x, r1.y);
-                        const float2 r2 = __fadd2_rn(r1, make_float2(-__uint_as_float(m1 << 16), -__uint_as_float(m1 & 0xFFFF0000u)));
+                        const float2 hf = make_float2(__uint_as_float(h << 16), __uint_as_float(h & 0xFFFF0000u));
+                        const float2 lr = __fadd2_rn(dz, make_float2(-hf.x, -hf.y));
                         d0p[e] = h;
-                        d1p[e] = m1;
-                        d2p[e] = pack_bf16x2(r2.x, r2.y);
+                        d1p[e] = pack_bf16x2(lr.x, lr.y);
                     }
                 }
                 if constexpr (!EMS) {
                     *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
                     *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d0p[0], d0p[1], d0p[2], d0p[3]);
                     *(uint4 *)(At + 2 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d1p[0], d1p[1], d1p[2], d1p[3]);
-                    *(uint4 *)(At + 3 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d2p[0], d2p[1], d2p[2], d2p[3]);
                 } else {
 #pragma unroll
                 for (int k = 0; k < K; ++k) {

@@ -10,6 +10,7 @@ from conftest import rel_err
 pytestmark = pytest.mark.gpu
 
 GRAD_TOL = 1e-5
+P_GRAD_TOL = 1e-5       # of sum_i |dz q_k|, the P-side gradient's term magnitude
 HESS_TOL = 2e-2
 
 
@@ -66,13 +67,31 @@ def test_mixed_run_reaches_fp64_optimum(oa, K):
     assert rel_err(finals[1], finals[0]) < 1e-6
 
 
+def _p_grad_scale(g, q, p):
+    """sum_i |d l_ij / d p_jk| = sum_i nm |g/qp - (2-g)/(1-qp)| q_ik, the magnitude of the terms the
+    P-side gradient adds up (J, K): the scale its rounding error is measured against, since the sum
+    cancels and can be far smaller than its terms."""
+    codes = np.stack([(g.data >> (2 * s)) & 3 for s in range(4)], axis=2).reshape(g.J, -1)[:, : g.I]
+    gv = np.where(codes == 3, 2.0, np.where(codes == 2, 1.0, 0.0))
+    nm = codes != 1
+    qp = p @ q.T                                              # (J, I)
+    dz = np.where(nm, gv / qp - (2 - gv) / (1 - qp), 0.0)
+    return np.abs(dz) @ q                                     # (J, K)
+
+
 @pytest.mark.parametrize("K", [1, 2, 3, 5, 8, 12, 16])
 def test_mixed_p_sweep_matches_fp64(oa, K):
+    """The P-side gradient is a cancelling sum (dz changes sign with the genotype): its error is
+    bounded against the magnitude of its terms, P_GRAD_TOL * sum_i |dz q_k| (each term carries about
+    2^-17 relative from the two-part BF16 split); the Hessian against each row's largest entry."""
     g, d, h64, hmx = _pair(oa, I=1037, J=517, K=K, seed=80 + K)   # partial individual chunk and SNP tile
     H0, z0 = h64.grad_hess_p(oa.X, oa.X)
     H1, z1 = hmx.grad_hess_p(oa.X, oa.X)
     assert np.all(np.isfinite(H1)) and np.all(np.isfinite(z1))
-    assert _row_rel(z1, z0) < 1e-4
+    scale = _p_grad_scale(g, d.x[: g.I], d.x[g.I:])
+    assert np.max(np.abs(z1 - z0) / scale) < P_GRAD_TOL
+    if K > 1:
+        assert _row_rel(z1, z0) < 1e-4
     assert _row_rel(H1, H0) < HESS_TOL
     h64.close(); hmx.close()
 
