@@ -126,7 +126,7 @@ struct MQ {
     static constexpr int KP = ((K + 7) / 8) * 8;                /* TF32 K extent of the qp MMAs */
     static constexpr int QPN = 2 * MQ_JC;                       /* qp MMA N: the chunk's p rows, then 1-p rows */
     static constexpr int NDG = DGShape<K>::NDG, GOFF = DGShape<K>::GOFF;
-    static constexpr uint32_t COL_H = 2 * QPN;                  /* TMEM: two qp / om buffers, then the Hessian */
+    static constexpr uint32_t COL_H = 64;                       /* TMEM column of the Hessian accumulator */
     static constexpr uint32_t COL_DG = COL_H + N;               /* TMEM column of the [diag | grad] accumulator */
     static constexpr uint32_t NCOLS = tmem_cols_for(COL_DG + NDG);
     static constexpr int E = T + K;                             /* partial entries per individual */
@@ -141,9 +141,8 @@ struct MQ {
     static constexpr uint32_t PK_DG = PK_QB + QB_BYTES;
     static constexpr uint32_t PKG = PK_DG + 4 * DGB_BYTES;
     static constexpr uint32_t GBUF = MQ_JC * 32;                /* genotype bytes of one chunk */
-    static constexpr uint32_t A_STAGE = 4 * A_BYTES;            /* one A stage: W1, W2, DZ0, DZ1 tiles */
-    static constexpr uint32_t OFF_A = 0;                        /* two A stages */
-    static constexpr uint32_t OFF_PKG = 2 * A_STAGE;
+    static constexpr uint32_t OFF_A = 0;                        /* W1, W2, DZ0, DZ1 tiles */
+    static constexpr uint32_t OFF_PKG = 4 * A_BYTES;
     static constexpr uint32_t OFF_QA = OFF_PKG + MQ_NPKG * PKG;
     static constexpr uint32_t OFF_G = OFF_QA + QA_BYTES;        /* two G buffers, [pair][byte][2] */
     static constexpr uint32_t OFF_TAB = OFF_G + 2 * GBUF;       /* float4 [16][8] code table */
@@ -285,17 +284,12 @@ __device__ __forceinline__ void issue_dg(uint32_t tmem_dg, uint32_t a_base, uint
 
 /* Warp roles: warps 0-3 are producers (thread = accumulator row), warp 4 is the controller
  * (bulk copies, genotype staging, MMA issue).  No CTA-wide barrier inside the chunk loop: the
- * roles hand off through mbarriers, one per buffer, so no wait can mistake a later phase for the
- * one it waits for.  The A tiles and the qp / om TMEM columns are double-buffered: while the
- * tensor core multiplies chunk c the producers already fill the other A stage with chunk c+1,
- * whose qp was computed during chunk c; the producers wait on the MMAs of chunk c only at the
- * end of chunk c+1 (to add its [diag | grad] sums) and before refilling stage c % 2 in chunk
- * c+2.  Every wait is bounded; after a failed wait a thread sets the shared abort flag and
- * both roles run to the end without waiting. */
+ * roles hand off through mbarriers.  Every wait is bounded; after a failed wait a thread sets
+ * the shared abort flag and both roles run to the end without waiting. */
 constexpr int MQ_CTA = MQ_THREADS + 32;
 
 template <int K>
-__global__ void __launch_bounds__(MQ_CTA, (K <= 12 ? 2 : 1))
+__global__ void __launch_bounds__(MQ_CTA, (K <= 8 ? 3 : (K <= 12 ? 2 : 1)))
 k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pitch,
                 const double *__restrict__ q, const uint8_t *__restrict__ pkg, int64_t jslice,
                 double *__restrict__ out, int *__restrict__ err)
@@ -304,14 +298,13 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     constexpr int T = C::T, N = C::N, E = C::E;
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    /* per buffer b: qp ready [b], qp read (4 warps) [b], A stage written (4 warps) [b], MMAs of
-     * the stage done [b]; G staged [b]; package landed [b] */
-    __shared__ uint64_t mbar[12];
+    /* qp ready, qp consumed (4 warps), A tiles written (4 warps), the chunk's Hessian and
+     * [diag | grad] MMAs done, G staged [2], package [NPKG] */
+    __shared__ uint64_t mbar[6 + MQ_NPKG];
     __shared__ uint32_t tmem_holder;
     __shared__ volatile int abort_flag;
-    uint64_t *bar_qp = &mbar[0], *bar_qfree = &mbar[2], *bar_afull = &mbar[4], *bar_h = &mbar[6];
-    uint64_t *bar_g = &mbar[8], *bar_p = &mbar[10];
-    static_assert(MQ_NPKG == 2, "one package slot per chunk parity");
+    uint64_t *bar_qp = &mbar[0], *bar_qfree = &mbar[1], *bar_afull = &mbar[2], *bar_h = &mbar[3];
+    uint64_t *bar_g = &mbar[4], *bar_p = &mbar[6];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool producer = warp < 4;
@@ -322,17 +315,17 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     const int64_t j1 = min(J, j0 + jslice);
     const int nchunk = (int)((j1 - j0 + MQ_JC - 1) / MQ_JC);
     const uint8_t *pk0 = pkg + (size_t)(j0 / MQ_JC) * C::PKG;
+    uint8_t *At = sm + C::OFF_A;
 
     if (warp == 4) tmem_alloc_warp(&tmem_holder, C::NCOLS);
     if (tid == 0) {
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&bar_qp[b], 1);
-            mbar_init(&bar_qfree[b], 4);
-            mbar_init(&bar_afull[b], 4);
-            mbar_init(&bar_h[b], 1);
-            mbar_init(&bar_g[b], 1);
-            mbar_init(&bar_p[b], 1);
-        }
+        mbar_init(bar_qp, 1);
+        mbar_init(bar_qfree, 4);
+        mbar_init(bar_afull, 4);
+        mbar_init(bar_h, 1);
+        mbar_init(&bar_g[0], 1);
+        mbar_init(&bar_g[1], 1);
+        for (int b = 0; b < MQ_NPKG; ++b) mbar_init(&bar_p[b], 1);
         abort_flag = 0;
         mbar_fence_init();
     }
@@ -397,59 +390,56 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         };
         auto copy_pkg = [&](int c) {
             if (leader) {
-                mbar_arrive_expect_tx(&bar_p[c & 1], C::PKG);
-                bulk_g2s(sm + C::OFF_PKG + (c & 1) * C::PKG, pk0 + (size_t)c * C::PKG, C::PKG, &bar_p[c & 1]);
+                mbar_arrive_expect_tx(&bar_p[c % MQ_NPKG], C::PKG);
+                bulk_g2s(sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG, pk0 + (size_t)c * C::PKG, C::PKG,
+                         &bar_p[c % MQ_NPKG]);
             }
         };
-        /* qp / om of chunk c into TMEM buffer c & 1 */
-        auto qp_mma = [&](int c) {
-            if (leader) {
-                tc_fence_after_sync();
-                issue_qp<K>(tmem + (uint32_t)((c & 1) * C::QPN), sm, sm + C::OFF_PKG + (c & 1) * C::PKG);
-                tc_commit(&bar_qp[c & 1]);
-            }
-            __syncwarp();
-        };
-        for (int c = 0; c < min(nchunk, 2); ++c) copy_pkg(c);
+        for (int c = 0; c < min(nchunk, MQ_NPKG); ++c) copy_pkg(c);
         if (nchunk > 0) stage_g(0);
         if (nchunk > 1) stage_g(1);
-        if (nchunk > 0 && wait(&bar_p[0], 0u)) qp_mma(0);
+        if (nchunk > 0 && wait(&bar_p[0], 0u) && leader) {
+            tc_fence_after_sync();
+            issue_qp<K>(tmem, sm, sm + C::OFF_PKG);
+            tc_commit(bar_qp);
+        }
         constexpr uint32_t idesc = idesc_bf16_f32(128, N);
         for (int c = 0; c < nchunk && ok; ++c) {
-            const int s = c & 1;
-            /* qp of chunk c+1 once its package landed and the producers read qp of chunk c-1 */
+            /* qp of chunk c+1 once its package landed and the producers read qp of chunk c */
             if (c + 1 < nchunk) {
                 const int cn = c + 1;
-                if (!wait(&bar_p[cn & 1], (uint32_t)((cn >> 1) & 1))) break;
-                if (cn >= 2 && !wait(&bar_qfree[cn & 1], (uint32_t)(((cn - 2) >> 1) & 1))) break;
-                qp_mma(cn);
-            }
-            /* Hessian and [diag | grad] of chunk c once the producers wrote its A stage */
-            if (!wait(&bar_afull[s], (uint32_t)((c >> 1) & 1))) break;
-            if (leader) {
-                tc_fence_after_sync();
-                const uint8_t *pk = sm + C::OFF_PKG + s * C::PKG;
-                const uint32_t abase = smem_u32(sm + C::OFF_A + s * C::A_STAGE), bbase = smem_u32(pk);
-#pragma unroll
-                for (int term = 0; term < 2; ++term) {
-#pragma unroll
-                    for (int ks = 0; ks < 2; ++ks) {
-                        const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
-                        const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
-                        tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || term > 0 || ks > 0) ? 1u : 0u);
-                    }
+                const bool landed = wait(&bar_p[cn % MQ_NPKG], (uint32_t)((cn / MQ_NPKG) & 1));
+                if (landed && wait(bar_qfree, (uint32_t)(c & 1)) && leader) {
+                    tc_fence_after_sync();
+                    issue_qp<K>(tmem, sm, sm + C::OFF_PKG + (cn % MQ_NPKG) * C::PKG);
+                    tc_commit(bar_qp);
                 }
-                issue_dg<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase, bbase + C::PK_DG);
-                tc_commit(&bar_h[s]);
             }
-            __syncwarp();
-            /* the producers are done with G buffer c & 1: stage chunk c+2 into it */
-            if (c + 2 < nchunk) stage_g(c + 2);
-            /* package slot c & 1 is free once the MMAs of chunk c are done: fetch chunk c+2 into it */
-            if (c + 2 < nchunk) {
-                if (!wait(&bar_h[s], (uint32_t)((c >> 1) & 1))) break;
+            /* Hessian and [diag | grad] of chunk c once the producers wrote its A tiles */
+            if (wait(bar_afull, (uint32_t)(c & 1))) {
+                if (leader) {
+                    tc_fence_after_sync();
+                    const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
+                    const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
+#pragma unroll
+                    for (int term = 0; term < 2; ++term) {
+#pragma unroll
+                        for (int ks = 0; ks < 2; ++ks) {
+                            const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
+                            const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
+                            tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || term > 0 || ks > 0) ? 1u : 0u);
+                        }
+                    }
+                    issue_dg<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase, bbase + C::PK_DG);
+                    tc_commit(bar_h);
+                }
+                /* the producers are done with G buffer c & 1: stage chunk c+2 into it */
+                if (c + 2 < nchunk) stage_g(c + 2);
+            }
+            /* package c is free once the MMAs of chunk c are done: fetch chunk c+NPKG into it */
+            if (c + MQ_NPKG < nchunk && wait(bar_h, (uint32_t)(c & 1))) {
                 fence_async_smem();
-                copy_pkg(c + 2);
+                copy_pkg(c + MQ_NPKG);
             }
         }
     } else {
@@ -471,10 +461,8 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         double gd[K], dd[K], zsd = 0.0;   /* gradient sum_j (z1 - z2) p_k, Hessian diagonal, sum_j z2 */
 #pragma unroll
         for (int k = 0; k < K; ++k) gd[k] = dd[k] = 0.0;
-        /* chunk cc's [diag | grad] sums into FP64 once its MMAs are done (the accumulator is single:
-         * chunk cc+1's MMAs, which overwrite it, are issued only after this thread's next afull) */
-        auto drain_dg = [&](int cc) -> bool {
-            if (!wait(&bar_h[cc & 1], (uint32_t)((cc >> 1) & 1))) return false;
+        /* the [diag | grad] accumulator of the last chunk whose MMAs completed, into FP64 */
+        auto drain_dg = [&]() {
             tc_fence_after_sync();
             float v[16];
             tmem_ld16(tmem + lane_base + C::COL_DG, v);
@@ -490,40 +478,42 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
 #pragma unroll
                 for (int k = 0; k < K; ++k) gd[k] += (double)v[k];
             }
-            if ((cc + 1) % MX_HBLOCK == 0 && cc + 1 < nchunk) {   /* the Hessian block ending at chunk cc */
-                hess_drain<N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E,
-                                 cc + 1 == MX_HBLOCK, valid);
-            }
             tc_fence_before_sync();
-            return true;
         };
         for (int c = 0; c < nchunk && ok; ++c) {
-            const int s = c & 1;
-            const uint32_t qcol = (uint32_t)(s * C::QPN);
-            uint8_t *At = sm + C::OFF_A + s * C::A_STAGE;
-            const uint8_t *Gb = sm + C::OFF_G + s * C::GBUF;
+            const uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF;
+            if (c > 0) {   /* the MMAs of chunk c-1 are done: its [diag | grad] sums, free A tiles */
+                if (!wait(bar_h, (uint32_t)((c - 1) & 1))) break;
+                drain_dg();
+                if (c % MX_HBLOCK == 0) {   /* drain the Hessian block of chunks c-MX_HBLOCK .. c-1 */
+                    tc_fence_after_sync();
+                    hess_drain<N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E,
+                                     c == MX_HBLOCK, valid);
+                    tc_fence_before_sync();
+                }
+            }
             /* qp / om of the chunk's 32 SNPs, read in two halves of 16 columns (SNPs 0-15, then
              * 16-31) to keep the producer within its registers */
             uint32_t rq[16], ro[16];
-            if (!wait(&bar_qp[s], (uint32_t)((c >> 1) & 1))) break;
+            if (!wait(bar_qp, (uint32_t)(c & 1))) break;
             tc_fence_after_sync();
-            tmem_ld16_raw(tmem + lane_base + qcol, rq);
-            tmem_ld16_raw(tmem + lane_base + qcol + 32u, ro);
+            tmem_ld16_raw(tmem + lane_base, rq);
+            tmem_ld16_raw(tmem + lane_base + 32u, ro);
             tmem_wait_ld();
-            if (!wait(&bar_g[s], (uint32_t)((c >> 1) & 1))) break;
-            if (c >= 2 && !wait(&bar_h[s], (uint32_t)(((c - 2) >> 1) & 1))) break;   /* A stage s is free */
+            if (!wait(&bar_p[c % MQ_NPKG], (uint32_t)((c / MQ_NPKG) & 1))) break;
+            if (!wait(&bar_g[c & 1], (uint32_t)((c >> 1) & 1))) break;
             const uint16_t *G2 = (const uint16_t *)Gb + (tid >> 2);
             float2 zs = make_float2(0.f, 0.f);
 #pragma unroll
             for (int kc = 0; kc < 4; ++kc) {
-                if (kc == 2) {   /* the second half of the columns; then qp buffer s is free */
+                if (kc == 2) {   /* the second half of the columns; then the qp columns are free */
                     tc_fence_after_sync();
-                    tmem_ld16_raw(tmem + lane_base + qcol + 16u, rq);
-                    tmem_ld16_raw(tmem + lane_base + qcol + 48u, ro);
+                    tmem_ld16_raw(tmem + lane_base + 16u, rq);
+                    tmem_ld16_raw(tmem + lane_base + 48u, ro);
                     tmem_wait_ld();
                     tc_fence_before_sync();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(&bar_qfree[s]);
+                    if (lane == 0) mbar_arrive(bar_qfree);
                 }
                 uint32_t w1p[4], w2p[4], d0p[4], d1p[4];
 #pragma unroll
@@ -558,13 +548,11 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 *(uint4 *)(At + 3 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d1p[0], d1p[1], d1p[2], d1p[3]);
             }
             zsd += (double)zs.x + (double)zs.y;
-            /* the previous chunk's sums (its MMAs ran while this chunk was computed) */
-            if (c > 0 && !drain_dg(c - 1)) break;
             fence_async_smem();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bar_afull[s]);
+            if (lane == 0) mbar_arrive(bar_afull);
         }
-        if (nchunk > 0) drain_dg(nchunk - 1);   /* the last chunk */
+        if (nchunk > 0 && wait(bar_h, (uint32_t)((nchunk - 1) & 1))) drain_dg();   /* the last chunk */
         if (valid) {
             double *o = out + ((size_t)blockIdx.y * I + i) * E;
 #pragma unroll
@@ -608,14 +596,11 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     /* controller: the same three CTA-wide barriers as the producers' epilogue */
     ok = __syncthreads_and(ok);
     if (!ok && tid == MQ_THREADS) {
-        for (int b = 0; b < 2; ++b) {
-            mbar_wait_bounded(&bar_h[b], 0u, 1024u);
-            mbar_wait_bounded(&bar_h[b], 1u, 1024u);
-            mbar_wait_bounded(&bar_qp[b], 0u, 1024u);
-            mbar_wait_bounded(&bar_qp[b], 1u, 1024u);
-            mbar_wait_bounded(&bar_p[b], 0u, 1024u);
-            mbar_wait_bounded(&bar_p[b], 1u, 1024u);
-        }
+        mbar_wait_bounded(bar_h, 0u, 1024u);
+        mbar_wait_bounded(bar_h, 1u, 1024u);
+        mbar_wait_bounded(bar_qp, 0u, 1024u);
+        mbar_wait_bounded(bar_qp, 1u, 1024u);
+        for (int b = 0; b < MQ_NPKG; ++b) { mbar_wait_bounded(&bar_p[b], 0u, 1024u); mbar_wait_bounded(&bar_p[b], 1u, 1024u); }
     }
     __syncthreads();
     tc_fence_before_sync();
