@@ -33,21 +33,72 @@ constexpr uint32_t MX_WAIT_LIMIT = 1u << 22;   /* polls; an MMA batch completes 
  * than 4 * MX_HBLOCK MMA accumulations (whose rounding is not to nearest) whatever J or I is. */
 constexpr int MX_HBLOCK = 256;
 
+/* Column order of the Hessian accumulators: the K diagonal pairs first (column k = pair (k, k)),
+ * then the off-diagonal pairs (a, b), b < a, in the packed order of the FP64 partial rows.
+ * col_out: the packed FP64 index a (a + 1) / 2 + b of column col's pair; col_pair: its factors. */
+__host__ __device__ constexpr int col_out(int K, int col)
+{
+    if (col < K) return col * (col + 1) / 2 + col;
+    int m = col - K, a = 1;
+    while ((a + 1) * a / 2 <= m) ++a;
+    return a * (a + 1) / 2 + (m - a * (a - 1) / 2);
+}
+
+__device__ __forceinline__ void col_pair(int K, int col, int &ka, int &kb)
+{
+    if (col < K) { ka = kb = col; return; }
+    int m = col - K, a = 1;
+    while ((a + 1) * a / 2 <= m) ++a;
+    ka = a;
+    kb = m - a * (a - 1) / 2;
+}
+
 /* add (or, for the first block, store) TMEM columns col .. col+N-1 of this thread's lane into the
- * FP64 Hessian entries o[0 .. T-1] */
-template <int N, int T>
+ * FP64 Hessian entries: column e holds the pair whose packed index is col_out(K, e) */
+template <int K, int N, int T>
 __device__ __forceinline__ void hess_drain(uint32_t taddr, double *o, bool first, bool valid)
 {
-#pragma unroll 1
+#pragma unroll
     for (int c0 = 0; c0 < N; c0 += 16) {
         float v[16];
         tmem_ld16(taddr + (uint32_t)c0, v);
         if (valid) {
 #pragma unroll
             for (int e = 0; e < 16; ++e)
-                if (c0 + e < T) o[c0 + e] = first ? (double)v[e] : o[c0 + e] + (double)v[e];
+                if (c0 + e < T) {
+                    double &x = o[col_out(K, c0 + e)];
+                    x = first ? (double)v[e] : x + (double)v[e];
+                }
         }
     }
+}
+
+/* After a chunk's MMAs completed (one producer thread = one TMEM lane; lane = this lane's base):
+ * the chunk's Hessian diagonal -- columns 0..K-1 of the Hessian accumulator at col_h -- is added
+ * into dd[] and those columns are set to zero for the next chunk; the chunk's gradient sums
+ * (columns 0..K-1 and K..2K-1 of the accumulator at col_g) are added into gd[]. */
+template <int K, int NDG>
+__device__ __forceinline__ void drain_chunk(uint32_t lane, uint32_t col_h, uint32_t col_g, double (&dd)[K], double (&gd)[K])
+{
+    static_assert(K <= 16 && 2 * K <= NDG && NDG <= 32, "diagonal columns within one 16-column load");
+    tc_fence_after_sync();
+    float h[16], g0[16], g1[16];
+    tmem_ld16(lane + col_h, h);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        dd[k] += (double)h[k];
+        h[k] = 0.f;
+    }
+    tmem_st16(lane + col_h, h);
+    tmem_ld16(lane + col_g, g0);
+    if constexpr (NDG == 32) tmem_ld16(lane + col_g + 16u, g1);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {   /* hi * hi + lo * hi, plus hi * lo (2^-8 of it: one FP32 rounding) */
+        const float hl = (K + k < 16) ? g0[K + k] : g1[(K + k) & 15];
+        gd[k] += (double)(g0[k] + hl);
+    }
+    tmem_wait_st();
+    tc_fence_before_sync();
 }
 
 __device__ __forceinline__ float rcp_approx(float x)
@@ -82,26 +133,26 @@ __device__ __forceinline__ uint4 interleave8(uint2 a, uint2 b)
  *   qp / om    D[128 x 64] = Qtile * [p ; 1-p]^T in TF32 split form (hi*hi + lo*hi + hi*lo, about
  *              2^-21 relative): the K-term dot products of every (individual, SNP) cell;
  *   Hessian    D[128 x N] += [w1 | w2] * [PP ; PbarPbar]^T in BF16 (FP32 accumulation), drained
- *              into FP64 every MX_HBLOCK chunks;
- *   diag/grad  D[128 x NDG] = [w1 | w2] * [p^2 ; (1-p)^2]^T (the Hessian diagonal) and
- *              [dz_hi | dz_lo | dz_hi] * [p_hi ; p_hi ; p_lo]^T (the gradient sum_j dz p_k with
- *              dz = z1 - z2 and both factors split into two BF16 parts, about 2^-17 relative), a
- *              fresh FP32 sum every chunk that the producers add into FP64;
+ *              into FP64 every MX_HBLOCK chunks; its columns hold the K diagonal pairs first;
+ *   gradient   D[128 x NDG] = dz_hi * [p_hi | p_lo]^T + dz_lo * [p_hi | 0]^T, the gradient sum_j dz p_k
+ *              with dz = z1 - z2 and both factors split into two BF16 parts (hi*hi + lo*hi in
+ *              columns 0..K-1, hi*lo in K..2K-1: about 2^-17 relative), a fresh FP32 sum every
+ *              chunk that the producers add into FP64;
  * and on the CUDA cores, per cell: the code lookup, one reciprocal, z1, z2, w1, w2, dz and its
  * split, and sum_j z2 (FP32 per chunk, FP64 across chunks).  The gradient is
  * sum_j (z1 - z2) p_k + z2 (= sum_j z1 p_k + z2 (1 - p_k)).
  *
- * The diagonal's per-chunk sum is the compensated correction of the BF16 Hessian: the tensor
- * core's FP32 accumulation rounds toward zero, so a sum carried over many chunks drifts low
- * (about 5e-5 relative over 256 chunks); restarted every chunk and carried in FP64, the
- * diagonal drifts only by what one chunk's four accumulations lose.  The off-diagonal entries
- * keep the MX_HBLOCK drains.
+ * The compensated diagonal: the tensor core's FP32 accumulation rounds toward zero, so a sum
+ * carried over many chunks drifts low (about 5e-5 relative over 256 chunks).  After every chunk
+ * the producers read the Hessian's K diagonal columns, add them into FP64 and store zeros back
+ * (tcgen05.st), so each chunk's diagonal is a fresh FP32 sum of four accumulations carried on in
+ * FP64.  The off-diagonal entries keep the MX_HBLOCK drains.
  *
  * Everything that depends on P alone -- the BF16 pair-product tiles, the TF32 hi / lo split of
- * [p ; 1-p], the diagonal and gradient B blocks -- is built once per sweep by k_q_pack, one
- * "package" per chunk laid out exactly as the sweep's shared memory wants it, and fetched by
- * each CTA with one bulk asynchronous copy.  The qp MMA of chunk c+1 runs while the CUDA cores
- * work on chunk c. */
+ * [p ; 1-p], the gradient B blocks -- is built once per sweep by k_q_pack, one "package" per
+ * chunk laid out exactly as the sweep's shared memory wants it, and fetched by each CTA with
+ * one bulk asynchronous copy.  The qp MMA of chunk c+1 runs while the CUDA cores work on
+ * chunk c. */
 
 constexpr int MQ_JC = 32;          /* SNPs per chunk = 2 BF16 MMA K-steps */
 constexpr int MQ_THREADS = 128;    /* one thread per individual = accumulator row */
@@ -110,13 +161,11 @@ constexpr int MQ_THREADS = 128;    /* one thread per individual = accumulator ro
 #endif
 constexpr int MQ_NPKG = ADMIX_MQ_NPKG;   /* package buffers */
 
-/* The [diagonal | gradient] accumulator of a chunk: N = NDG columns, the Hessian diagonal
- * sum_j w1 p_k^2 + w2 (1-p_k)^2 in columns 0..K-1 and the gradient sum_j (z1 - z2) p_k in columns
- * GOFF..GOFF+K-1.  It starts afresh every chunk and the producers add it into FP64, so no FP32
- * partial of these entries sees more than one chunk's accumulations. */
+/* The gradient accumulator of a chunk: NDG columns, sum_j dz_hi p_hi + dz_lo p_hi in columns 0..K-1
+ * and sum_j dz_hi p_lo in columns K..2K-1.  It starts afresh every chunk and the producers add it
+ * into FP64, so no FP32 partial of the gradient sees more than one chunk's accumulations. */
 template <int K> struct DGShape {
     static constexpr int NDG = K <= 8 ? 16 : 32;
-    static constexpr int GOFF = K <= 8 ? 8 : 16;
 };
 
 template <int K>
@@ -125,21 +174,21 @@ struct MQ {
     static constexpr int N = ((T + 15) / 16) * 16;              /* Hessian MMA N (multiple of 16 for M = 128) */
     static constexpr int KP = ((K + 7) / 8) * 8;                /* TF32 K extent of the qp MMAs */
     static constexpr int QPN = 2 * MQ_JC;                       /* qp MMA N: the chunk's p rows, then 1-p rows */
-    static constexpr int NDG = DGShape<K>::NDG, GOFF = DGShape<K>::GOFF;
+    static constexpr int NDG = DGShape<K>::NDG;
     static constexpr uint32_t COL_H = 64;                       /* TMEM column of the Hessian accumulator */
-    static constexpr uint32_t COL_DG = COL_H + N;               /* TMEM column of the [diag | grad] accumulator */
+    static constexpr uint32_t COL_DG = COL_H + N;               /* TMEM column of the gradient accumulator */
     static constexpr uint32_t NCOLS = tmem_cols_for(COL_DG + NDG);
     static constexpr int E = T + K;                             /* partial entries per individual */
     static constexpr uint32_t A_BYTES = 128 * MQ_JC * 2;        /* one BF16 A tile (128 rows x 32 SNPs): 8 KB */
     static constexpr uint32_t B_BYTES = N * MQ_JC * 2;          /* one BF16 pair-product tile */
     static constexpr uint32_t QA_BYTES = 128 * 2 * KP * 4;      /* TF32 Q tile [hi | lo] */
     static constexpr uint32_t QB_BYTES = QPN * 2 * KP * 4;      /* TF32 [p ; 1-p] chunk [hi | lo] */
-    static constexpr uint32_t DGB_BYTES = NDG * MQ_JC * 2;      /* one BF16 B block of the [diag | grad] MMA */
-    /* package of one chunk: [PP tile | PbarPbar tile | TF32 [p ; 1-p] | diag p^2 | diag (1-p)^2 |
-     * gradient p (BF16 high part) | gradient p (BF16 low part)] */
+    static constexpr uint32_t DGB_BYTES = NDG * MQ_JC * 2;      /* one BF16 B block of the gradient MMAs */
+    /* package of one chunk: [PP tile | PbarPbar tile | TF32 [p ; 1-p] | gradient B blocks
+     * [p_hi | p_lo] and [p_hi | 0]] */
     static constexpr uint32_t PK_QB = 2 * B_BYTES;
     static constexpr uint32_t PK_DG = PK_QB + QB_BYTES;
-    static constexpr uint32_t PKG = PK_DG + 4 * DGB_BYTES;
+    static constexpr uint32_t PKG = PK_DG + 2 * DGB_BYTES;
     static constexpr uint32_t GBUF = MQ_JC * 32;                /* genotype bytes of one chunk */
     static constexpr uint32_t OFF_A = 0;                        /* W1, W2, DZ0, DZ1 tiles */
     static constexpr uint32_t OFF_PKG = 4 * A_BYTES;
@@ -149,7 +198,7 @@ struct MQ {
     static constexpr uint32_t SMEM = OFF_TAB + 128 * 16 + 1024; /* + alignment slack */
     /* core matrices (8 rows x 16 B): BF16 A 128 B apart along M, 2048 B along K; BF16 B 128 B
      * along N, 16 N bytes along K; TF32 Q tile 128 B along M, 2048 B along K; TF32 [p ; 1-p]
-     * 128 B along N, 1024 B along K; [diag | grad] B blocks 128 B along N, 16 NDG bytes along K */
+     * 128 B along N, 1024 B along K; gradient B blocks 128 B along N, 16 NDG bytes along K */
     static constexpr uint32_t A_LBO = 2048, A_SBO = 128;
     static constexpr uint32_t B_LBO = 16 * N, B_SBO = 128;
     static constexpr uint32_t QA_LBO = 2048, QB_LBO = 1024, Q_SBO = 128;
@@ -204,27 +253,27 @@ k_q_pack(const double *__restrict__ p, int64_t J, uint8_t *__restrict__ pkg)
         tf32_split(b, h, l);
         *(float *)(buf + C::PK_QB + kmaj_off(MQ_JC + jj, k, C::QB_LBO)) = h;
         *(float *)(buf + C::PK_QB + kmaj_off(MQ_JC + jj, C::KP + k, C::QB_LBO)) = l;
-        /* [diag | grad] B blocks: element (row n, SNP jj) at granule jj / 8, half-word jj % 8 */
-        uint16_t *dgp = (uint16_t *)(buf + C::PK_DG + bblk_off(k, jj >> 3, C::DG_LBO)) + (jj & 7);
-        uint16_t *dgb = (uint16_t *)(buf + C::PK_DG + C::DGB_BYTES + bblk_off(k, jj >> 3, C::DG_LBO)) + (jj & 7);
-        uint16_t *gp0 = (uint16_t *)(buf + C::PK_DG + 2 * C::DGB_BYTES + bblk_off(C::GOFF + k, jj >> 3, C::DG_LBO)) + (jj & 7);
-        uint16_t *gp1 = (uint16_t *)(buf + C::PK_DG + 3 * C::DGB_BYTES + bblk_off(C::GOFF + k, jj >> 3, C::DG_LBO)) + (jj & 7);
-        *dgp = (uint16_t)(pack_bf16x2(a * a, 0.f) & 0xFFFFu);
-        *dgb = (uint16_t)(pack_bf16x2(b * b, 0.f) & 0xFFFFu);
+        /* gradient B blocks [p_hi | p_lo] and [p_hi | 0]: element (row n, SNP jj) at granule jj / 8,
+         * half-word jj % 8 */
+        uint16_t *g0 = (uint16_t *)(buf + C::PK_DG + bblk_off(k, jj >> 3, C::DG_LBO)) + (jj & 7);
+        uint16_t *g0l = (uint16_t *)(buf + C::PK_DG + bblk_off(K + k, jj >> 3, C::DG_LBO)) + (jj & 7);
+        uint16_t *g1 = (uint16_t *)(buf + C::PK_DG + C::DGB_BYTES + bblk_off(k, jj >> 3, C::DG_LBO)) + (jj & 7);
         uint16_t hi, lo;
         bf16_split(a, hi, lo);
-        *gp0 = hi;
-        *gp1 = lo;
+        *g0 = hi;
+        *g0l = lo;
+        *g1 = hi;
     }
     __syncthreads();
-    /* pair-product tiles: task (term, kc, nn) writes pair nn's 8 SNPs of k-chunk kc at kc*16N + 16nn */
+    /* pair-product tiles: task (term, kc, nn) writes column nn's pair (diagonal pairs first), 8 SNPs
+     * of k-chunk kc, at kc*16N + 16nn */
     for (int t = tid; t < 2 * 4 * N; t += 128) {
         const int term = t / (4 * N), rem = t - term * 4 * N;
         const int kc = rem / N, nn = rem - kc * N;
         uint32_t w[4] = {0u, 0u, 0u, 0u};
         if (nn < T) {
             int ka, kb;
-            tri_pair(nn, ka, kb);
+            col_pair(K, nn, ka, kb);
             const float *src = pf + term * K * PS + kc * 8;
             const float4 a0 = *(const float4 *)(src + ka * PS), a1 = *(const float4 *)(src + ka * PS + 4);
             const float4 b0 = *(const float4 *)(src + kb * PS), b1 = *(const float4 *)(src + kb * PS + 4);
@@ -261,22 +310,21 @@ __device__ __forceinline__ void issue_qp(uint32_t tmem, const uint8_t *sm, const
     }
 }
 
-/* The chunk's [diag | grad] MMAs (one thread), a fresh sum into TMEM columns COL_DG..:
- *   diag:  [W1 | W2] x [p^2 block ; (1-p)^2 block]                      (4 K-steps)
- *   grad:  [DZ0 | DZ1 | DZ0] x [p hi block ; p hi block ; p lo block]   (6 K-steps)
- * a_base: the A tiles W1, W2, DZ0, DZ1 (A_BYTES apart); b_base: the package's PK_DG blocks. */
+/* The chunk's gradient MMAs (one thread), a fresh sum into TMEM columns COL_DG..:
+ *   DZ0 x [hi | lo block]   dz_hi p_hi in columns 0..K-1, dz_hi p_lo in K..2K-1   (2 K-steps)
+ *   DZ1 x [hi | 0 block]    dz_lo p_hi added into columns 0..K-1                   (2 K-steps)
+ * a_dz: the A tile DZ0 (DZ1 follows at +A_BYTES); b_base: the package's two gradient B blocks.
+ * Shared by both sides (P side: p -> q). */
 template <int K, uint32_t A_BYTES, uint32_t A_LBO, uint32_t DGB_BYTES, uint32_t DG_LBO>
-__device__ __forceinline__ void issue_dg(uint32_t tmem_dg, uint32_t a_base, uint32_t b_base)
+__device__ __forceinline__ void issue_grad(uint32_t tmem_dg, uint32_t a_dz, uint32_t b_base)
 {
     constexpr uint32_t id = idesc_bf16_f32(128, DGShape<K>::NDG);
-    constexpr int AT[5] = {0, 1, 2, 3, 2};   /* A tile of each term: W1, W2, DZ0, DZ1, DZ0 */
-    constexpr int BB[5] = {0, 1, 2, 2, 3};   /* B block of each term: p^2, (1-p)^2, p hi, p hi, p lo */
 #pragma unroll
-    for (int t = 0; t < 5; ++t) {
+    for (int t = 0; t < 2; ++t) {
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
-            const uint64_t ad = umma_desc_kmajor(a_base + AT[t] * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
-            const uint64_t bd = umma_desc_kmajor(b_base + BB[t] * DGB_BYTES + ks * 2 * DG_LBO, DG_LBO, 128);
+            const uint64_t ad = umma_desc_kmajor(a_dz + t * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
+            const uint64_t bd = umma_desc_kmajor(b_base + t * DGB_BYTES + ks * 2 * DG_LBO, DG_LBO, 128);
             tc_mma_bf16(tmem_dg, ad, bd, id, (t > 0 || ks > 0) ? 1u : 0u);
         }
     }
@@ -299,7 +347,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
     /* qp ready, qp consumed (4 warps), A tiles written (4 warps), the chunk's Hessian and
-     * [diag | grad] MMAs done, G staged [2], package [NPKG] */
+     * gradient MMAs done, G staged [2], package [NPKG] */
     __shared__ uint64_t mbar[6 + MQ_NPKG];
     __shared__ uint32_t tmem_holder;
     __shared__ volatile int abort_flag;
@@ -415,7 +463,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     tc_commit(bar_qp);
                 }
             }
-            /* Hessian and [diag | grad] of chunk c once the producers wrote its A tiles */
+            /* Hessian and gradient MMAs of chunk c once the producers wrote its A tiles */
             if (wait(bar_afull, (uint32_t)(c & 1))) {
                 if (leader) {
                     tc_fence_after_sync();
@@ -430,7 +478,8 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                             tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || term > 0 || ks > 0) ? 1u : 0u);
                         }
                     }
-                    issue_dg<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase, bbase + C::PK_DG);
+                    issue_grad<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase + 2 * C::A_BYTES,
+                                                                                 bbase + C::PK_DG);
                     tc_commit(bar_h);
                 }
                 /* the producers are done with G buffer c & 1: stage chunk c+2 into it */
@@ -461,33 +510,17 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         double gd[K], dd[K], zsd = 0.0;   /* gradient sum_j (z1 - z2) p_k, Hessian diagonal, sum_j z2 */
 #pragma unroll
         for (int k = 0; k < K; ++k) gd[k] = dd[k] = 0.0;
-        /* the [diag | grad] accumulator of the last chunk whose MMAs completed, into FP64 */
-        auto drain_dg = [&]() {
-            tc_fence_after_sync();
-            float v[16];
-            tmem_ld16(tmem + lane_base + C::COL_DG, v);
-#pragma unroll
-            for (int k = 0; k < K && k < 8; ++k) {
-                dd[k] += (double)v[k];
-                if (C::NDG == 16) gd[k] += (double)v[C::GOFF + k];
-            }
-            if constexpr (C::NDG == 32) {
-#pragma unroll
-                for (int k = 8; k < K; ++k) dd[k] += (double)v[k];
-                tmem_ld16(tmem + lane_base + C::COL_DG + 16u, v);
-#pragma unroll
-                for (int k = 0; k < K; ++k) gd[k] += (double)v[k];
-            }
-            tc_fence_before_sync();
-        };
+        /* the last chunk whose MMAs completed: its Hessian diagonal (columns 0..K-1 of the Hessian
+         * accumulator, cleared for the next chunk) and its gradient sums, into FP64 */
+        auto drain_dg = [&]() { drain_chunk<K, C::NDG>(tmem + lane_base, C::COL_H, C::COL_DG, dd, gd); };
         for (int c = 0; c < nchunk && ok; ++c) {
             const uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF;
-            if (c > 0) {   /* the MMAs of chunk c-1 are done: its [diag | grad] sums, free A tiles */
+            if (c > 0) {   /* the MMAs of chunk c-1 are done: its diagonal and gradient sums, free A tiles */
                 if (!wait(bar_h, (uint32_t)((c - 1) & 1))) break;
                 drain_dg();
                 if (c % MX_HBLOCK == 0) {   /* drain the Hessian block of chunks c-MX_HBLOCK .. c-1 */
                     tc_fence_after_sync();
-                    hess_drain<N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E,
+                    hess_drain<K, N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E,
                                      c == MX_HBLOCK, valid);
                     tc_fence_before_sync();
                 }
@@ -564,7 +597,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         __syncthreads();
         tc_fence_after_sync();
         if (nchunk > 0) {
-#pragma unroll 1
+#pragma unroll
             for (int c0 = 0; c0 < N; c0 += 16) {
                 float v[16];
                 tmem_ld16(tmem + lane_base + C::COL_H + (uint32_t)c0, v);
@@ -573,13 +606,14 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const bool first = nchunk <= MX_HBLOCK;
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        if (c0 + e < T)
-                            o[c0 + e] = ok ? (first ? (double)v[e] : o[c0 + e] + (double)v[e])
-                                           : __longlong_as_double(0x7ff8000000000000LL);
+                        if (c0 + e < T) {
+                            double &x = o[col_out(K, c0 + e)];
+                            x = ok ? (first ? (double)v[e] : x + (double)v[e]) : __longlong_as_double(0x7ff8000000000000LL);
+                        }
                 }
             }
         }
-        if (valid) {   /* the diagonal from the per-chunk [diag | grad] sums (FP64 across chunks) */
+        if (valid) {   /* the diagonal from the per-chunk sums (FP64 across chunks) */
             double *o = out + ((size_t)blockIdx.y * I + i) * E;
             if (nchunk == 0) {
                 for (int e = 0; e < T; ++e) o[e] = 0.0;
@@ -613,14 +647,14 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
  * Mirror of the Q side with the roles of the axes swapped: rows = 128 SNPs, reduction over
  * chunks of 32 individuals.  Per chunk:
  *   qp, om     D[128 x 32] = Ptile * Qchunk^T and (1-P)tile * Qchunk^T, TF32 split form;
- *   Hessian    D[128 x N] += C * QQ^T in BF16, C = nm (g/qp^2 + (2-g)/(1-qp)^2);
- *   diag/grad  D[128 x NDG] = C * [q^2]^T (the Hessian diagonal) and
- *              [dz_hi | dz_lo | dz_hi] * [q_hi ; q_hi ; q_lo]^T (the gradient sum_i dz q_k,
- *              dz = nm (g/qp - (2-g)/(1-qp))), afresh every chunk and added into FP64;
+ *   Hessian    D[128 x N] += C * QQ^T in BF16, C = nm (g/qp^2 + (2-g)/(1-qp)^2), diagonal pairs
+ *              in the first K columns, read, added into FP64 and cleared after every chunk;
+ *   gradient   D[128 x NDG] = dz_hi * [q_hi | q_lo]^T + dz_lo * [q_hi | 0]^T (the gradient
+ *              sum_i dz q_k, dz = nm (g/qp - (2-g)/(1-qp))), afresh every chunk and added into FP64;
  * and per cell on the CUDA cores the code (from the thread's own genotype word), one reciprocal,
  * C, dz and its BF16 split.  The Q-derived tiles of each chunk (QQ in BF16, Q split into TF32
- * hi / lo, the diagonal and gradient B blocks, q in FP32 for the EM mode) are built once per
- * sweep by k_p_pack and fetched with one bulk copy per chunk. */
+ * hi / lo, the gradient B blocks, q in FP32 for the EM mode) are built once per sweep by
+ * k_p_pack and fetched with one bulk copy per chunk. */
 
 constexpr int MP_IC = 32;          /* individuals per chunk = 2 BF16 MMA K-steps */
 constexpr int MP_THREADS = 128;    /* one thread per SNP = accumulator row */
@@ -631,23 +665,23 @@ struct MP {
     static constexpr int T = K * (K + 1) / 2;
     static constexpr int N = ((T + 15) / 16) * 16;
     static constexpr int KP = ((K + 7) / 8) * 8;
-    static constexpr int NDG = DGShape<K>::NDG, GOFF = DGShape<K>::GOFF;
+    static constexpr int NDG = DGShape<K>::NDG;
     static constexpr uint32_t COL_OM = 32, COL_H = 64;          /* TMEM: qp 0..31, om 32..63, Hessian */
-    static constexpr uint32_t COL_DG = COL_H + N;               /* [diag | grad] accumulator */
+    static constexpr uint32_t COL_DG = COL_H + N;               /* gradient accumulator */
     static constexpr uint32_t NCOLS = tmem_cols_for(COL_DG + NDG);
     static constexpr int E = T + K;
     static constexpr uint32_t A_BYTES = 128 * MP_IC * 2;        /* one BF16 A tile (C, DZ0, DZ1): 8 KB */
     static constexpr uint32_t B_BYTES = N * MP_IC * 2;          /* BF16 QQ tile */
     static constexpr uint32_t PA_BYTES = 128 * 2 * KP * 4;      /* TF32 P tile [hi | lo] (and 1-P) */
     static constexpr uint32_t QB_BYTES = MP_IC * 2 * KP * 4;    /* TF32 Q chunk [hi | lo] */
-    static constexpr uint32_t DGB_BYTES = NDG * MP_IC * 2;      /* one BF16 B block of the [diag | grad] MMA */
+    static constexpr uint32_t DGB_BYTES = NDG * MP_IC * 2;      /* one BF16 B block of the gradient MMAs */
     static constexpr int QS = MP_IC + 4;                        /* FP32 q row stride (floats) */
-    /* package: [QQ | TF32 Q | FP32 q (EM mode) | 1 - sum q | diag q^2 | grad q hi | grad q lo] */
+    /* package: [QQ | TF32 Q | FP32 q (EM mode) | 1 - sum q | gradient blocks [q_hi | q_lo], [q_hi | 0]] */
     static constexpr uint32_t PK_QB = B_BYTES;
     static constexpr uint32_t PK_QF = PK_QB + QB_BYTES;
     static constexpr uint32_t PK_S = PK_QF + K * QS * 4;         /* 1 - sum_k q_k per individual */
     static constexpr uint32_t PK_DG = PK_S + MP_IC * 4;
-    static constexpr uint32_t PKG = PK_DG + 3 * DGB_BYTES;
+    static constexpr uint32_t PKG = PK_DG + 2 * DGB_BYTES;
     static constexpr uint32_t OFF_A = 0;                        /* C, DZ0, DZ1 */
     static constexpr uint32_t OFF_PKG = 3 * A_BYTES;
     static constexpr uint32_t OFF_PA = OFF_PKG + MP_NPKG * PKG; /* P tile, then (1-P) tile */
@@ -690,24 +724,26 @@ k_p_pack(const double *__restrict__ q, int64_t I, uint8_t *__restrict__ pkg)
         tf32_split(a, h, l);
         *(float *)(buf + C::PK_QB + kmaj_off(ii, k, C::QB_LBO)) = h;
         *(float *)(buf + C::PK_QB + kmaj_off(ii, C::KP + k, C::QB_LBO)) = l;
-        /* [diag | grad] B blocks: element (row n, individual ii) at granule ii / 8, half-word ii % 8 */
-        uint16_t *dg = (uint16_t *)(buf + C::PK_DG + bblk_off(k, ii >> 3, C::DG_LBO)) + (ii & 7);
-        uint16_t *g0 = (uint16_t *)(buf + C::PK_DG + C::DGB_BYTES + bblk_off(C::GOFF + k, ii >> 3, C::DG_LBO)) + (ii & 7);
-        uint16_t *g1 = (uint16_t *)(buf + C::PK_DG + 2 * C::DGB_BYTES + bblk_off(C::GOFF + k, ii >> 3, C::DG_LBO)) + (ii & 7);
-        *dg = (uint16_t)(pack_bf16x2(a * a, 0.f) & 0xFFFFu);
+        /* gradient B blocks [q_hi | q_lo] and [q_hi | 0]: element (row n, individual ii) at granule
+         * ii / 8, half-word ii % 8 */
+        uint16_t *g0 = (uint16_t *)(buf + C::PK_DG + bblk_off(k, ii >> 3, C::DG_LBO)) + (ii & 7);
+        uint16_t *g0l = (uint16_t *)(buf + C::PK_DG + bblk_off(K + k, ii >> 3, C::DG_LBO)) + (ii & 7);
+        uint16_t *g1 = (uint16_t *)(buf + C::PK_DG + C::DGB_BYTES + bblk_off(k, ii >> 3, C::DG_LBO)) + (ii & 7);
         uint16_t hi, lo;
         bf16_split(a, hi, lo);
         *g0 = hi;
-        *g1 = lo;
+        *g0l = lo;
+        *g1 = hi;
     }
     __syncthreads();
-    /* QQ tile: task (kc, nn) writes pair nn's 8 individuals of k-chunk kc at kc*16N + 16nn */
+    /* QQ tile: task (kc, nn) writes column nn's pair (diagonal pairs first), 8 individuals of
+     * k-chunk kc, at kc*16N + 16nn */
     for (int t = tid; t < 4 * N; t += 128) {
         const int kc = t / N, nn = t - kc * N;
         uint32_t w[4] = {0u, 0u, 0u, 0u};
         if (nn < T) {
             int ka, kb;
-            tri_pair(nn, ka, kb);
+            col_pair(K, nn, ka, kb);
             const float *src = qf + kc * 8;
             const float4 a0 = *(const float4 *)(src + ka * C::QS), a1 = *(const float4 *)(src + ka * C::QS + 4);
             const float4 b0 = *(const float4 *)(src + kb * C::QS), b1 = *(const float4 *)(src + kb * C::QS + 4);
@@ -763,27 +799,6 @@ __device__ __forceinline__ uint2 col_load32(const uint8_t *__restrict__ bed, int
  * same pipeline: per SNP the two sums sum_i nm g q_k / qp and sum_i nm (2-g) q_k / (1-qp)
  * (rows of 2K, the FP64 EM sweep's layout, finalised by k_emp_finalize), with no Hessian tile,
  * MMAs or drains; a package slot is handed back once the four producer warps have read it. */
-/* The chunk's [diag | grad] MMAs of the P side (one thread), a fresh sum into COL_DG..:
- *   diag:  C x [q^2 block]                                                (2 K-steps)
- *   grad:  [DZ0 | DZ1 | DZ0] x [q hi block ; q hi block ; q lo block]   (6 K-steps)
- * a_base: the A tiles C, DZ0, DZ1 (A_BYTES apart); b_base: the package's PK_DG blocks. */
-template <int K, uint32_t A_BYTES, uint32_t A_LBO, uint32_t DGB_BYTES, uint32_t DG_LBO>
-__device__ __forceinline__ void issue_dg_p(uint32_t tmem_dg, uint32_t a_base, uint32_t b_base)
-{
-    constexpr uint32_t id = idesc_bf16_f32(128, DGShape<K>::NDG);
-    constexpr int AT[4] = {0, 1, 2, 1};   /* A tile of each term: C, DZ0, DZ1, DZ0 */
-    constexpr int BB[4] = {0, 1, 1, 2};   /* B block of each term: q^2, q hi, q hi, q lo */
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-#pragma unroll
-        for (int ks = 0; ks < 2; ++ks) {
-            const uint64_t ad = umma_desc_kmajor(a_base + AT[t] * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
-            const uint64_t bd = umma_desc_kmajor(b_base + BB[t] * DGB_BYTES + ks * 2 * DG_LBO, DG_LBO, 128);
-            tc_mma_bf16(tmem_dg, ad, bd, id, (t > 0 || ks > 0) ? 1u : 0u);
-        }
-    }
-}
-
 constexpr int MP_CTA = MP_THREADS + 32;
 
 template <int K, bool EMS>
@@ -912,7 +927,8 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
                     tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || ks > 0) ? 1u : 0u);
                 }
-                issue_dg_p<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase, bbase + C::PK_DG);
+                issue_grad<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase + C::A_BYTES,
+                                                                             bbase + C::PK_DG);
                 tc_commit(bar_h);
             }
             if (c + MP_NPKG < nchunk && wait(bar_h, (uint32_t)(c & 1))) {
@@ -936,38 +952,22 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         for (int k = 0; k < (EMS ? 1 : K); ++k) dd[k] = 0.0;
 #pragma unroll
         for (int k = 0; k < (EMS ? K : 1); ++k) hd[k] = 0.0;
-        /* the [diag | grad] accumulator of the last chunk whose MMAs completed, into FP64 */
+        /* the last chunk whose MMAs completed: its Hessian diagonal (columns 0..K-1 of the Hessian
+         * accumulator, cleared for the next chunk) and its gradient sums, into FP64 */
         auto drain_dg = [&]() {
-            if constexpr (!EMS) {
-                tc_fence_after_sync();
-                float v[16];
-                tmem_ld16(tmem + lane_base + C::COL_DG, v);
-#pragma unroll
-                for (int k = 0; k < K && k < 8; ++k) {
-                    dd[k] += (double)v[k];
-                    if (C::NDG == 16) gd[k] += (double)v[C::GOFF + k];
-                }
-                if constexpr (C::NDG == 32) {
-#pragma unroll
-                    for (int k = 8; k < K; ++k) dd[k] += (double)v[k];
-                    tmem_ld16(tmem + lane_base + C::COL_DG + 16u, v);
-#pragma unroll
-                    for (int k = 0; k < K; ++k) gd[k] += (double)v[k];
-                }
-                tc_fence_before_sync();
-            }
+            if constexpr (!EMS) drain_chunk<K, C::NDG>(tmem + lane_base, C::COL_H, C::COL_DG, dd, gd);
         };
         for (int c = 0; c < nchunk && ok; ++c) {
             const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
             const float *Qf = (const float *)(pk + C::PK_QF);
             const float2 *Sres = (const float2 *)(pk + C::PK_S);
             if constexpr (!EMS) {
-                if (c > 0) {   /* the MMAs of chunk c-1 are done: its [diag | grad] sums, free A tiles */
+                if (c > 0) {   /* the MMAs of chunk c-1 are done: its diagonal and gradient sums, free A tiles */
                     if (!wait(bar_h, (uint32_t)((c - 1) & 1))) break;
                     drain_dg();
                     if (c % MX_HBLOCK == 0) {   /* drain the Hessian block of chunks c-MX_HBLOCK .. c-1 */
                         tc_fence_after_sync();
-                        hess_drain<N, T>(tmem + lane_base + C::COL_H,
+                        hess_drain<K, N, T>(tmem + lane_base + C::COL_H,
                                          out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E, c == MX_HBLOCK, valid);
                         tc_fence_before_sync();
                     }
@@ -1105,7 +1105,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     if (producer && !EMS) {
         const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
         if (nchunk > 0) {
-#pragma unroll 1
+#pragma unroll
             for (int c0 = 0; c0 < N; c0 += 16) {
                 float v[16];
                 tmem_ld16(tmem + lane_base + C::COL_H + (uint32_t)c0, v);
@@ -1114,16 +1114,17 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const bool first = nchunk <= MX_HBLOCK;
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        if (c0 + e < T)
-                            o[c0 + e] = ok ? (first ? (double)v[e] : o[c0 + e] + (double)v[e])
-                                           : __longlong_as_double(0x7ff8000000000000LL);
+                        if (c0 + e < T) {
+                            double &x = o[col_out(K, c0 + e)];
+                            x = ok ? (first ? (double)v[e] : x + (double)v[e]) : __longlong_as_double(0x7ff8000000000000LL);
+                        }
                 }
             }
         } else if (valid) {
             double *o = out + ((size_t)blockIdx.y * J + j) * E;
             for (int e = 0; e < T; ++e) o[e] = 0.0;
         }
-        if (valid && nchunk > 0) {   /* the diagonal from the per-chunk [diag | grad] sums (FP64 across chunks) */
+        if (valid && nchunk > 0) {   /* the diagonal from the per-chunk sums (FP64 across chunks) */
             double *o = out + ((size_t)blockIdx.y * J + j) * E;
 #pragma unroll
             for (int k = 0; k < K; ++k)

@@ -147,6 +147,23 @@ __device__ __forceinline__ void tmem_ld16_raw(uint32_t taddr, uint32_t (&r)[16])
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+/* 16 consecutive FP32 columns of this thread's TMEM lane from registers (32x32b shape); complete
+ * once tmem_wait_st returns. */
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16])
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+                 "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+                 :: "r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                    "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+                    "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+                    "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+                    "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+                    "r"(__float_as_uint(v[15]))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 /* x = hi + lo with hi a TF32 value (round to nearest) and lo the FP32 remainder, itself rounded
  * to TF32: hi*b_hi + lo*b_hi + hi*b_lo recovers a*b to about 2^-21 relative. */
 __device__ __forceinline__ void tf32_split(float x, float &hi, float &lo)
