@@ -33,12 +33,17 @@ constexpr uint32_t MX_WAIT_LIMIT = 1u << 22;   /* polls; an MMA batch completes 
  * than 4 * MX_HBLOCK MMA accumulations (whose rounding is not to nearest) whatever J or I is. */
 constexpr int MX_HBLOCK = 256;
 
-/* Column order of the Hessian accumulators: the K diagonal pairs first (column k = pair (k, k)),
- * then the off-diagonal pairs (a, b), b < a, in the packed order of the FP64 partial rows.
- * col_out: the packed FP64 index a (a + 1) / 2 + b of column col's pair; col_pair: its factors. */
+/* Column order of the Hessian accumulators (T = K (K + 1) / 2 pairs): the K diagonal pairs first
+ * (column k = pair (k, k)), then the off-diagonal pairs (a, b), b < a, in the packed order of the
+ * FP64 partial rows, then K residual columns: column T + k holds the diagonal's B-operand rounding
+ * residual sum_j w (x_k^2 - bf16(x_k^2)), which belongs to entry (k, k).
+ * col_out: the packed FP64 index a (a + 1) / 2 + b that column col adds into; col_pair: the
+ * factors of a pair column. */
 __host__ __device__ constexpr int col_out(int K, int col)
 {
     if (col < K) return col * (col + 1) / 2 + col;
+    const int T = K * (K + 1) / 2;
+    if (col >= T) return (col - T) * (col - T + 1) / 2 + (col - T);
     int m = col - K, a = 1;
     while ((a + 1) * a / 2 <= m) ++a;
     return a * (a + 1) / 2 + (m - a * (a - 1) / 2);
@@ -53,8 +58,9 @@ __device__ __forceinline__ void col_pair(int K, int col, int &ka, int &kb)
     kb = m - a * (a - 1) / 2;
 }
 
-/* add (or, for the first block, store) TMEM columns col .. col+N-1 of this thread's lane into the
- * FP64 Hessian entries: column e holds the pair whose packed index is col_out(K, e) */
+/* add (or, for the first block, store) the Hessian accumulator's columns K .. T+K-1 (off-diagonal
+ * pairs and diagonal residuals; the diagonal columns 0..K-1 are drained every chunk) of this
+ * thread's lane into the FP64 entries o[col_out(K, e)] */
 template <int K, int N, int T>
 __device__ __forceinline__ void hess_drain(uint32_t taddr, double *o, bool first, bool valid)
 {
@@ -65,7 +71,7 @@ __device__ __forceinline__ void hess_drain(uint32_t taddr, double *o, bool first
         if (valid) {
 #pragma unroll
             for (int e = 0; e < 16; ++e)
-                if (c0 + e < T) {
+                if (c0 + e >= K && c0 + e < T + K) {
                     double &x = o[col_out(K, c0 + e)];
                     x = first ? (double)v[e] : x + (double)v[e];
                 }
@@ -171,7 +177,7 @@ template <int K> struct DGShape {
 template <int K>
 struct MQ {
     static constexpr int T = K * (K + 1) / 2;
-    static constexpr int N = ((T + 15) / 16) * 16;              /* Hessian MMA N (multiple of 16 for M = 128) */
+    static constexpr int N = ((T + K + 15) / 16) * 16;          /* Hessian MMA N: pairs + diagonal residuals, a multiple of 16 */
     static constexpr int KP = ((K + 7) / 8) * 8;                /* TF32 K extent of the qp MMAs */
     static constexpr int QPN = 2 * MQ_JC;                       /* qp MMA N: the chunk's p rows, then 1-p rows */
     static constexpr int NDG = DGShape<K>::NDG;
@@ -223,6 +229,35 @@ __device__ __forceinline__ void bf16_split(float x, uint16_t &hi, uint16_t &lo)
     lo = (uint16_t)(pack_bf16x2(r, 0.f) & 0xFFFFu);
 }
 
+/* BF16 pair of non-negative x, y rounded with dither: the 16 dropped bits plus d (< 2^16) carry into
+ * the kept ones, so x rounds up with probability (dropped bits + d) / 2^16 -- without bias when d
+ * is uniform on [0, 2^16) and independent of x.  Round to nearest is biased for these operands:
+ * applied to the Hessian weights it biased the BF16 Hessian diagonal by -3e-6 (Q side) and
+ * -4.5e-5 (P side) relative, the same in an exact-arithmetic emulation of the rounding alone. */
+__device__ __forceinline__ uint32_t pack_bf16x2_dither(float x, float y, uint32_t dx, uint32_t dy)
+{
+    return __byte_perm(__float_as_uint(x) + dx, __float_as_uint(y) + dy, 0x7632);
+}
+
+/* Dither stream of one accumulator row: a 32-bit LCG stepped once per cell pair; the pair's two
+ * cells use its high 16 bits and their complement modulo 2^16 (antithetic) */
+__device__ __forceinline__ uint32_t dither_seed(int64_t row, int64_t slice)
+{
+    return (uint32_t)row * 2654435761u + (uint32_t)slice * 40503u + 12345u;
+}
+__device__ __forceinline__ uint32_t dither_step(uint32_t &st)
+{
+    st = st * 1664525u + 1013904223u;
+    return st >> 16;
+}
+
+/* BF16 pair of the rounding residuals x - bf16(x), y - bf16(y) (bf16 rounding to nearest) */
+__device__ __forceinline__ uint32_t pack_bf16x2_res(float x, float y)
+{
+    const uint32_t h = pack_bf16x2(x, y);
+    return pack_bf16x2(x - __uint_as_float(h << 16), y - __uint_as_float(h & 0xFFFF0000u));
+}
+
 /* Row n's 8 BF16 values of granule kc (8 SNPs) in a B block of `rows` rows */
 __device__ __forceinline__ uint32_t bblk_off(int n, int kc, uint32_t lbo) { return (uint32_t)kc * lbo + 16u * (uint32_t)n; }
 
@@ -265,22 +300,30 @@ k_q_pack(const double *__restrict__ p, int64_t J, uint8_t *__restrict__ pkg)
         *g1 = hi;
     }
     __syncthreads();
-    /* pair-product tiles: task (term, kc, nn) writes column nn's pair (diagonal pairs first), 8 SNPs
-     * of k-chunk kc, at kc*16N + 16nn */
+    /* pair-product tiles: task (term, kc, nn) writes column nn's pair (diagonal pairs first, then the
+     * diagonal residual rows), 8 SNPs of k-chunk kc, at kc*16N + 16nn */
     for (int t = tid; t < 2 * 4 * N; t += 128) {
         const int term = t / (4 * N), rem = t - term * 4 * N;
         const int kc = rem / N, nn = rem - kc * N;
         uint32_t w[4] = {0u, 0u, 0u, 0u};
-        if (nn < T) {
+        if (nn < T + K) {
             int ka, kb;
-            col_pair(K, nn, ka, kb);
+            if (nn < T) col_pair(K, nn, ka, kb);
+            else ka = kb = nn - T;
             const float *src = pf + term * K * PS + kc * 8;
             const float4 a0 = *(const float4 *)(src + ka * PS), a1 = *(const float4 *)(src + ka * PS + 4);
             const float4 b0 = *(const float4 *)(src + kb * PS), b1 = *(const float4 *)(src + kb * PS + 4);
-            w[0] = pack_bf16x2(a0.x * b0.x, a0.y * b0.y);
-            w[1] = pack_bf16x2(a0.z * b0.z, a0.w * b0.w);
-            w[2] = pack_bf16x2(a1.x * b1.x, a1.y * b1.y);
-            w[3] = pack_bf16x2(a1.z * b1.z, a1.w * b1.w);
+            if (nn < T) {   /* pair products */
+                w[0] = pack_bf16x2(a0.x * b0.x, a0.y * b0.y);
+                w[1] = pack_bf16x2(a0.z * b0.z, a0.w * b0.w);
+                w[2] = pack_bf16x2(a1.x * b1.x, a1.y * b1.y);
+                w[3] = pack_bf16x2(a1.z * b1.z, a1.w * b1.w);
+            } else {        /* the rounding residuals of the diagonal pair products */
+                w[0] = pack_bf16x2_res(a0.x * b0.x, a0.y * b0.y);
+                w[1] = pack_bf16x2_res(a0.z * b0.z, a0.w * b0.w);
+                w[2] = pack_bf16x2_res(a1.x * b1.x, a1.y * b1.y);
+                w[3] = pack_bf16x2_res(a1.z * b1.z, a1.w * b1.w);
+            }
         }
         *(uint4 *)(buf + term * C::B_BYTES + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
     }
@@ -507,6 +550,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             sres = (float)(1.0 - sq);
         }
         const float2 sres2 = make_float2(sres, sres);
+        uint32_t dst = dither_seed(i, blockIdx.y);   /* rounding dither of this row's Hessian weights */
         double gd[K], dd[K], zsd = 0.0;   /* gradient sum_j (z1 - z2) p_k, Hessian diagonal, sum_j z2 */
 #pragma unroll
         for (int k = 0; k < K; ++k) gd[k] = dd[k] = 0.0;
@@ -566,8 +610,9 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const float2 w1 = __fmul2_rn(z1, r1), w2 = __fmul2_rn(z2, r2);
                     const float2 dz = __ffma2_rn(z2, make_float2(-1.f, -1.f), z1);
                     zs = __fadd2_rn(zs, z2);
-                    w1p[e] = pack_bf16x2(w1.x, w1.y);
-                    w2p[e] = pack_bf16x2(w2.x, w2.y);
+                    const uint32_t d0 = dither_step(dst), d1 = d0 ^ 0x8000u;
+                    w1p[e] = pack_bf16x2_dither(w1.x, w1.y, d0, d1);
+                    w2p[e] = pack_bf16x2_dither(w2.x, w2.y, d0, d1);
                     /* dz = hi + lo in BF16: hi rounded to nearest, lo the BF16 of the remainder */
                     const uint32_t h = pack_bf16x2(dz.x, dz.y);
                     const float2 hf = make_float2(__uint_as_float(h << 16), __uint_as_float(h & 0xFFFF0000u));
@@ -606,21 +651,21 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const bool first = nchunk <= MX_HBLOCK;
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        if (c0 + e < T) {
+                        if (c0 + e >= K && c0 + e < T + K) {
                             double &x = o[col_out(K, c0 + e)];
                             x = ok ? (first ? (double)v[e] : x + (double)v[e]) : __longlong_as_double(0x7ff8000000000000LL);
                         }
                 }
             }
         }
-        if (valid) {   /* the diagonal from the per-chunk sums (FP64 across chunks) */
+        if (valid) {   /* the diagonal: per-chunk sums (FP64 across chunks) plus the residual columns */
             double *o = out + ((size_t)blockIdx.y * I + i) * E;
             if (nchunk == 0) {
                 for (int e = 0; e < T; ++e) o[e] = 0.0;
             } else {
 #pragma unroll
                 for (int k = 0; k < K; ++k)
-                    o[k * (k + 1) / 2 + k] = ok ? dd[k] : __longlong_as_double(0x7ff8000000000000LL);
+                    o[k * (k + 1) / 2 + k] = ok ? o[k * (k + 1) / 2 + k] + dd[k] : __longlong_as_double(0x7ff8000000000000LL);
             }
         }
         tc_fence_before_sync();
@@ -663,7 +708,7 @@ constexpr int MP_NPKG = 3;
 template <int K>
 struct MP {
     static constexpr int T = K * (K + 1) / 2;
-    static constexpr int N = ((T + 15) / 16) * 16;
+    static constexpr int N = ((T + K + 15) / 16) * 16;          /* pairs + diagonal residuals */
     static constexpr int KP = ((K + 7) / 8) * 8;
     static constexpr int NDG = DGShape<K>::NDG;
     static constexpr uint32_t COL_OM = 32, COL_H = 64;          /* TMEM: qp 0..31, om 32..63, Hessian */
@@ -736,21 +781,29 @@ k_p_pack(const double *__restrict__ q, int64_t I, uint8_t *__restrict__ pkg)
         *g1 = hi;
     }
     __syncthreads();
-    /* QQ tile: task (kc, nn) writes column nn's pair (diagonal pairs first), 8 individuals of
-     * k-chunk kc, at kc*16N + 16nn */
+    /* QQ tile: task (kc, nn) writes column nn's pair (diagonal pairs first, then the diagonal
+     * residual rows), 8 individuals of k-chunk kc, at kc*16N + 16nn */
     for (int t = tid; t < 4 * N; t += 128) {
         const int kc = t / N, nn = t - kc * N;
         uint32_t w[4] = {0u, 0u, 0u, 0u};
-        if (nn < T) {
+        if (nn < T + K) {
             int ka, kb;
-            col_pair(K, nn, ka, kb);
+            if (nn < T) col_pair(K, nn, ka, kb);
+            else ka = kb = nn - T;
             const float *src = qf + kc * 8;
             const float4 a0 = *(const float4 *)(src + ka * C::QS), a1 = *(const float4 *)(src + ka * C::QS + 4);
             const float4 b0 = *(const float4 *)(src + kb * C::QS), b1 = *(const float4 *)(src + kb * C::QS + 4);
-            w[0] = pack_bf16x2(a0.x * b0.x, a0.y * b0.y);
-            w[1] = pack_bf16x2(a0.z * b0.z, a0.w * b0.w);
-            w[2] = pack_bf16x2(a1.x * b1.x, a1.y * b1.y);
-            w[3] = pack_bf16x2(a1.z * b1.z, a1.w * b1.w);
+            if (nn < T) {   /* pair products */
+                w[0] = pack_bf16x2(a0.x * b0.x, a0.y * b0.y);
+                w[1] = pack_bf16x2(a0.z * b0.z, a0.w * b0.w);
+                w[2] = pack_bf16x2(a1.x * b1.x, a1.y * b1.y);
+                w[3] = pack_bf16x2(a1.z * b1.z, a1.w * b1.w);
+            } else {        /* the rounding residuals of the diagonal pair products */
+                w[0] = pack_bf16x2_res(a0.x * b0.x, a0.y * b0.y);
+                w[1] = pack_bf16x2_res(a0.z * b0.z, a0.w * b0.w);
+                w[2] = pack_bf16x2_res(a1.x * b1.x, a1.y * b1.y);
+                w[3] = pack_bf16x2_res(a1.z * b1.z, a1.w * b1.w);
+            }
         }
         *(uint4 *)(buf + kc * C::B_LBO + 16 * nn) = make_uint4(w[0], w[1], w[2], w[3]);
     }
@@ -945,6 +998,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         if (nchunk > 1) gnext = col_load32(bed, pitch, j, valid, ia + MP_IC);
         /* gradient sum_i dz q_k (EM mode: sum_i nm g q_k / qp), Hessian diagonal, and the EM mode's
          * second sums */
+        uint32_t dst = dither_seed(j, blockIdx.y);   /* rounding dither of this row's Hessian weights */
         double gd[K], dd[EMS ? 1 : K], hd[EMS ? K : 1];
 #pragma unroll
         for (int k = 0; k < K; ++k) gd[k] = 0.0;
@@ -1020,7 +1074,8 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     } else {
                         const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
                         const float2 dz = __ffma2_rn(z2, make_float2(-1.f, -1.f), z1);   /* nm (g/qp - (2-g)/(1-qp)) */
-                        cp[e] = pack_bf16x2(cw.x, cw.y);
+                        const uint32_t d0 = dither_step(dst);
+                        cp[e] = pack_bf16x2_dither(cw.x, cw.y, d0, d0 ^ 0x8000u);
                         /* dz = hi + lo in BF16: hi rounded to nearest, lo the BF16 of the remainder */
                         const uint32_t h = pack_bf16x2(dz.x, dz.y);
                         const float2 hf = make_float2(__uint_as_float(h << 16), __uint_as_float(h & 0xFFFF0000u));
@@ -1114,7 +1169,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const bool first = nchunk <= MX_HBLOCK;
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        if (c0 + e < T) {
+                        if (c0 + e >= K && c0 + e < T + K) {
                             double &x = o[col_out(K, c0 + e)];
                             x = ok ? (first ? (double)v[e] : x + (double)v[e]) : __longlong_as_double(0x7ff8000000000000LL);
                         }
@@ -1124,11 +1179,11 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             double *o = out + ((size_t)blockIdx.y * J + j) * E;
             for (int e = 0; e < T; ++e) o[e] = 0.0;
         }
-        if (valid && nchunk > 0) {   /* the diagonal from the per-chunk sums (FP64 across chunks) */
+        if (valid && nchunk > 0) {   /* the diagonal: per-chunk sums (FP64 across chunks) plus the residual columns */
             double *o = out + ((size_t)blockIdx.y * J + j) * E;
 #pragma unroll
             for (int k = 0; k < K; ++k)
-                o[k * (k + 1) / 2 + k] = ok ? diag_keep[k] : __longlong_as_double(0x7ff8000000000000LL);
+                o[k * (k + 1) / 2 + k] = ok ? o[k * (k + 1) / 2 + k] + diag_keep[k] : __longlong_as_double(0x7ff8000000000000LL);
         }
     }
     tc_fence_before_sync();

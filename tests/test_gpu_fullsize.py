@@ -10,7 +10,8 @@
   against the oracle on a subset of rows (512 individuals x all SNPs for the Q side, 256 SNPs x
   all individuals for the P side: each row of a sweep is independent of the others, so the
   subset runs the full reduction), and the mixed form against the FP64 engine at the full size,
-  within the bounds the precision statement gives.
+  within the bounds the precision statement gives (Hessian 1.1e-2 of the row maximum, diagonal
+  unbiased to 1e-6).
 
 Tolerances as in test_gpu_parity: FP64 passes 1e-10 relative (row-wise for sums with
 cancellation), SQP steps 1e-9 absolute with QP statuses equal to the oracle's QPs run on the
@@ -146,5 +147,6 @@ def test_c3_full_size_fp64_rows_match_oracle_and_mixed_within_bounds(oa, orc):
         h64.close(); hmx.close()
     print("C3_PRECISION " + json.dumps(report))
     assert report["q"]["grad_max"] < 1e-5 and report["p"]["grad_max"] < 1e-4
-    assert report["q"]["hess_max"] < 2e-2 and report["p"]["hess_max"] < 2e-2
+    assert report["q"]["hess_max"] < 1.1e-2 and report["p"]["hess_max"] < 1.1e-2
+    assert abs(report["q"]["diag_bias_mean"]) < 1e-6 and abs(report["p"]["diag_bias_mean"]) < 1e-6
     assert abs(report["loglik"]["basic_rel"]) < 1e-8 and abs(report["loglik"]["qn_rel"]) < 1e-8
