@@ -164,6 +164,13 @@ int admix_set_fixed(admix_ctx *h, int32_t fix_q, int32_t fix_p);
  * with the same message, and the flag is cleared, so the handle stays usable.  Mixed-form
  * handles only (ADMIX_ERR_STATE otherwise). */
 int admix_selftest_wait_timeout(admix_ctx *h);
+/* (No counterpart in the reference.)  Diagnostic of the tensor-core arithmetic the mixed form is
+ * designed around: d[128 x 16] (row-major FP32) = sum over K-steps s < nsteps (1..4) of
+ * A[:, 16s:16s+16] * B[:, 16s:16s+16]^T, one tcgen05 BF16 MMA per step with the FP32 accumulator
+ * in tensor memory.  a: 128 x 64 and b: 16 x 64 row-major BF16 bit patterns (host memory);
+ * a_in_tmem = 1 reads A from tensor memory instead of shared memory.  Returns ADMIX_OK,
+ * ADMIX_ERR_ARG or ADMIX_ERR_CUDA (no message; no handle needed). */
+int admix_tc_probe(const uint16_t *a, const uint16_t *b, float *d, int32_t nsteps, int32_t a_in_tmem);
 int admix_qn_iteration(admix_ctx *h, int32_t iter, admix_iterinfo *out);
 /* admixture_qn!'s `mode` keyword (algorithms_outer.jl:63-65,126-137): ADMIX_QN_ZAL (default,
  * update_UV! / update_QN!, quasi_newton.jl:5-9,29-31) or ADMIX_QN_LBQN (limited-memory Broyden,

@@ -91,6 +91,7 @@ ADMIX_SIGNATURES = {
     "admix_update_p": (C.c_int, [_P, C.c_int32, _I32]),
     "admix_set_fixed": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "admix_selftest_wait_timeout": (C.c_int, [_P]),
+    "admix_tc_probe": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
     "admix_qn_iteration": (C.c_int, [_P, C.c_int32, C.POINTER(IterInfo)]),
     "admix_run_qn": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32, C.POINTER(IterInfo), _I32, _I32]),
     "admix_decode_counts": (C.c_int, [_P, _I64, _I64]),

@@ -1209,8 +1209,9 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
  * products q1 p2, q2 p1, q2 p2 are of random sign.
  *
  * Per cell the CUDA cores then form qp^g (1-qp)^(2-g) (1 when missing) and fold it into a
- * running product: two cells' factors multiplied in FP32, one FP64 multiply per pair, the
- * exponent moved into an integer every 16 cells, one log per thread at the end.
+ * running product: four cells' factors multiplied in FP32 (with an exact 2^60 scale), one FP64
+ * multiply per four cells, the exponent moved into an integer every 16 cells, one log per thread
+ * at the end.
  *
  * Roles as in the sweeps: warps 0-3 producers (thread = SNP = TMEM lane), warp 4 controller
  * (bulk copies of the per-chunk individual packages, MMA issue).  TMEM holds two chunk buffers
@@ -1427,8 +1428,9 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
                         const float2 l01 = make_float2(__uint_as_float(ra[e]), __uint_as_float(ra[e + 1]));
                         const float2 l2 = make_float2(__uint_as_float(rb[e]), __uint_as_float(rb[e + 1]));
                         const float2 qp = __fadd2_rn(l01, l2);
-                        const float2 om = __fadd2_rn(__ffma2_rn(l01, make_float2(-1.f, -1.f), make_float2(1.f, 1.f)),
-                                                     make_float2(-l2.x, -l2.y));
+                        /* (1 - L01) - L2: 1 - L01 is exact, the subtraction rounds once */
+                        const float2 om = __ffma2_rn(l2, make_float2(-1.f, -1.f),
+                                                     __ffma2_rn(l01, make_float2(-1.f, -1.f), make_float2(1.f, 1.f)));
                         const float2 oo = __fmul2_rn(om, om), qo = __fmul2_rn(qp, om), qq = __fmul2_rn(qp, qp);
                         const int bp = 2 * e;   /* this pair's 4 code bits in w */
                         const bool lo0 = (w >> bp) & 1u, hi0 = (w >> (bp + 1)) & 1u;
@@ -1436,15 +1438,16 @@ k_loglik_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t pi
                         f[2 * hm] = hi0 ? (lo0 ? qq.x : qo.x) : (lo0 ? 1.f : oo.x);
                         f[2 * hm + 1] = hi1 ? (lo1 ? qq.y : qo.y) : (lo1 ? 1.f : oo.y);
                     }
-                    /* each pair's product (factors >= 1e-10 inside the projections' bounds: >= 1e-20,
-                     * normal in FP32), then into the FP64 running product */
+                    /* each pair's product (factors >= 1e-10 inside the projections' bounds: in
+                     * [1e-20, 1]), then the four cells' product scaled by 2^60 (exact) so that it
+                     * stays normal in FP32 ([1e-22, 1.2e18]), then into the FP64 running product */
                     const float2 ff = __fmul2_rn(make_float2(f[0], f[2]), make_float2(f[1], f[3]));
-                    prod *= (double)ff.x;
-                    prod *= (double)ff.y;
+                    prod *= (double)(ff.x * (ff.y * 1152921504606846976.0f));
                 }
-                /* 16 cells: a product >= 1e-160 stays normal; move its exponent into the integer */
+                /* 16 cells: the product stays in [1e-88, 1e73]; move its exponent (less the four
+                 * 2^60 scales) into the integer */
                 const int64_t bits = __double_as_longlong(prod);
-                ex += ((bits >> 52) & 0x7FF) - 1023;
+                ex += ((bits >> 52) & 0x7FF) - 1023 - 240;
                 prod = __longlong_as_double((bits & ~(0x7FFLL << 52)) | (1023LL << 52));
             }
             if (c + 1 < nchunk) {
