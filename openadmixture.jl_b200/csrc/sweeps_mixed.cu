@@ -353,23 +353,21 @@ __device__ __forceinline__ void issue_qp(uint32_t tmem, const uint8_t *sm, const
     }
 }
 
-/* The chunk's gradient MMAs (one thread), a fresh sum into TMEM columns COL_DG..:
- *   DZ0 x [hi | lo block]   dz_hi p_hi in columns 0..K-1, dz_hi p_lo in K..2K-1   (2 K-steps)
- *   DZ1 x [hi | 0 block]    dz_lo p_hi added into columns 0..K-1                   (2 K-steps)
+/* K-step ks (0 or 1) of a chunk's gradient MMAs (one thread), a fresh sum into TMEM columns
+ * COL_DG.. that K-step 0 starts:
+ *   DZ0 x [hi | lo block]   dz_hi p_hi in columns 0..K-1, dz_hi p_lo in K..2K-1
+ *   DZ1 x [hi | 0 block]    dz_lo p_hi added into columns 0..K-1
  * a_dz: the A tile DZ0 (DZ1 follows at +A_BYTES); b_base: the package's two gradient B blocks.
  * Shared by both sides (P side: p -> q). */
 template <int K, uint32_t A_BYTES, uint32_t A_LBO, uint32_t DGB_BYTES, uint32_t DG_LBO>
-__device__ __forceinline__ void issue_grad(uint32_t tmem_dg, uint32_t a_dz, uint32_t b_base)
+__device__ __forceinline__ void issue_grad(uint32_t tmem_dg, uint32_t a_dz, uint32_t b_base, int ks)
 {
     constexpr uint32_t id = idesc_bf16_f32(128, DGShape<K>::NDG);
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-#pragma unroll
-        for (int ks = 0; ks < 2; ++ks) {
-            const uint64_t ad = umma_desc_kmajor(a_dz + t * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
-            const uint64_t bd = umma_desc_kmajor(b_base + t * DGB_BYTES + ks * 2 * DG_LBO, DG_LBO, 128);
-            tc_mma_bf16(tmem_dg, ad, bd, id, (t > 0 || ks > 0) ? 1u : 0u);
-        }
+        const uint64_t ad = umma_desc_kmajor(a_dz + t * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
+        const uint64_t bd = umma_desc_kmajor(b_base + t * DGB_BYTES + ks * 2 * DG_LBO, DG_LBO, 128);
+        tc_mma_bf16(tmem_dg, ad, bd, id, (t > 0 || ks > 0) ? 1u : 0u);
     }
 }
 
@@ -391,11 +389,11 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
     /* qp ready, qp consumed (4 warps), A tiles written (4 warps), the chunk's Hessian and
      * gradient MMAs done, G staged [2], package [NPKG] */
-    __shared__ uint64_t mbar[6 + MQ_NPKG];
+    __shared__ uint64_t mbar[7 + MQ_NPKG];
     __shared__ uint32_t tmem_holder;
     __shared__ volatile int abort_flag;
     uint64_t *bar_qp = &mbar[0], *bar_qfree = &mbar[1], *bar_afull = &mbar[2], *bar_h = &mbar[3];
-    uint64_t *bar_g = &mbar[4], *bar_p = &mbar[6];
+    uint64_t *bar_g = &mbar[4], *bar_p = &mbar[6], *bar_ahalf = &mbar[6 + MQ_NPKG];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool producer = warp < 4;
@@ -413,6 +411,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         mbar_init(bar_qp, 1);
         mbar_init(bar_qfree, 4);
         mbar_init(bar_afull, 4);
+        mbar_init(bar_ahalf, 4);
         mbar_init(bar_h, 1);
         mbar_init(&bar_g[0], 1);
         mbar_init(&bar_g[1], 1);
@@ -495,7 +494,24 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             tc_commit(bar_qp);
         }
         constexpr uint32_t idesc = idesc_bf16_f32(128, N);
+        /* K-step ks of chunk c's Hessian and gradient MMAs (leader thread) */
+        auto issue_ks = [&](int c, int ks) {
+            tc_fence_after_sync();
+            const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
+            const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
+#pragma unroll
+            for (int term = 0; term < 2; ++term) {
+                const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
+                const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
+                tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || term > 0 || ks > 0) ? 1u : 0u);
+            }
+            issue_grad<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase + 2 * C::A_BYTES,
+                                                                         bbase + C::PK_DG, ks);
+        };
         for (int c = 0; c < nchunk && ok; ++c) {
+            /* the first K-step (SNPs 0-15) of chunk c as soon as the producers wrote it, so its MMAs
+             * run while they compute the second */
+            if (wait(bar_ahalf, (uint32_t)(c & 1)) && leader) issue_ks(c, 0);
             /* qp of chunk c+1 once its package landed and the producers read qp of chunk c */
             if (c + 1 < nchunk) {
                 const int cn = c + 1;
@@ -506,23 +522,10 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     tc_commit(bar_qp);
                 }
             }
-            /* Hessian and gradient MMAs of chunk c once the producers wrote its A tiles */
+            /* the second K-step once the producers wrote the rest of chunk c's A tiles */
             if (wait(bar_afull, (uint32_t)(c & 1))) {
                 if (leader) {
-                    tc_fence_after_sync();
-                    const uint8_t *pk = sm + C::OFF_PKG + (c % MQ_NPKG) * C::PKG;
-                    const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
-#pragma unroll
-                    for (int term = 0; term < 2; ++term) {
-#pragma unroll
-                        for (int ks = 0; ks < 2; ++ks) {
-                            const uint64_t ad = umma_desc_kmajor(abase + term * C::A_BYTES + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
-                            const uint64_t bd = umma_desc_kmajor(bbase + term * C::B_BYTES + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
-                            tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || term > 0 || ks > 0) ? 1u : 0u);
-                        }
-                    }
-                    issue_grad<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase + 2 * C::A_BYTES,
-                                                                                 bbase + C::PK_DG);
+                    issue_ks(c, 1);
                     tc_commit(bar_h);
                 }
                 /* the producers are done with G buffer c & 1: stage chunk c+2 into it */
@@ -624,6 +627,11 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(w2p[0], w2p[1], w2p[2], w2p[3]);
                 *(uint4 *)(At + 2 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d0p[0], d0p[1], d0p[2], d0p[3]);
                 *(uint4 *)(At + 3 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d1p[0], d1p[1], d1p[2], d1p[3]);
+                if (kc == 1) {   /* the first K-step's A tiles are written: its MMAs may start */
+                    fence_async_smem();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(bar_ahalf);
+                }
             }
             zsd += (double)zs.x + (double)zs.y;
             fence_async_smem();
@@ -952,6 +960,16 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             tc_commit(bar_qp);
         }
         constexpr uint32_t idesc = idesc_bf16_f32(128, N);
+        /* K-step ks of chunk c's Hessian and gradient MMAs (leader thread) */
+        auto issue_ks = [&](int c, int ks) {
+            const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
+            const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
+            const uint64_t ad = umma_desc_kmajor(abase + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
+            const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
+            tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || ks > 0) ? 1u : 0u);
+            issue_grad<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase + C::A_BYTES,
+                                                                         bbase + C::PK_DG, ks);
+        };
         for (int c = 0; c < nchunk && ok; ++c) {
             if (c + 1 < nchunk) {
                 const int cn = c + 1;
@@ -970,18 +988,12 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 }
                 continue;
             }
+            /* both K-steps once the producers wrote the chunk's A tiles (issuing the first K-step
+             * at half time, as the Q sweep does, measured 1 % slower here) */
             if (wait(bar_afull, (uint32_t)(c & 1)) && leader) {
                 tc_fence_after_sync();
-                const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
-                const uint32_t abase = smem_u32(At), bbase = smem_u32(pk);
-#pragma unroll
-                for (int ks = 0; ks < 2; ++ks) {
-                    const uint64_t ad = umma_desc_kmajor(abase + ks * 2 * C::A_LBO, C::A_LBO, C::A_SBO);
-                    const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
-                    tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || ks > 0) ? 1u : 0u);
-                }
-                issue_grad<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase + C::A_BYTES,
-                                                                             bbase + C::PK_DG);
+                issue_ks(c, 0);
+                issue_ks(c, 1);
                 tc_commit(bar_h);
             }
             if (c + MP_NPKG < nchunk && wait(bar_h, (uint32_t)(c & 1))) {
