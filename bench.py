@@ -310,7 +310,7 @@ def _hit(r: dict, target: float):
 
 def ttc_legs(oa, g, spec, rank, world, mixed: bool, plain: bool) -> dict:
     """Time to converge (reldiff < 1e-7, admixture_qn's test) from the start of initialisation:
-    the chosen form from the learned warm start (sketch + MLP + closed-form P step, no EM; when a
+    the chosen form from the learned warm start (sketch + MLP + closed-form P step + LEARNED_EM EM; when a
     model for K applies) and from the random start + 5 EM iterations; with plain=True also the
     plain FP64 form from the random start + 5 EM, whose final log-likelihood sets the target
     (within 1e-6 relative) that every leg is scored against.  Wall-clock seconds with the device

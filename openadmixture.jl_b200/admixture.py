@@ -359,8 +359,8 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
     init_q (K x I) / init_p (K x J): as in the reference, EM priming runs unless both are given
     (driver.jl:180); a given one overwrites the primed value.  warm_start ("learned", a model
     path or a WarmStartMLP) starts from the learned encoder's Q and the closed-form P instead
-    of the random start, with no EM; where no model applies it falls back to the random start +
-    EM.  Explicit init_q / init_p take precedence over the warm start.  stream_block keeps the
+    of the random start, followed by warmstart.LEARNED_EM EM iterations instead of
+    admix_n_em_iters; where no model applies it falls back to the random start + EM.  Explicit init_q / init_p take precedence over the warm start.  stream_block keeps the
     genotypes in host memory and streams them in blocks of that many SNPs (cohorts larger than
     device memory).
 
@@ -383,6 +383,7 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
     d = AdmixData(g.I, g.J, K, Q, rng=rng)
     d_cu, g_cu = _cu_admixture_base(d, g, g.I, g.J, flags=flags, stream_block=stream_block)
     try:
+        learned = False
         if warm_start is not None and (init_q is None or init_p is None):
             from . import warmstart
             info = {}
@@ -390,6 +391,7 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
             if start is not None:
                 if not quiet:
                     print("Starting from the learned warm start")
+                learned = init_q is None and init_p is None
                 init_q = start[0].T if init_q is None else init_q
                 init_p = start[1].T if init_p is None else init_p
             elif not quiet:
@@ -400,6 +402,8 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
             d.q[:] = init_q
         if init_p is not None:
             d.p[:] = init_p
+        if learned:   # the learned start's P is a closed-form step behind its Q: EM to pair them
+            init_em(d, g, warmstart.LEARNED_EM, d_cu=d_cu, g_cu=g_cu, quiet=quiet)
         admixture_qn(d, g, admix_n_iter, admix_rtol, d_cu=d_cu, g_cu=g_cu, fix_q=fix_q, fix_p=fix_p,
                      verbose=verbose, progress_bar=progress_bar, quiet=quiet)
     finally:

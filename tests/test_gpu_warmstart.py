@@ -181,8 +181,8 @@ def test_learned_start_beats_random_start(oa, ws):
     # a millisecond, so wall time is launch noise; test_committed_model_gain compares seconds):
     # a QN iteration is 6 passes (4 sweeps, 2 log-likelihoods), an EM iteration 3 (2 sweeps and
     # its log-likelihood), the learned start 1 (the closed-form P step; sketch and encoder read
-    # 4096 SNPs).  The learned arm must need strictly fewer.
-    work_learned = 6 * learned["iterations_to_target"] + 1
+    # 4096 SNPs) plus its LEARNED_EM EM iterations.  The learned arm must need strictly fewer.
+    work_learned = 6 * learned["iterations_to_target"] + 1 + 3 * ws.LEARNED_EM
     work_rand = 3 * 5 + 6 * rand["iterations_to_target"]
     assert work_learned < work_rand, (learned["iterations_to_target"], rand["iterations_to_target"], t_pred)
     # the learned start ends at the same optimum
