@@ -388,12 +388,13 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
     /* qp ready, qp consumed (4 warps), A tiles written (4 warps), the chunk's Hessian and
-     * gradient MMAs done, G staged [2], package [NPKG] */
-    __shared__ uint64_t mbar[7 + MQ_NPKG];
+     * gradient MMAs done, G staged [2], package [NPKG], first half of the A tiles written (4
+     * warps), the first K-step's MMAs done */
+    __shared__ uint64_t mbar[8 + MQ_NPKG];
     __shared__ uint32_t tmem_holder;
     __shared__ volatile int abort_flag;
     uint64_t *bar_qp = &mbar[0], *bar_qfree = &mbar[1], *bar_afull = &mbar[2], *bar_h = &mbar[3];
-    uint64_t *bar_g = &mbar[4], *bar_p = &mbar[6], *bar_ahalf = &mbar[6 + MQ_NPKG];
+    uint64_t *bar_g = &mbar[4], *bar_p = &mbar[6], *bar_ahalf = &mbar[6 + MQ_NPKG], *bar_h0 = &mbar[7 + MQ_NPKG];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool producer = warp < 4;
@@ -412,6 +413,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         mbar_init(bar_qfree, 4);
         mbar_init(bar_afull, 4);
         mbar_init(bar_ahalf, 4);
+        mbar_init(bar_h0, 1);
         mbar_init(bar_h, 1);
         mbar_init(&bar_g[0], 1);
         mbar_init(&bar_g[1], 1);
@@ -511,7 +513,10 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         for (int c = 0; c < nchunk && ok; ++c) {
             /* the first K-step (SNPs 0-15) of chunk c as soon as the producers wrote it, so its MMAs
              * run while they compute the second */
-            if (wait(bar_ahalf, (uint32_t)(c & 1)) && leader) issue_ks(c, 0);
+            if (wait(bar_ahalf, (uint32_t)(c & 1)) && leader) {
+                issue_ks(c, 0);
+                tc_commit(bar_h0);
+            }
             /* qp of chunk c+1 once its package landed and the producers read qp of chunk c */
             if (c + 1 < nchunk) {
                 const int cn = c + 1;
@@ -562,16 +567,8 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         auto drain_dg = [&]() { drain_chunk<K, C::NDG>(tmem + lane_base, C::COL_H, C::COL_DG, dd, gd); };
         for (int c = 0; c < nchunk && ok; ++c) {
             const uint8_t *Gb = sm + C::OFF_G + (c & 1) * C::GBUF;
-            if (c > 0) {   /* the MMAs of chunk c-1 are done: its diagonal and gradient sums, free A tiles */
-                if (!wait(bar_h, (uint32_t)((c - 1) & 1))) break;
-                drain_dg();
-                if (c % MX_HBLOCK == 0) {   /* drain the Hessian block of chunks c-MX_HBLOCK .. c-1 */
-                    tc_fence_after_sync();
-                    hess_drain<K, N, T>(tmem + lane_base + C::COL_H, out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E,
-                                     c == MX_HBLOCK, valid);
-                    tc_fence_before_sync();
-                }
-            }
+            /* chunk c-1's first K-step MMAs are done: the A tiles' first half is free */
+            if (c > 0 && !wait(bar_h0, (uint32_t)((c - 1) & 1))) break;
             /* qp / om of the chunk's 32 SNPs, read in two halves of 16 columns (SNPs 0-15, then
              * 16-31) to keep the producer within its registers */
             uint32_t rq[16], ro[16];
@@ -627,7 +624,19 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(w2p[0], w2p[1], w2p[2], w2p[3]);
                 *(uint4 *)(At + 2 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d0p[0], d0p[1], d0p[2], d0p[3]);
                 *(uint4 *)(At + 3 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d1p[0], d1p[1], d1p[2], d1p[3]);
-                if (kc == 1) {   /* the first K-step's A tiles are written: its MMAs may start */
+                if (kc == 1) {
+                    /* all of chunk c-1's MMAs are done: its diagonal and gradient sums (and, at a block
+                     * boundary, the Hessian block), and the A tiles' second half is free */
+                    if (c > 0 && wait(bar_h, (uint32_t)((c - 1) & 1))) {
+                        drain_dg();
+                        if (c % MX_HBLOCK == 0) {   /* the Hessian block of chunks c-MX_HBLOCK .. c-1 */
+                            tc_fence_after_sync();
+                            hess_drain<K, N, T>(tmem + lane_base + C::COL_H,
+                                                out + ((size_t)blockIdx.y * I + (valid ? i : 0)) * E, c == MX_HBLOCK, valid);
+                            tc_fence_before_sync();
+                        }
+                    }
+                    /* the first K-step's A tiles are written and chunk c-1 drained: its MMAs may start */
                     fence_async_smem();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(bar_ahalf);
@@ -683,6 +692,8 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     /* controller: the same three CTA-wide barriers as the producers' epilogue */
     ok = __syncthreads_and(ok);
     if (!ok && tid == MQ_THREADS) {
+        mbar_wait_bounded(bar_h0, 0u, 1024u);
+        mbar_wait_bounded(bar_h0, 1u, 1024u);
         mbar_wait_bounded(bar_h, 0u, 1024u);
         mbar_wait_bounded(bar_h, 1u, 1024u);
         mbar_wait_bounded(bar_qp, 0u, 1024u);
@@ -872,13 +883,14 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     constexpr int T = C::T, N = C::N, E = EMS ? 2 * K : C::E;
     extern __shared__ __align__(1024) uint8_t smraw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-    /* qp ready, qp consumed (4 warps), C tile written (4 warps), Hessian done, package landed [3],
-     * package read (4 warps, EM sums only) [3] */
-    __shared__ uint64_t mbar[4 + 2 * MP_NPKG];
+    /* qp ready, qp consumed (4 warps), A tiles written (4 warps), the chunk's MMAs done, package
+     * landed [3], package read (4 warps, EM sums only) [3], first half of the A tiles written (4
+     * warps), the first K-step's MMAs done */
+    __shared__ uint64_t mbar[6 + 2 * MP_NPKG];
     __shared__ uint32_t tmem_holder;
     __shared__ volatile int abort_flag;
     uint64_t *bar_qp = &mbar[0], *bar_qfree = &mbar[1], *bar_afull = &mbar[2], *bar_h = &mbar[3], *bar_p = &mbar[4];
-    uint64_t *bar_read = &mbar[4 + MP_NPKG];
+    uint64_t *bar_read = &mbar[4 + MP_NPKG], *bar_ahalf = &mbar[4 + 2 * MP_NPKG], *bar_h0 = &mbar[5 + 2 * MP_NPKG];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool producer = warp < 4;
@@ -901,6 +913,8 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         mbar_init(bar_h, 1);
         for (int b = 0; b < MP_NPKG; ++b) mbar_init(&bar_p[b], 1);
         for (int b = 0; b < MP_NPKG; ++b) mbar_init(&bar_read[b], 4);
+        mbar_init(bar_ahalf, 4);
+        mbar_init(bar_h0, 1);
         abort_flag = 0;
         mbar_fence_init();
     }
@@ -971,6 +985,13 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                                                                          bbase + C::PK_DG, ks);
         };
         for (int c = 0; c < nchunk && ok; ++c) {
+            if constexpr (!EMS) {   /* the first K-step (individuals 0-15) as soon as it is written */
+                if (wait(bar_ahalf, (uint32_t)(c & 1)) && leader) {
+                    tc_fence_after_sync();
+                    issue_ks(c, 0);
+                    tc_commit(bar_h0);
+                }
+            }
             if (c + 1 < nchunk) {
                 const int cn = c + 1;
                 const bool landed = wait(&bar_p[cn % MP_NPKG], (uint32_t)((cn / MP_NPKG) & 1));
@@ -988,11 +1009,9 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 }
                 continue;
             }
-            /* both K-steps once the producers wrote the chunk's A tiles (issuing the first K-step
-             * at half time, as the Q sweep does, measured 1 % slower here) */
+            /* the second K-step once the producers wrote the rest of the chunk's A tiles */
             if (wait(bar_afull, (uint32_t)(c & 1)) && leader) {
                 tc_fence_after_sync();
-                issue_ks(c, 0);
                 issue_ks(c, 1);
                 tc_commit(bar_h);
             }
@@ -1027,17 +1046,8 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             const uint8_t *pk = sm + C::OFF_PKG + (c % MP_NPKG) * C::PKG;
             const float *Qf = (const float *)(pk + C::PK_QF);
             const float2 *Sres = (const float2 *)(pk + C::PK_S);
-            if constexpr (!EMS) {
-                if (c > 0) {   /* the MMAs of chunk c-1 are done: its diagonal and gradient sums, free A tiles */
-                    if (!wait(bar_h, (uint32_t)((c - 1) & 1))) break;
-                    drain_dg();
-                    if (c % MX_HBLOCK == 0) {   /* drain the Hessian block of chunks c-MX_HBLOCK .. c-1 */
-                        tc_fence_after_sync();
-                        hess_drain<K, N, T>(tmem + lane_base + C::COL_H,
-                                         out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E, c == MX_HBLOCK, valid);
-                        tc_fence_before_sync();
-                    }
-                }
+            if constexpr (!EMS) {   /* chunk c-1's first K-step MMAs are done: the A tiles' first half is free */
+                if (c > 0 && !wait(bar_h0, (uint32_t)((c - 1) & 1))) break;
             }
             /* qp / om of the chunk's 32 individuals, read in two halves of 16 columns
              * (individuals 0-15, then 16-31) to keep the producer within its registers */
@@ -1100,6 +1110,20 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     *(uint4 *)(At + kc * C::A_LBO + 16 * tid) = make_uint4(cp[0], cp[1], cp[2], cp[3]);
                     *(uint4 *)(At + C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d0p[0], d0p[1], d0p[2], d0p[3]);
                     *(uint4 *)(At + 2 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d1p[0], d1p[1], d1p[2], d1p[3]);
+                    if (kc == 1) {   /* as on the Q side: drain chunk c-1, then release the first K-step */
+                        if (c > 0 && wait(bar_h, (uint32_t)((c - 1) & 1))) {
+                            drain_dg();
+                            if (c % MX_HBLOCK == 0) {
+                                tc_fence_after_sync();
+                                hess_drain<K, N, T>(tmem + lane_base + C::COL_H,
+                                                    out + ((size_t)blockIdx.y * J + (valid ? j : 0)) * E, c == MX_HBLOCK, valid);
+                                tc_fence_before_sync();
+                            }
+                        }
+                        fence_async_smem();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(bar_ahalf);
+                    }
                 } else {
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
@@ -1161,6 +1185,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
     }
     ok = __syncthreads_and(ok);
     if (!ok && tid == MP_THREADS) {
+        if constexpr (!EMS) { mbar_wait_bounded(bar_h0, 0u, 1024u); mbar_wait_bounded(bar_h0, 1u, 1024u); }
         mbar_wait_bounded(bar_h, 0u, 1024u);
         mbar_wait_bounded(bar_h, 1u, 1024u);
         mbar_wait_bounded(bar_qp, 0u, 1024u);
