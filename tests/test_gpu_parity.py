@@ -409,6 +409,41 @@ def test_streamed_handle_matches_resident_handle(oa, flags):
     hr.close(); hs.close()
 
 
+def test_streamed_handle_matches_oracle(oa, orc):
+    """The out-of-core path against the oracle directly (not only against the resident handle):
+    genotypes in host memory streamed in 3 SNP blocks (1024 + 1024 + 953), FP64 form -- decode
+    counts bit-exact, log-likelihood, Q- and P-side gradient and Hessian at 1e-10, EM priming and
+    QN iterations at the tolerances of the resident-handle parity tests."""
+    K = 4
+    g = _cohort(oa, I=437, J=3001, K=K, seed=54)
+    I, J = g.I, g.J
+    d = oa.AdmixData(I, J, K, 3, rng=7)
+    q, p = np.ascontiguousarray(d.x[:I]), np.ascontiguousarray(d.x[I:])
+    with oa.CuAdmixData(d, g, stream_block=1024) as h:
+        h.upload(oa.X, d.x)
+        snp, ind = h.decode_counts()
+        snp_o, ind_o = orc.decode_counts(g.data, I, J)
+        assert np.array_equal(snp, snp_o) and np.array_equal(ind, ind_o)
+        assert rel_err(h.loglik(oa.X), orc.loglik(g.data, I, J, K, q, p)) < FP64_TOL
+        H, z = h.grad_hess_q(oa.X, oa.X)
+        Ho, zo = orc.grad_hess_q(g.data, I, J, K, q, p)
+        assert _row_rel(H, Ho) < FP64_TOL and _row_rel(z, zo) < FP64_TOL
+        H, z = h.grad_hess_p(oa.X, oa.X)
+        Ho, zo = orc.grad_hess_p(g.data, I, J, K, q, p)
+        assert _row_rel(H, Ho) < FP64_TOL and _row_rel(z, zo) < FP64_TOL
+        r = orc.OracleRun(g.data, I, J, K, 3, d.x)
+        ll_em_o = r.init_em(3)
+        ll_em = oa.init_em(d, g, 3, d_cu=h, quiet=True)
+        assert rel_err(np.array(ll_em), np.array(ll_em_o)) < FP64_TOL
+        d.x[:] = r.x
+        d.ll_new = r.ll_new
+        recs = oa.admixture_qn(d, g, 4, 0.0, d_cu=h, quiet=True)
+    for it, rec in enumerate(recs, start=1):
+        o = r.qn_iteration(it)
+        for k in ("ll_prev", "ll_basic", "ll_qn", "ll_new"):
+            assert rel_err(rec[k], o[k]) < 1e-8, (it, k, rec[k], o[k])
+
+
 @pytest.mark.parametrize("flags", [0, 2])
 def test_run_admixture_streamed(oa, flags):
     g = _cohort(oa, I=300, J=2000, K=3, seed=53)
