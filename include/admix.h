@@ -164,6 +164,23 @@ int admix_set_fixed(admix_ctx *h, int32_t fix_q, int32_t fix_p);
  * with the same message, and the flag is cleared, so the handle stays usable.  Mixed-form
  * handles only (ADMIX_ERR_STATE otherwise). */
 int admix_selftest_wait_timeout(admix_ctx *h);
+/* --- SKFR AIM pre-selection (run_admixture's sparsity keyword, driver.jl:56-69; _filter_SKFR,
+ * driver.jl:80-101; the reference calls the third-party SparseKmeansFeatureRanking.jl) ---------
+ * Sparse k-means via feature ranking on the handle's genotypes, imputed and standardised per SNP:
+ * k-means++ seeding from a splitmix64 stream (seed), then centres, per-SNP scores, the `sparsity`
+ * SNPs of largest score kept and individuals reassigned on them, until no assignment changes or
+ * max_iter iterations; mode ADMIX_SKFR_GLOBAL keeps one SNP set for all clusters
+ * (sparsekmeans1), ADMIX_SKFR_LOCAL one per cluster (sparsekmeans2; the AIMs are their union).
+ * tries > 1 repeats from new seeds (the stream continues) and keeps the run of least
+ * within-cluster sum of squares (sparsekmeans_repeat).  k clusters (1..16).  Outputs: clusters
+ * (I cluster indices 0..k-1), aims (the selected SNPs, 0-based, increasing; at most
+ * aims_capacity written, *n_aims = how many there are), objective, iterations of the kept run.
+ * Device-resident handles only (ADMIX_ERR_UNSUPPORTED for streamed ones). */
+#define ADMIX_SKFR_GLOBAL 0
+#define ADMIX_SKFR_LOCAL  1
+int admix_skfr(admix_ctx *h, int32_t k, int64_t sparsity, int32_t mode, int32_t max_iter, int32_t tries,
+               uint64_t seed, int32_t *clusters, int32_t *aims, int64_t aims_capacity, int64_t *n_aims,
+               double *objective, int32_t *iterations);
 /* (No counterpart in the reference.)  Diagnostic of the tensor-core arithmetic the mixed form is
  * designed around: d[128 x 16] (row-major FP32) = sum over K-steps s < nsteps (1..4) of
  * A[:, 16s:16s+16] * B[:, 16s:16s+16]^T, one tcgen05 BF16 MMA per step with the FP32 accumulator

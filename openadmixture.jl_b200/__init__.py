@@ -8,7 +8,7 @@ side that mirrors the reference's Julia API over it.  Import it as ``openadmixtu
 from . import _native
 from ._native import AdmixError, IterInfo, ADMIX_FLAG_MIXED, ADMIX_FLAG_MU_GERSHGORIN, ADMIX_FLAG_MEAN_IMPUTE
 from .admixture import (AdmixData, CuAdmixData, X, X_NEXT, X_NEXT2, X_TMP, _cu_admixture_base,
-                        admixture_qn, em_p, em_q, init_em, loglikelihood, run_admixture, update_p,
+                        admixture_qn, em_p, em_q, init_em, loglikelihood, run_admixture, skfr, update_p,
                         update_q)
 from .bed import BedFormatError, DeviceGenotypes, Genotypes, read_bed, write_bed
 from .synth import COHORTS, CohortSpec, genotypes, genotypes_device, init_x, make_cohort, truth
@@ -19,7 +19,7 @@ __all__ = [
     "AdmixData", "CuAdmixData", "AdmixError", "IterInfo", "Genotypes", "DeviceGenotypes", "BedFormatError",
     "X", "X_NEXT", "X_NEXT2", "X_TMP", "ADMIX_FLAG_MIXED", "ADMIX_FLAG_MU_GERSHGORIN", "ADMIX_FLAG_MEAN_IMPUTE",
     "_cu_admixture_base", "admixture_qn", "em_p", "em_q", "init_em", "loglikelihood",
-    "run_admixture", "update_p", "update_q", "read_bed", "write_bed",
+    "run_admixture", "skfr", "update_p", "update_q", "read_bed", "write_bed",
     "COHORTS", "CohortSpec", "genotypes", "genotypes_device", "init_x", "make_cohort", "truth",
     "warmstart", "AdmixBatch", "BatchMember", "k_sweep", "run_restarts",
 ]

@@ -27,6 +27,7 @@ ADMIX_MAX_K = 16
 ADMIX_MAX_Q = 8
 
 ADMIX_QN_ZAL, ADMIX_QN_LBQN = 0, 1
+ADMIX_SKFR_GLOBAL, ADMIX_SKFR_LOCAL = 0, 1
 ADMIX_PASS_LOGLIK, ADMIX_PASS_QSWEEP, ADMIX_PASS_PSWEEP, ADMIX_PASS_QQP, ADMIX_PASS_PQP, ADMIX_PASS_EM = range(6)
 
 
@@ -92,6 +93,7 @@ ADMIX_SIGNATURES = {
     "admix_set_fixed": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "admix_selftest_wait_timeout": (C.c_int, [_P]),
     "admix_tc_probe": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
+    "admix_skfr": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, _I32, _I32, C.c_int64, _I64, _D, _I32]),
     "admix_qn_iteration": (C.c_int, [_P, C.c_int32, C.POINTER(IterInfo)]),
     "admix_run_qn": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32, C.POINTER(IterInfo), _I32, _I32]),
     "admix_decode_counts": (C.c_int, [_P, _I64, _I64]),

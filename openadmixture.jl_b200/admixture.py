@@ -345,7 +345,63 @@ def _admixture_qn_loop(d: AdmixData, d_cu: CuAdmixData, iter: int, rtol: float, 
     return recs
 
 
-def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter: int = 1000,
+def skfr(g, K: int, sparsity: int, *, mode: str = "global", max_iter: int = 50, tries: int = 1, rng: int = 0):
+    """Sparse k-means via feature ranking (the reference's SparseKmeansFeatureRanking.sparsekmeans1
+    for mode "global", sparsekmeans2 for "local", sparsekmeans_repeat for tries > 1; driver.jl:56-69,
+    80-101) on the device: K clusters of the individuals on the `sparsity` most informative SNPs of
+    the imputed, standardised genotypes.  Returns (clusters (I,) in 0..K-1, aims (the selected SNP
+    indices, 0-based and increasing), objective, iterations).  ``rng`` seeds the k-means++
+    seeding (a splitmix64 stream; the reference's Julia RNG is not reproduced)."""
+    modes = {"global": N.ADMIX_SKFR_GLOBAL, "local": N.ADMIX_SKFR_LOCAL}
+    mode = str(mode).lstrip(":")
+    if mode not in modes:
+        raise ValueError("skfr_mode can only be :global or :local")        # driver.jl:63
+    d = AdmixData(g.I, g.J, min(K, 16), 1, rng=rng)
+    with CuAdmixData(d, g) as h:
+        clusters = np.empty(g.I, dtype=np.int32)
+        cap = min(g.J, sparsity * (K if mode == "local" else 1))
+        aims = np.empty(max(cap, 1), dtype=np.int32)
+        n_aims = C.c_int64(0)
+        obj = C.c_double(0.0)
+        iters = C.c_int32(0)
+        h._chk(N.admix_lib().admix_skfr(h.handle, int(K), int(sparsity), modes[mode], int(max_iter), int(tries),
+                                        int(rng) & ((1 << 64) - 1), N.i32ptr(clusters), N.i32ptr(aims), cap,
+                                        C.byref(n_aims), C.byref(obj), C.byref(iters)))
+    return clusters, aims[: n_aims.value].copy(), obj.value, iters.value
+
+
+def _filter_skfr(g, K: int, sparsity: int, *, rng: int = 0, prefix=None, tries: int = 1, max_inner_iter: int = 50,
+                 mode: str = "global", source=None, quiet: bool = False):
+    """_filter_SKFR (driver.jl:80-101): SKFR, then the genotypes of the selected SNPs only --
+    written as `{prefix}_{K}_{sparsity}aims.bed` (.bim / .fam beside it, copied from the source's
+    where it has them) when a prefix is given -- returned with clusters and aims."""
+    clusters, aims, _, _ = skfr(g, K, sparsity, mode=mode, max_iter=max_inner_iter, tries=tries, rng=rng)
+    if isinstance(g, DeviceGenotypes):
+        import torch
+        sub = DeviceGenotypes(g.data.index_select(0, torch.as_tensor(aims, dtype=torch.long, device=g.data.device)),
+                              g.I, len(aims))
+    else:
+        sub = Genotypes(np.ascontiguousarray(np.asarray(g.data)[aims]), g.I, len(aims))
+    if prefix is not None:
+        from pathlib import Path
+        from .bed import write_bed
+        des = Path(f"{prefix}_{K}_{sparsity}aims.bed")
+        if not quiet:
+            print(des.with_suffix(""))
+        host = sub.to_host() if isinstance(sub, DeviceGenotypes) else sub
+        write_bed(des, host, write_sidecars=True)
+        if source is not None:                      # keep the source's identifiers
+            src = Path(source).with_suffix("")
+            if src.with_suffix(".fam").exists():
+                des.with_suffix(".fam").write_text(src.with_suffix(".fam").read_text())
+            if src.with_suffix(".bim").exists():
+                lines = src.with_suffix(".bim").read_text().splitlines()
+                des.with_suffix(".bim").write_text("".join(lines[j] + "\n" for j in aims))
+    return sub, clusters, aims
+
+
+def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, prefix=None, skfr_tries: int = 1,
+                  skfr_max_inner_iter: int = 50, skfr_mode: str = "global", admix_n_iter: int = 1000,
                   admix_rtol: float = 1e-7, admix_n_em_iters: int = 5, T=np.float64, Q: int = 3,
                   use_gpu: bool = True, verbose: bool = False, progress_bar: bool = False,
                   fix_q: bool = False, fix_p: bool = False, init_q=None, init_p=None,
@@ -354,23 +410,25 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
 
     ``filename`` is a .bed path, an in-memory Genotypes or a DeviceGenotypes.  ``rng`` is an
     integer seed of this engine's generator (the reference's Julia RNG streams are not
-    reproduced).  SKFR (sparsity) is not part of the likelihood engine and raises.
+    reproduced).  sparsity (an integer) first selects that many ancestry-informative SNPs with
+    SKFR on the device (`skfr`; skfr_mode, skfr_tries and skfr_max_inner_iter as the reference's
+    keywords) and runs the engine on them; the filtered genotypes are written as
+    `{prefix}_{K}_{sparsity}aims.bed` (prefix defaults to the .bed path without its suffix; no
+    file for in-memory genotypes without a prefix), and clusters and aims are returned.
 
     init_q (K x I) / init_p (K x J): as in the reference, EM priming runs unless both are given
     (driver.jl:180); a given one overwrites the primed value.  warm_start ("learned", a model
     path or a WarmStartMLP) starts from the learned encoder's Q and the closed-form P instead
     of the random start, followed by warmstart.LEARNED_EM EM iterations instead of
-    admix_n_em_iters; where no model applies it falls back to the random start + EM.  Explicit init_q / init_p take precedence over the warm start.  stream_block keeps the
-    genotypes in host memory and streams them in blocks of that many SNPs (cohorts larger than
-    device memory).
+    admix_n_em_iters; where no model applies it falls back to the random start + EM.  Explicit
+    init_q / init_p take precedence over the warm start.  stream_block keeps the genotypes in host
+    memory and streams them in blocks of that many SNPs (cohorts larger than device memory).
 
     T = Float32 (np.float32 or "Float32"): the reference then holds and computes every array in
     Float32 (AdmixData{T}, structs.jl:9-91) for speed.  Here it selects the mixed form
     (ADMIX_FLAG_MIXED: FP32 cells and tensor-core Hessians with FP64 sums, QPs and state), which
     is faster than the FP64 form and more accurate than an all-Float32 run; the returned
     AdmixData holds Float32 arrays."""
-    if sparsity is not None:
-        raise NotImplementedError("sparsity (SKFR AIM pre-selection) is outside the likelihood engine")
     if T in (np.float32, "Float32"):
         flags |= N.ADMIX_FLAG_MIXED
     elif T not in (np.float64, float, "Float64"):
@@ -378,6 +436,17 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
     if not use_gpu:
         raise NotImplementedError("use_gpu=False is the reference's CPU path; this engine runs on the GPU")
     g = filename if isinstance(filename, (Genotypes, DeviceGenotypes)) else read_bed(filename)
+    clusters = aims = None
+    if sparsity is not None:
+        if not isinstance(sparsity, (int, np.integer)):
+            raise NotImplementedError("sparsity: an integer (the reference's vector of sparsities writes one file per "
+                                      "value and does not run the likelihood engine)")
+        in_memory = isinstance(filename, (Genotypes, DeviceGenotypes))
+        if prefix is None and not in_memory:
+            prefix = str(filename)[:-4]
+        g, clusters, aims = _filter_skfr(g, K, int(sparsity), rng=rng, prefix=prefix, tries=skfr_tries,
+                                         max_inner_iter=skfr_max_inner_iter, mode=skfr_mode,
+                                         source=None if in_memory else filename, quiet=quiet)
     if not quiet:
         print(f"Loaded {g.I} samples and {g.J} SNPs")
     d = AdmixData(g.I, g.J, K, Q, rng=rng)
@@ -411,4 +480,4 @@ def run_admixture(filename, K: int, *, rng: int = 0, sparsity=None, admix_n_iter
     if T in (np.float32, "Float32"):
         for name in ("x", "x_next", "x_next2", "x_tmp"):
             setattr(d, name, getattr(d, name).astype(np.float32))
-    return d, None, None
+    return d, clusters, aims

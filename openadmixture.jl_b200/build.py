@@ -23,7 +23,7 @@ REPO = PKG.parent
 INCLUDE = REPO / "include"
 
 ENGINE_SOURCES = ["admix_capi.cu", "sweeps_f64.cu", "qp_batch.cu", "qn.cu", "loglik_noalloc.cu", "sweeps_mixed.cu", "mlp.cu",
-                  "tc_probe.cu"]
+                  "tc_probe.cu", "skfr.cu"]
 SYNTH_SOURCES = ["synth.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

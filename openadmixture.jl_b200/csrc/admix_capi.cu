@@ -681,6 +681,23 @@ int admix_grad_hess_p(admix_ctx *h, int32_t which_q, int32_t which_p, double *Xt
     return grad_hess_common(h, false, which_q, which_p, XtX, Xtz);
 }
 
+int admix_skfr(admix_ctx *h, int32_t k, int64_t sparsity, int32_t mode, int32_t max_iter, int32_t tries,
+               uint64_t seed, int32_t *clusters, int32_t *aims, int64_t aims_capacity, int64_t *n_aims,
+               double *objective, int32_t *iterations)
+{
+    if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");
+    if (!clusters || !aims || !n_aims || !objective || !iterations) return fail(h, ADMIX_ERR_ARG, "an output pointer is NULL");
+    if (k < 1 || k > 16) return fail(h, ADMIX_ERR_UNSUPPORTED, "k=%d outside [1, 16]", k);
+    if (sparsity < 1) return fail(h, ADMIX_ERR_ARG, "sparsity must be >= 1 (got %lld)", (long long)sparsity);
+    if (mode != ADMIX_SKFR_GLOBAL && mode != ADMIX_SKFR_LOCAL) return fail(h, ADMIX_ERR_ARG, "skfr mode can only be global (0) or local (1)");
+    if (max_iter < 1 || tries < 1) return fail(h, ADMIX_ERR_ARG, "max_iter and tries must be >= 1");
+    if (aims_capacity < 0) return fail(h, ADMIX_ERR_ARG, "aims_capacity < 0");
+    if (h->streamed) return fail(h, ADMIX_ERR_UNSUPPORTED, "SKFR needs device-resident genotypes");
+    CK(h, skfr_run(h->bed, h->pitch, h->I, h->J, k, sparsity, mode == ADMIX_SKFR_LOCAL ? 1 : 0, max_iter, tries, seed, h->st,
+                   clusters, aims, aims_capacity, n_aims, objective, iterations));
+    return ADMIX_OK;
+}
+
 int admix_selftest_wait_timeout(admix_ctx *h)
 {
     if (!h) return fail(nullptr, ADMIX_ERR_ARG, "handle is NULL");

@@ -28,6 +28,11 @@ cudaError_t launch_sweep_p_f64(int K, int mode, const uint8_t *bed, int64_t I, i
                                cudaStream_t st, const double *mu = nullptr);
 /* g.mu of the SnpLinAlg: mean non-missing dosage per SNP of the padded device genotypes */
 cudaError_t launch_snp_means(const uint8_t *bed, int64_t J, int64_t pitch, double *mu, cudaStream_t st);
+/* SKFR AIM pre-selection (csrc/skfr.cu) on padded device genotypes; clusters_out: I, aims_out:
+ * up to aims_capacity sorted SNP indices (n_aims: how many there are) */
+cudaError_t skfr_run(const uint8_t *bed, int64_t pitch, int64_t I, int64_t J, int K, int64_t sparsity, int local,
+                     int max_iter, int tries, uint64_t seed, cudaStream_t st, int32_t *clusters_out, int32_t *aims_out,
+                     int64_t aims_capacity, int64_t *n_aims, double *objective_out, int32_t *iters_out);
 /* fixed-order FP64 sum of n doubles into *dst (one block) */
 cudaError_t launch_sum_doubles(const double *src, int64_t n, double *dst, cudaStream_t st);
 cudaError_t launch_emq_finalize(int64_t I, int K, int64_t J, int S, const double *parts,

@@ -47,8 +47,9 @@ def test_create_rejects_bad_arguments_without_touching_a_gpu(oa):
     # device variant: a source pitch below ceil(I/4) is rejected before any device call
     assert lib.admix_create_device(40, 4, 3, 3, None, 9, 0, C.byref(h)) == N.ADMIX_ERR_ARG
     assert b"src_pitch" in lib.admix_last_error(None)
-    # the failure-reporting self-test needs a handle
+    # the failure-reporting self-test and SKFR need a handle
     assert lib.admix_selftest_wait_timeout(None) == N.ADMIX_ERR_ARG
+    assert lib.admix_skfr(None, 3, 10, 0, 50, 1, 0, None, None, 0, None, None, None) == N.ADMIX_ERR_ARG
     assert b"handle is NULL" in lib.admix_last_error(None)
 
 
@@ -58,8 +59,10 @@ def test_engine_requires_gpu_path(oa):
         oa.update_q(d, None, d_cu=None)
     with pytest.raises(NotImplementedError):
         oa.run_admixture(oa.Genotypes(np.zeros((8, 2), np.uint8), 8, 8), 2, use_gpu=False)
-    with pytest.raises(NotImplementedError):
-        oa.run_admixture(oa.Genotypes(np.zeros((8, 2), np.uint8), 8, 8), 2, sparsity=100)
+    with pytest.raises(NotImplementedError, match="an integer"):     # a vector of sparsities
+        oa.run_admixture(oa.Genotypes(np.zeros((8, 2), np.uint8), 8, 8), 2, sparsity=[100, 50])
+    with pytest.raises(ValueError, match="global or :local"):        # driver.jl:63
+        oa.run_admixture(oa.Genotypes(np.zeros((8, 2), np.uint8), 8, 8), 2, sparsity=4, skfr_mode=":nearest")
     with pytest.raises(NotImplementedError, match="Float64 and Float32"):
         oa.run_admixture(oa.Genotypes(np.zeros((8, 2), np.uint8), 8, 8), 2, T=np.float16)
 
