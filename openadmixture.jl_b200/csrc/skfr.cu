@@ -8,24 +8,30 @@
  *
  * Device work, all on the handle's padded genotypes (padding coded missing):
  *   - per-SNP class counts by popcount of the code bit planes (k_skfr_counts);
- *   - k-means++ seeding distances ||x_i - x_c||^2 over all SNPs: a thread owns 16 individuals (one
- *     32-bit word of a column) and a slice of SKFR_SLICE SNPs, FP64 sums per slice added in slice
- *     order (k_skfr_dist, k_skfr_dist_sum);
+ *   - k-means++ seeding distances ||x_i - x_c||^2 over all SNPs: the squared difference of every
+ *     (SNP, code) to the centre in a table (k_skfr_sqtab), then a thread owns 16 individuals (one
+ *     32-bit word of a column) and a slice of SKFR_SLICE SNPs, adding table entries staged in
+ *     shared memory in FP64, the slice sums added in slice order (k_skfr_dist, k_skfr_dist_sum);
  *   - per iteration, the cluster sums of every SNP as exact integers: membership bit masks per
- *     16-individual word (k_skfr_masks), then per SNP and cluster popc(h & m) + popc(h & l & m)
- *     dosage sums and popc(~h & l & m) missing counts over the column (k_skfr_sums, one thread per
- *     SNP streaming its column, masks broadcast from shared memory); centres and feature scores in
- *     FP64 (k_skfr_means);
- *   - the reassignment scores of every individual on the kept SNPs, FP64 in SNP order
- *     (k_skfr_assign, one thread per individual).
- * The host keeps the small sequential steps: the k-means++ draws from a splitmix64 stream, the
- * choice of the `sparsity` largest scores, the argmin over clusters and the convergence test.
- * Every FP64 operation whose rounding the oracle reproduces is written with explicit
+ *     16-individual word and the cluster sizes (k_skfr_masks), then per SNP and cluster one popcount
+ *     of the dosage bits and one of the missing bits under the mask (k_skfr_sums, one thread per SNP
+ *     streaming its column, masks broadcast from shared memory); centres and feature scores in FP64
+ *     (k_skfr_means);
+ *   - the `sparsity` largest scores of each kept list (ties to the lower index) by a radix select
+ *     on the scores' bit patterns and an index-order compaction, one block per list (k_skfr_select);
+ *   - the reassignment scores of every individual on the kept SNPs: one thread per individual and
+ *     slice of SKFR_ASLICE kept SNPs, FP64 sums in SNP order with the terms of SKFR_ACHUNK SNPs at a
+ *     time in shared memory (k_skfr_assign_shared: one list for all clusters, each code read once;
+ *     k_skfr_assign_own: each cluster's own list), the slice sums then added in order
+ *     (k_skfr_assign_sum); the argmin over clusters and the count of changed assignments
+ *     (k_skfr_argmin).
+ * The host keeps the sequential k-means++ draws from a splitmix64 stream, reads one count per
+ * iteration for the convergence test, and sums the objective in individual order at the end of a
+ * try.  Every FP64 operation whose rounding the oracle reproduces is written with explicit
  * round-to-nearest intrinsics, so no multiply-add is contracted.
  */
 #include <algorithm>
 #include <cuda_runtime.h>
-#include <numeric>
 #include <stdint.h>
 #include <stdio.h>
 #include <vector>
@@ -33,8 +39,12 @@
 
 namespace {
 
-constexpr int SKFR_SLICE = 4096;     /* SNPs per partial sum of the seeding distances */
+constexpr int SKFR_SLICE = 1024;     /* SNPs per partial sum of the seeding distances */
+constexpr int SKFR_DCHUNK = 128;     /* SNPs whose squared differences are staged in shared memory at a time */
 constexpr int SKFR_WCHUNK = 256;     /* 16-individual words of masks staged per shared-memory chunk */
+constexpr int SKFR_ASLICE = 1024;    /* kept SNPs per partial sum of the reassignment scores */
+constexpr int SKFR_ACHUNK = 64;      /* kept SNPs whose terms are staged in shared memory at a time */
+constexpr int SKFR_SEL_THREADS = 1024;
 
 __device__ __forceinline__ uint32_t col_word(const uint8_t *bed, int64_t pitch, int64_t l, int64_t w)
 {
@@ -68,34 +78,66 @@ __global__ void k_skfr_counts(const uint8_t *__restrict__ bed, int64_t pitch, in
     }
 }
 
-/* partial[s][i] = sum over SNPs l of slice s of (x_il - x_cl)^2, x from the per-SNP table xt[l][code] */
-__global__ void k_skfr_dist(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, int64_t J,
-                            const double *__restrict__ xt, int64_t center, double *__restrict__ partial)
+/* sq[l][c] = (x_lc - x_l,centre)^2 for every SNP l and code c, x from the table xt[l][code] */
+__global__ void k_skfr_sqtab(const uint8_t *__restrict__ bed, int64_t pitch, int64_t J, const double *__restrict__ xt,
+                             int64_t center, double *__restrict__ sq)
 {
-    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;   /* word = 16 individuals */
+    const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= J) return;
+    const double *t = xt + 4 * l;
+    const double xc = t[(bed[(size_t)l * pitch + (size_t)(center >> 2)] >> ((center & 3) * 2)) & 3];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const double d = __dsub_rn(t[c], xc);
+        sq[4 * l + c] = __dmul_rn(d, d);
+    }
+}
+
+/* partial[s][i] = sum over the SNPs l of slice s, in order, of sq[l][code_il] */
+__global__ void __launch_bounds__(128)
+k_skfr_dist(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, int64_t J, const double *__restrict__ sq,
+            double *__restrict__ partial)
+{
+    __shared__ double tab[SKFR_DCHUNK * 4];
+    const int64_t w = (int64_t)blockIdx.x * 128 + threadIdx.x;   /* word = 16 individuals */
     const int64_t s = blockIdx.y;
-    if (w * 16 >= I) return;
+    const bool live = w * 16 < I;
     const int64_t l0 = s * SKFR_SLICE, l1 = min(J, l0 + SKFR_SLICE);
     double part[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) part[j] = 0.0;
-    const int cs = (int)(center & 3) * 2;
-    for (int64_t l = l0; l < l1; ++l) {
-        const uint32_t x = col_word(bed, pitch, l, w);
-        const double *t = xt + 4 * l;
-        const double xc = __ldg(t + ((bed[(size_t)l * pitch + (size_t)(center >> 2)] >> cs) & 3));
-        const double t0 = __ldg(t), t1 = __ldg(t + 1), t2 = __ldg(t + 2), t3 = __ldg(t + 3);
+    for (int64_t c0 = l0; c0 < l1; c0 += SKFR_DCHUNK) {
+        const int n = (int)min((int64_t)SKFR_DCHUNK, l1 - c0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < 4 * n; t += 128) tab[t] = sq[4 * c0 + t];
+        __syncthreads();
+        if (live) {
+            const uint8_t *col = bed + (size_t)c0 * pitch + (size_t)w * 4;
+            int u = 0;
+            for (; u + 4 <= n; u += 4) {
+                uint32_t x[4];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const uint32_t c = (x >> (2 * j)) & 3u;
-            const double xi = c == 0 ? t0 : (c == 1 ? t1 : (c == 2 ? t2 : t3));
-            const double d = __dsub_rn(xi, xc);
-            part[j] = __dadd_rn(part[j], __dmul_rn(d, d));
+                for (int v = 0; v < 4; ++v) x[v] = *(const uint32_t *)(col + (size_t)(u + v) * pitch);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const double *tb = tab + (u + v) * 4;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) part[j] = __dadd_rn(part[j], tb[(x[v] >> (2 * j)) & 3u]);
+                }
+            }
+            for (; u < n; ++u) {
+                const uint32_t x = *(const uint32_t *)(col + (size_t)u * pitch);
+                const double *tb = tab + u * 4;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) part[j] = __dadd_rn(part[j], tb[(x >> (2 * j)) & 3u]);
+            }
         }
     }
+    if (live) {
 #pragma unroll
-    for (int j = 0; j < 16; ++j)
-        if (w * 16 + j < I) partial[(size_t)s * I + w * 16 + j] = part[j];
+        for (int j = 0; j < 16; ++j)
+            if (w * 16 + j < I) partial[(size_t)s * I + w * 16 + j] = part[j];
+    }
 }
 
 __global__ void k_skfr_dist_sum(const double *__restrict__ partial, int64_t I, int nslice, double *__restrict__ D)
@@ -107,22 +149,48 @@ __global__ void k_skfr_dist_sum(const double *__restrict__ partial, int64_t I, i
     D[i] = t;
 }
 
-/* membership masks: bit 2j of mask[k][w] is set when individual 16w + j is in cluster k */
-__global__ void k_skfr_masks(const int32_t *__restrict__ cl, int64_t I, int64_t nw, int K, uint32_t *__restrict__ mask)
+/* membership masks (bit 2j of mask[k][w] set when individual 16w + j is in cluster k) and the
+ * cluster sizes nk[k] (added to; zeroed before the launch) */
+__global__ void k_skfr_masks(const int32_t *__restrict__ cl, int64_t I, int64_t nw, int K, uint32_t *__restrict__ mask,
+                             int32_t *__restrict__ nk)
 {
+    __shared__ int cnt[16];
+    if (threadIdx.x < 16) cnt[threadIdx.x] = 0;
+    __syncthreads();
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= nw) return;
-    uint32_t m[16];
-    for (int k = 0; k < K; ++k) m[k] = 0u;
-    for (int j = 0; j < 16; ++j) {
-        const int64_t i = w * 16 + j;
-        if (i < I) m[cl[i]] |= 1u << (2 * j);
+    if (w < nw) {
+        uint32_t m[16];
+        for (int k = 0; k < K; ++k) m[k] = 0u;
+        for (int j = 0; j < 16; ++j) {
+            const int64_t i = w * 16 + j;
+            if (i < I) m[cl[i]] |= 1u << (2 * j);
+        }
+        for (int k = 0; k < K; ++k) {
+            mask[(size_t)k * nw + w] = m[k];
+            if (m[k]) atomicAdd(&cnt[k], __popc(m[k]));
+        }
     }
-    for (int k = 0; k < K; ++k) mask[(size_t)k * nw + w] = m[k];
+    __syncthreads();
+    if (threadIdx.x < K && cnt[threadIdx.x]) atomicAdd(&nk[threadIdx.x], cnt[threadIdx.x]);
+}
+
+/* one word of a column: dosage sums and missing counts under each cluster's mask */
+template <int K>
+__device__ __forceinline__ void sums_word(uint32_t x, const uint32_t (*ms)[SKFR_WCHUNK], int w, int32_t *sg, int32_t *sm)
+{
+    const uint32_t hi = (x >> 1) & 0x55555555u, lo = x & 0x55555555u;
+    const uint32_t h2 = hi & lo, mi = ~hi & lo;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        /* dosage = hi + (hi & lo), both on the even bits: one count of (hi & m) | ((hi & lo & m) << 1) */
+        const uint32_t m = ms[k][w];
+        sg[k] += __popc((hi & m) | ((h2 & m) << 1));
+        sm[k] += __popc(mi & m);
+    }
 }
 
 /* per SNP l and cluster k: S = sum of the members' dosages, M = members with a missing code
- * (one thread per SNP, its column streamed in 16-byte loads, masks staged in shared memory) */
+ * (one thread per SNP, its column streamed 64 bytes at a time, masks staged in shared memory) */
 template <int K>
 __global__ void __launch_bounds__(128)
 k_skfr_sums(const uint8_t *__restrict__ bed, int64_t pitch, int64_t nw, int64_t J, const uint32_t *__restrict__ mask,
@@ -142,23 +210,25 @@ k_skfr_sums(const uint8_t *__restrict__ bed, int64_t pitch, int64_t nw, int64_t 
         }
         __syncthreads();
         if (l < J) {
+            /* the column pitch is a multiple of 16 bytes and covers every word up to nw rounded up to 4 */
             const uint8_t *col = bed + (size_t)l * pitch + (size_t)w0 * 4;
-            for (int w = 0; w < nwc; w += 4) {   /* the column pitch is a multiple of 16 bytes */
+            int w = 0;
+            for (; w + 16 <= nwc; w += 16) {
+                uint4 v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) v[u] = *(const uint4 *)(col + (size_t)(w + 4 * u) * 4);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    sums_word<K>(v[u].x, ms, w + 4 * u, sg, sm);
+                    sums_word<K>(v[u].y, ms, w + 4 * u + 1, sg, sm);
+                    sums_word<K>(v[u].z, ms, w + 4 * u + 2, sg, sm);
+                    sums_word<K>(v[u].w, ms, w + 4 * u + 3, sg, sm);
+                }
+            }
+            for (; w < nwc; w += 4) {
                 const uint4 v = *(const uint4 *)(col + (size_t)w * 4);
                 const uint32_t xs[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (w + q >= nwc) break;
-                    const uint32_t x = xs[q];
-                    const uint32_t hi = (x >> 1) & 0x55555555u, lo = x & 0x55555555u;
-                    const uint32_t h1 = hi, h2 = hi & lo, mi = ~hi & lo;
-#pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const uint32_t m = ms[k][w + q];
-                        sg[k] += __popc(h1 & m) + __popc(h2 & m);
-                        sm[k] += __popc(mi & m);
-                    }
-                }
+                for (int q = 0; q < 4 && w + q < nwc; ++q) sums_word<K>(xs[q], ms, w + q, sg, sm);
             }
         }
     }
@@ -174,7 +244,7 @@ k_skfr_sums(const uint8_t *__restrict__ bed, int64_t pitch, int64_t nw, int64_t 
 /* theta_kl = (a_l S_kl - b_l n_kl) / N_k (n_kl = N_k - M_kl non-missing members) and the feature
  * scores: global r_l = sum_k N_k theta_kl^2, local r_kl = N_k theta_kl^2 */
 __global__ void k_skfr_means(const int32_t *__restrict__ S, const int32_t *__restrict__ M, const double *__restrict__ ab,
-                             const double *__restrict__ Nk, int K, int64_t J, int local, double *__restrict__ theta,
+                             const int32_t *__restrict__ Nk, int K, int64_t J, int local, double *__restrict__ theta,
                              double *__restrict__ score)
 {
     const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -183,7 +253,7 @@ __global__ void k_skfr_means(const int32_t *__restrict__ S, const int32_t *__res
     double r = 0.0;
     for (int k = 0; k < K; ++k) {
         double t = 0.0;
-        const double nk = Nk[k];
+        const double nk = (double)Nk[k];
         if (nk > 0.0) {
             const double n = nk - (double)M[(size_t)k * J + l];
             t = __ddiv_rn(__dsub_rn(__dmul_rn(a, (double)S[(size_t)k * J + l]), __dmul_rn(b, n)), nk);
@@ -196,36 +266,253 @@ __global__ void k_skfr_means(const int32_t *__restrict__ S, const int32_t *__res
     if (!local) score[l] = r;
 }
 
-/* per kept SNP (cluster k's list position p) and code: theta^2 - (2 x) theta, x = xt[l][code] */
+/* exclusive scan of v over a block of SKFR_SEL_THREADS threads; *total = the block's sum */
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *wsum, uint32_t *total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t t = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        wsum[lane] = t;
+    }
+    __syncthreads();
+    const uint32_t before = (wid ? wsum[wid - 1] : 0u) + x - v;
+    *total = wsum[31];
+    __syncthreads();
+    return before;
+}
+
+/* The s largest of the J scores of list blockIdx.x (ties to the lower index), written to out in
+ * increasing index order.  The scores are non-negative doubles, so their bit patterns order as the
+ * values: eight radix passes of 8 bits find the s-th largest pattern T and how many copies of it
+ * are needed; one pass in index order then keeps every score above T and the first `need` equal
+ * to T, each thread taking 4 consecutive SNPs and one packed scan of (above, equal) counts giving
+ * every kept SNP its output position. */
+__global__ void __launch_bounds__(SKFR_SEL_THREADS)
+k_skfr_select(const double *__restrict__ score, int64_t J, int64_t s, int32_t *__restrict__ out)
+{
+    __shared__ uint32_t hist[256];
+    __shared__ uint32_t wsum[32];
+    __shared__ unsigned long long s_prefix;
+    __shared__ long long s_rank;
+    const unsigned long long *key = (const unsigned long long *)(score + (size_t)blockIdx.x * J);
+    int32_t *o = out + (size_t)blockIdx.x * s;
+    const int tid = threadIdx.x, lane = tid & 31;
+    unsigned long long prefix = 0ull, pmask = 0ull;
+    long long rank = s;                     /* rank of the wanted pattern among those under the prefix */
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int t = tid; t < 256; t += SKFR_SEL_THREADS) hist[t] = 0u;
+        __syncthreads();
+        for (int64_t l0 = 0; l0 < J; l0 += 4 * SKFR_SEL_THREADS) {
+            unsigned long long kv[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int64_t l = l0 + tid + (int64_t)v * SKFR_SEL_THREADS;
+                kv[v] = l < J ? key[l] : 0ull;
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const int64_t l = l0 + tid + (int64_t)v * SKFR_SEL_THREADS;
+                const bool act = l < J && (kv[v] & pmask) == prefix;
+                const uint32_t bin = act ? (uint32_t)((kv[v] >> shift) & 255u) : 256u;
+                const uint32_t peers = __match_any_sync(0xffffffffu, bin);
+                if (act && lane == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            long long acc = 0;
+            int b = 255;
+            for (; b > 0; --b) {
+                if (acc + (long long)hist[b] >= rank) break;
+                acc += hist[b];
+            }
+            s_prefix = prefix | ((unsigned long long)b << shift);
+            s_rank = rank - acc;
+        }
+        __syncthreads();
+        prefix = s_prefix;
+        rank = s_rank;
+        pmask |= 255ull << shift;
+    }
+    const unsigned long long T = prefix;
+    const uint32_t need = (uint32_t)rank;   /* copies of T kept; s - need patterns lie above T */
+    uint32_t base_gt = 0, base_eq = 0;
+    for (int64_t l0 = 0; l0 < J; l0 += 4 * SKFR_SEL_THREADS) {
+        const int64_t lb = l0 + 4 * (int64_t)tid;
+        uint32_t gt = 0, eq = 0, gtm = 0, eqm = 0;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            if (lb + v < J) {
+                const unsigned long long kv = key[lb + v];
+                if (kv > T) { gt++; gtm |= 1u << v; }
+                else if (kv == T) { eq++; eqm |= 1u << v; }
+            }
+        }
+        uint32_t tot;
+        const uint32_t pre = block_excl_scan((gt << 16) | eq, wsum, &tot);
+        uint32_t g = base_gt + (pre >> 16), e = base_eq + (pre & 0xffffu);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            if (gtm & (1u << v)) {
+                o[g + min(e, need)] = (int32_t)(lb + v);
+                g++;
+            } else if (eqm & (1u << v)) {
+                if (e < need) o[g + e] = (int32_t)(lb + v);
+                e++;
+            }
+        }
+        base_gt += tot >> 16;
+        base_eq += tot & 0xffffu;
+    }
+}
+
+/* per cluster k, kept SNP (list position p, list k * kstride: one shared list when kstride is 0) and
+ * code: terms[k][p][code] = theta^2 - (2 x) theta, x = xt[l][code] */
 __global__ void k_skfr_terms(const double *__restrict__ theta, const double *__restrict__ xt, const int32_t *__restrict__ kept,
-                             int64_t nkept, int K, int64_t J, double *__restrict__ terms)
+                             int64_t nkept, int64_t kstride, int K, int64_t J, double *__restrict__ terms)
 {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (int64_t)K * nkept) return;
     const int k = (int)(t / nkept);
-    const int64_t l = kept[t];
+    const int64_t l = kept[k * kstride + (t - k * nkept)];
     const double th = theta[(size_t)k * J + l], tt = __dmul_rn(th, th);
     for (int c = 0; c < 4; ++c)
         terms[4 * t + c] = __dsub_rn(tt, __dmul_rn(__dmul_rn(2.0, xt[4 * l + c]), th));
 }
 
-/* sc[i][k] = sum over cluster k's kept SNPs (in list order) of terms[k][p][code_il] */
-__global__ void k_skfr_assign(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, const int32_t *__restrict__ kept,
-                              int64_t nkept, int K, const double *__restrict__ terms, double *__restrict__ sc)
+/* Reassignment scores, one shared kept list (global mode): thread = individual i, blockIdx.y = slice
+ * of SKFR_ASLICE list positions; part[y][i][k] = sum over the slice (list order, FP64 from 0) of
+ * terms[k][p][code_ip].  The terms of SKFR_ACHUNK positions are staged in shared memory as
+ * [p][code][k] with an odd row stride, so the four codes of one position fall in different banks;
+ * each code is read once for all K clusters. */
+template <int K>
+__global__ void __launch_bounds__(128)
+k_skfr_assign_shared(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, const int32_t *__restrict__ kept,
+                     int64_t nkept, const double *__restrict__ terms, double *__restrict__ part)
+{
+    constexpr int KS = K | 1;
+    __shared__ double ts[SKFR_ACHUNK * 4 * KS];
+    __shared__ int32_t ls[SKFR_ACHUNK];
+    const int64_t i = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    const int64_t p0 = (int64_t)blockIdx.y * SKFR_ASLICE, p1 = min(nkept, p0 + SKFR_ASLICE);
+    const int sh = (int)(i & 3) * 2;
+    const uint8_t *base = bed + (size_t)(i >> 2);
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    for (int64_t q0 = p0; q0 < p1; q0 += SKFR_ACHUNK) {
+        const int n = (int)min((int64_t)SKFR_ACHUNK, p1 - q0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < n * 4 * K; t += 128) {
+            const int k = t / (n * 4), r = t - k * (n * 4);          /* r = position * 4 + code */
+            ts[r * KS + k] = terms[((size_t)k * nkept + q0) * 4 + r];
+        }
+        for (int t = threadIdx.x; t < n; t += 128) ls[t] = kept[q0 + t];
+        __syncthreads();
+        if (i < I) {
+            int pp = 0;
+            for (; pp + 8 <= n; pp += 8) {
+                uint32_t c[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) c[u] = base[(size_t)ls[pp + u] * pitch];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const double *tp = ts + ((pp + u) * 4 + ((c[u] >> sh) & 3)) * KS;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) acc[k] = __dadd_rn(acc[k], tp[k]);
+                }
+            }
+            for (; pp < n; ++pp) {
+                const double *tp = ts + (pp * 4 + ((base[(size_t)ls[pp] * pitch] >> sh) & 3)) * KS;
+#pragma unroll
+                for (int k = 0; k < K; ++k) acc[k] = __dadd_rn(acc[k], tp[k]);
+            }
+        }
+    }
+    if (i < I) {
+        double *o = part + ((size_t)blockIdx.y * I + i) * K;
+#pragma unroll
+        for (int k = 0; k < K; ++k) o[k] = acc[k];
+    }
+}
+
+/* Reassignment scores, each cluster its own kept list (local mode): as k_skfr_assign_shared with
+ * blockIdx.z = cluster k, its list kept[k] and terms[k]. */
+__global__ void __launch_bounds__(128)
+k_skfr_assign_own(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, const int32_t *__restrict__ kept,
+                  int64_t nkept, int K, const double *__restrict__ terms, double *__restrict__ part)
+{
+    __shared__ double ts[SKFR_ACHUNK * 4];
+    __shared__ int32_t ls[SKFR_ACHUNK];
+    const int k = blockIdx.z;
+    const int64_t i = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    const int64_t p0 = (int64_t)blockIdx.y * SKFR_ASLICE, p1 = min(nkept, p0 + SKFR_ASLICE);
+    const int sh = (int)(i & 3) * 2;
+    const uint8_t *base = bed + (size_t)(i >> 2);
+    const int32_t *kl = kept + (size_t)k * nkept;
+    const double *tk = terms + (size_t)k * nkept * 4;
+    double acc = 0.0;
+    for (int64_t q0 = p0; q0 < p1; q0 += SKFR_ACHUNK) {
+        const int n = (int)min((int64_t)SKFR_ACHUNK, p1 - q0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < n * 4; t += 128) ts[t] = tk[q0 * 4 + t];
+        for (int t = threadIdx.x; t < n; t += 128) ls[t] = kl[q0 + t];
+        __syncthreads();
+        if (i < I) {
+            int pp = 0;
+            for (; pp + 8 <= n; pp += 8) {
+                uint32_t c[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) c[u] = base[(size_t)ls[pp + u] * pitch];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc = __dadd_rn(acc, ts[(pp + u) * 4 + ((c[u] >> sh) & 3)]);
+            }
+            for (; pp < n; ++pp) acc = __dadd_rn(acc, ts[pp * 4 + ((base[(size_t)ls[pp] * pitch] >> sh) & 3)]);
+        }
+    }
+    if (i < I) part[((size_t)blockIdx.y * I + i) * K + k] = acc;
+}
+
+/* sc[i][k] = the slice sums part[y][i][k] added in slice order (FP64 from 0) */
+__global__ void k_skfr_assign_sum(const double *__restrict__ part, int64_t IK, int nslice, double *__restrict__ sc)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= IK) return;
+    double v = 0.0;
+    for (int y = 0; y < nslice; ++y) v = __dadd_rn(v, part[(size_t)y * IK + t]);
+    sc[t] = v;
+}
+
+/* cl_new[i] = argmin_k sc[i][k] (ties to the lower cluster); *changed += individuals whose cluster moved */
+__global__ void k_skfr_argmin(const double *__restrict__ sc, int64_t I, int K, const int32_t *__restrict__ cl,
+                              int32_t *__restrict__ cl_new, int32_t *__restrict__ changed)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= I) return;
-    const int sh = (int)(i & 3) * 2;
-    for (int k = 0; k < K; ++k) {
-        const int32_t *kl = kept + (size_t)k * nkept;
-        const double *tk = terms + (size_t)k * nkept * 4;
-        double acc = 0.0;
-        for (int64_t p = 0; p < nkept; ++p) {
-            const int c = (bed[(size_t)kl[p] * pitch + (size_t)(i >> 2)] >> sh) & 3;
-            acc = __dadd_rn(acc, tk[4 * p + c]);
-        }
-        sc[(size_t)i * K + k] = acc;
+    bool moved = false;
+    if (i < I) {
+        const double *r = sc + (size_t)i * K;
+        int best = 0;
+        double rb = r[0];
+        for (int k = 1; k < K; ++k)
+            if (r[k] < rb) { best = k; rb = r[k]; }
+        cl_new[i] = best;
+        moved = best != cl[i];
     }
+    const uint32_t b = __ballot_sync(0xffffffffu, moved);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(changed, __popc(b));
 }
 
 struct SplitMix64 {
@@ -241,39 +528,47 @@ struct SplitMix64 {
     double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
 };
 
-/* the s largest scores, ties to the lower index, in increasing index order */
-void top_s(const double *score, int64_t J, int64_t s, int32_t *out)
-{
-    std::vector<int32_t> idx((size_t)J);
-    std::iota(idx.begin(), idx.end(), 0);
-    const int64_t n = std::min(s, J);
-    auto better = [&](int32_t x, int32_t y) { return score[x] > score[y] || (score[x] == score[y] && x < y); };
-    std::nth_element(idx.begin(), idx.begin() + (n - 1), idx.end(), better);
-    std::sort(idx.begin(), idx.begin() + n, better);
-    std::vector<int32_t> pick(idx.begin(), idx.begin() + n);
-    std::sort(pick.begin(), pick.end());
-    std::copy(pick.begin(), pick.end(), out);
-}
-
+/* the kernels templated on the cluster count, for one K */
 template <int K>
-cudaError_t launch_sums(const uint8_t *bed, int64_t pitch, int64_t nw, int64_t J, const uint32_t *mask, int32_t *S,
-                        int32_t *M, cudaStream_t st)
-{
-    k_skfr_sums<K><<<(unsigned)((J + 127) / 128), 128, 0, st>>>(bed, pitch, nw, J, mask, S, M);
-    return cudaGetLastError();
-}
+struct SkfrK {
+    static cudaError_t sums(const uint8_t *bed, int64_t pitch, int64_t nw, int64_t J, const uint32_t *mask, int32_t *S,
+                            int32_t *M, cudaStream_t st)
+    {
+        k_skfr_sums<K><<<(unsigned)((J + 127) / 128), 128, 0, st>>>(bed, pitch, nw, J, mask, S, M);
+        return cudaGetLastError();
+    }
+    static cudaError_t assign_shared(const uint8_t *bed, int64_t pitch, int64_t I, const int32_t *kept, int64_t nkept,
+                                     const double *terms, double *part, cudaStream_t st)
+    {
+        const dim3 grid((unsigned)((I + 127) / 128), (unsigned)((nkept + SKFR_ASLICE - 1) / SKFR_ASLICE));
+        k_skfr_assign_shared<K><<<grid, 128, 0, st>>>(bed, pitch, I, kept, nkept, terms, part);
+        return cudaGetLastError();
+    }
+};
+
+#define SKFR_DISPATCH(K, CALL)                                                                              \
+    switch (K) {                                                                                            \
+    case 1: return SkfrK<1>::CALL; case 2: return SkfrK<2>::CALL; case 3: return SkfrK<3>::CALL;             \
+    case 4: return SkfrK<4>::CALL; case 5: return SkfrK<5>::CALL; case 6: return SkfrK<6>::CALL;             \
+    case 7: return SkfrK<7>::CALL; case 8: return SkfrK<8>::CALL; case 9: return SkfrK<9>::CALL;             \
+    case 10: return SkfrK<10>::CALL; case 11: return SkfrK<11>::CALL; case 12: return SkfrK<12>::CALL;       \
+    case 13: return SkfrK<13>::CALL; case 14: return SkfrK<14>::CALL; case 15: return SkfrK<15>::CALL;       \
+    case 16: return SkfrK<16>::CALL;                                                                        \
+    }                                                                                                       \
+    return cudaErrorInvalidValue;
 
 cudaError_t sums_for_k(int K, const uint8_t *bed, int64_t pitch, int64_t nw, int64_t J, const uint32_t *mask, int32_t *S,
                        int32_t *M, cudaStream_t st)
 {
-    switch (K) {
-#define SK_CASE(k) case k: return launch_sums<k>(bed, pitch, nw, J, mask, S, M, st);
-        SK_CASE(1) SK_CASE(2) SK_CASE(3) SK_CASE(4) SK_CASE(5) SK_CASE(6) SK_CASE(7) SK_CASE(8)
-        SK_CASE(9) SK_CASE(10) SK_CASE(11) SK_CASE(12) SK_CASE(13) SK_CASE(14) SK_CASE(15) SK_CASE(16)
-#undef SK_CASE
-    }
-    return cudaErrorInvalidValue;
+    SKFR_DISPATCH(K, sums(bed, pitch, nw, J, mask, S, M, st))
 }
+
+cudaError_t assign_shared_for_k(int K, const uint8_t *bed, int64_t pitch, int64_t I, const int32_t *kept, int64_t nkept,
+                                const double *terms, double *part, cudaStream_t st)
+{
+    SKFR_DISPATCH(K, assign_shared(bed, pitch, I, kept, nkept, terms, part, st))
+}
+#undef SKFR_DISPATCH
 
 template <class T>
 struct DevBuf {
@@ -281,6 +576,12 @@ struct DevBuf {
     cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * std::max<size_t>(n, 1)); }
     ~DevBuf() { if (p) cudaFree(p); }
 };
+
+#define SK_TRY(x)                                                                                           \
+    do {                                                                                                    \
+        const cudaError_t e_ = (x);                                                                         \
+        if (e_ != cudaSuccess) return e_;                                                                   \
+    } while (0)
 
 }  // namespace
 
@@ -292,24 +593,39 @@ cudaError_t skfr_run(const uint8_t *bed, int64_t pitch, int64_t I, int64_t J, in
     const int64_t nw = (I + 15) / 16;                 /* 16-individual words per column (within the pitch) */
     const int nslice = (int)((J + SKFR_SLICE - 1) / SKFR_SLICE);
     const int64_t s = std::min(sparsity, J);
-    cudaError_t e = cudaSuccess;
+    const int naslice = (int)((s + SKFR_ASLICE - 1) / SKFR_ASLICE);
+    const int nlists = local ? K : 1;                 /* kept lists: one for all clusters, or one per cluster */
+    if ((int64_t)nslice > 65535 || (int64_t)naslice > 65535 || J > INT32_MAX) return cudaErrorInvalidValue;
     DevBuf<int64_t> d_cnt;
-    DevBuf<double> d_xt, d_ab, d_partial, d_D, d_theta, d_score, d_Nk, d_terms, d_sc;
+    DevBuf<double> d_xt, d_ab, d_sq, d_partial, d_D, d_theta, d_score, d_terms, d_apart, d_sc;
     DevBuf<uint32_t> d_mask;
-    DevBuf<int32_t> d_cl, d_S, d_M, d_kept;
-    if ((e = d_cnt.alloc(3 * J)) || (e = d_xt.alloc(4 * J)) || (e = d_ab.alloc(2 * J)) ||
-        (e = d_partial.alloc((size_t)nslice * I)) || (e = d_D.alloc(I)) || (e = d_theta.alloc((size_t)K * J)) ||
-        (e = d_score.alloc((size_t)K * J)) || (e = d_Nk.alloc(K)) || (e = d_terms.alloc((size_t)K * s * 4)) ||
-        (e = d_sc.alloc((size_t)I * K)) || (e = d_mask.alloc((size_t)K * nw)) || (e = d_cl.alloc(I)) ||
-        (e = d_S.alloc((size_t)K * J)) || (e = d_M.alloc((size_t)K * J)) || (e = d_kept.alloc((size_t)K * s)))
-        return e;
+    DevBuf<int32_t> d_cl, d_cl2, d_nk, d_changed, d_S, d_M, d_kept;
+    SK_TRY(d_cnt.alloc(3 * J));
+    SK_TRY(d_xt.alloc(4 * J));
+    SK_TRY(d_ab.alloc(2 * J));
+    SK_TRY(d_sq.alloc(4 * J));
+    SK_TRY(d_partial.alloc((size_t)nslice * I));
+    SK_TRY(d_D.alloc(I));
+    SK_TRY(d_theta.alloc((size_t)K * J));
+    SK_TRY(d_score.alloc((size_t)nlists * J));
+    SK_TRY(d_terms.alloc((size_t)K * s * 4));
+    SK_TRY(d_apart.alloc((size_t)naslice * I * K));
+    SK_TRY(d_sc.alloc((size_t)I * K));
+    SK_TRY(d_mask.alloc((size_t)K * nw));
+    SK_TRY(d_cl.alloc(I));
+    SK_TRY(d_cl2.alloc(I));
+    SK_TRY(d_nk.alloc(K));
+    SK_TRY(d_changed.alloc(1));
+    SK_TRY(d_S.alloc((size_t)K * J));
+    SK_TRY(d_M.alloc((size_t)K * J));
+    SK_TRY(d_kept.alloc((size_t)nlists * s));
 
     /* per-SNP standardisation from the class counts (host FP64, as the oracle) */
     k_skfr_counts<<<(unsigned)((J + 3) / 4), 128, 0, st>>>(bed, pitch, nw, J, d_cnt.p);
+    SK_TRY(cudaGetLastError());
     std::vector<int64_t> cnt((size_t)3 * J);
-    if ((e = cudaGetLastError()) || (e = cudaMemcpyAsync(cnt.data(), d_cnt.p, sizeof(int64_t) * 3 * J, cudaMemcpyDeviceToHost, st)) ||
-        (e = cudaStreamSynchronize(st)))
-        return e;
+    SK_TRY(cudaMemcpyAsync(cnt.data(), d_cnt.p, sizeof(int64_t) * 3 * J, cudaMemcpyDeviceToHost, st));
+    SK_TRY(cudaStreamSynchronize(st));
     std::vector<double> xt((size_t)4 * J), ab((size_t)2 * J);
     double x2_total = 0.0;
     for (int64_t l = 0; l < J; ++l) {
@@ -332,68 +648,56 @@ cudaError_t skfr_run(const uint8_t *bed, int64_t pitch, int64_t I, int64_t J, in
         xt[4 * l + 2] = a - b;
         xt[4 * l + 3] = 2.0 * a - b;
     }
-    if ((e = cudaMemcpyAsync(d_xt.p, xt.data(), sizeof(double) * 4 * J, cudaMemcpyHostToDevice, st)) ||
-        (e = cudaMemcpyAsync(d_ab.p, ab.data(), sizeof(double) * 2 * J, cudaMemcpyHostToDevice, st)))
-        return e;
+    SK_TRY(cudaMemcpyAsync(d_xt.p, xt.data(), sizeof(double) * 4 * J, cudaMemcpyHostToDevice, st));
+    SK_TRY(cudaMemcpyAsync(d_ab.p, ab.data(), sizeof(double) * 2 * J, cudaMemcpyHostToDevice, st));
 
     SplitMix64 rng{seed};
-    std::vector<double> D((size_t)I), dk((size_t)I * K), sc((size_t)I * K), score((size_t)K * J);
-    std::vector<int32_t> cl((size_t)I), cl_new((size_t)I), kept((size_t)K * s);
-    std::vector<double> Nk((size_t)K);
+    std::vector<double> D((size_t)I), dk((size_t)I * K), sc((size_t)I * K);
+    std::vector<int32_t> cl((size_t)I), kept((size_t)nlists * s);
     double best_obj = 0.0;
     bool have_best = false;
 
+    /* squared distances of every individual to individual `center` over all SNPs, into out (host) */
     auto dist = [&](int64_t center, double *out) -> cudaError_t {
-        dim3 grid((unsigned)((nw + 127) / 128), (unsigned)nslice);
-        k_skfr_dist<<<grid, 128, 0, st>>>(bed, pitch, I, J, d_xt.p, center, d_partial.p);
-        cudaError_t r = cudaGetLastError();
-        if (r == cudaSuccess) {
-            k_skfr_dist_sum<<<(unsigned)((I + 255) / 256), 256, 0, st>>>(d_partial.p, I, nslice, d_D.p);
-            r = cudaGetLastError();
-        }
-        if (r == cudaSuccess) r = cudaMemcpyAsync(out, d_D.p, sizeof(double) * I, cudaMemcpyDeviceToHost, st);
-        if (r == cudaSuccess) r = cudaStreamSynchronize(st);
-        return r;
+        k_skfr_sqtab<<<(unsigned)((J + 255) / 256), 256, 0, st>>>(bed, pitch, J, d_xt.p, center, d_sq.p);
+        SK_TRY(cudaGetLastError());
+        const dim3 grid((unsigned)((nw + 127) / 128), (unsigned)nslice);
+        k_skfr_dist<<<grid, 128, 0, st>>>(bed, pitch, I, J, d_sq.p, d_partial.p);
+        SK_TRY(cudaGetLastError());
+        k_skfr_dist_sum<<<(unsigned)((I + 255) / 256), 256, 0, st>>>(d_partial.p, I, nslice, d_D.p);
+        SK_TRY(cudaGetLastError());
+        SK_TRY(cudaMemcpyAsync(out, d_D.p, sizeof(double) * I, cudaMemcpyDeviceToHost, st));
+        return cudaStreamSynchronize(st);
     };
-    /* centres, scores and the kept SNP lists of the assignment cl; then sc[i][k] */
-    auto pass = [&]() -> cudaError_t {
-        std::fill(Nk.begin(), Nk.end(), 0.0);
-        for (int64_t i = 0; i < I; ++i) Nk[cl[i]] += 1.0;
-        cudaError_t r = cudaMemcpyAsync(d_cl.p, cl.data(), sizeof(int32_t) * I, cudaMemcpyHostToDevice, st);
-        if (r == cudaSuccess) r = cudaMemcpyAsync(d_Nk.p, Nk.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st);
-        if (r == cudaSuccess) {
-            k_skfr_masks<<<(unsigned)((nw + 127) / 128), 128, 0, st>>>(d_cl.p, I, nw, K, d_mask.p);
-            r = cudaGetLastError();
+    /* for the assignment dcl: cluster sizes, centres, scores, kept lists, terms and sc[i][k] (no sync) */
+    auto pass = [&](const int32_t *dcl) -> cudaError_t {
+        SK_TRY(cudaMemsetAsync(d_nk.p, 0, sizeof(int32_t) * K, st));
+        k_skfr_masks<<<(unsigned)((nw + 127) / 128), 128, 0, st>>>(dcl, I, nw, K, d_mask.p, d_nk.p);
+        SK_TRY(cudaGetLastError());
+        SK_TRY(sums_for_k(K, bed, pitch, nw, J, d_mask.p, d_S.p, d_M.p, st));
+        k_skfr_means<<<(unsigned)((J + 255) / 256), 256, 0, st>>>(d_S.p, d_M.p, d_ab.p, d_nk.p, K, J, local, d_theta.p,
+                                                                d_score.p);
+        SK_TRY(cudaGetLastError());
+        k_skfr_select<<<(unsigned)nlists, SKFR_SEL_THREADS, 0, st>>>(d_score.p, J, s, d_kept.p);
+        SK_TRY(cudaGetLastError());
+        k_skfr_terms<<<(unsigned)((K * s + 255) / 256), 256, 0, st>>>(d_theta.p, d_xt.p, d_kept.p, s, local ? s : 0, K, J,
+                                                                     d_terms.p);
+        SK_TRY(cudaGetLastError());
+        if (local) {
+            const dim3 grid((unsigned)((I + 127) / 128), (unsigned)naslice, (unsigned)K);
+            k_skfr_assign_own<<<grid, 128, 0, st>>>(bed, pitch, I, d_kept.p, s, K, d_terms.p, d_apart.p);
+            SK_TRY(cudaGetLastError());
+        } else {
+            SK_TRY(assign_shared_for_k(K, bed, pitch, I, d_kept.p, s, d_terms.p, d_apart.p, st));
         }
-        if (r == cudaSuccess) r = sums_for_k(K, bed, pitch, nw, J, d_mask.p, d_S.p, d_M.p, st);
-        if (r == cudaSuccess) {
-            k_skfr_means<<<(unsigned)((J + 255) / 256), 256, 0, st>>>(d_S.p, d_M.p, d_ab.p, d_Nk.p, K, J, local, d_theta.p,
-                                                                    d_score.p);
-            r = cudaGetLastError();
-        }
-        if (r == cudaSuccess)
-            r = cudaMemcpyAsync(score.data(), d_score.p, sizeof(double) * (local ? K : 1) * J, cudaMemcpyDeviceToHost, st);
-        if (r == cudaSuccess) r = cudaStreamSynchronize(st);
-        if (r != cudaSuccess) return r;
-        for (int k = 0; k < K; ++k) top_s(score.data() + (local ? (size_t)k * J : 0), J, s, kept.data() + (size_t)k * s);
-        r = cudaMemcpyAsync(d_kept.p, kept.data(), sizeof(int32_t) * K * s, cudaMemcpyHostToDevice, st);
-        if (r == cudaSuccess) {
-            k_skfr_terms<<<(unsigned)((K * s + 255) / 256), 256, 0, st>>>(d_theta.p, d_xt.p, d_kept.p, s, K, J, d_terms.p);
-            r = cudaGetLastError();
-        }
-        if (r == cudaSuccess) {
-            k_skfr_assign<<<(unsigned)((I + 127) / 128), 128, 0, st>>>(bed, pitch, I, d_kept.p, s, K, d_terms.p, d_sc.p);
-            r = cudaGetLastError();
-        }
-        if (r == cudaSuccess) r = cudaMemcpyAsync(sc.data(), d_sc.p, sizeof(double) * I * K, cudaMemcpyDeviceToHost, st);
-        if (r == cudaSuccess) r = cudaStreamSynchronize(st);
-        return r;
+        k_skfr_assign_sum<<<(unsigned)((I * K + 255) / 256), 256, 0, st>>>(d_apart.p, I * K, naslice, d_sc.p);
+        return cudaGetLastError();
     };
 
     for (int t = 0; t < tries; ++t) {
         /* k-means++ seeding */
-        int64_t c0 = std::min((int64_t)(rng.uniform() * (double)I), I - 1);
-        if ((e = dist(c0, dk.data()))) return e;                      /* column 0 of dk: centre 0 */
+        const int64_t c0 = std::min((int64_t)(rng.uniform() * (double)I), I - 1);
+        SK_TRY(dist(c0, dk.data()));                                     /* row 0 of dk: centre 0 */
         std::copy(dk.begin(), dk.begin() + I, D.begin());
         for (int k = 1; k < K; ++k) {
             double tot = 0.0;
@@ -410,7 +714,7 @@ cudaError_t skfr_run(const uint8_t *bed, int64_t pitch, int64_t I, int64_t J, in
             } else {
                 pick = std::min((int64_t)(u * (double)I), I - 1);
             }
-            if ((e = dist(pick, dk.data() + (size_t)k * I))) return e;
+            SK_TRY(dist(pick, dk.data() + (size_t)k * I));
             for (int64_t i = 0; i < I; ++i) D[i] = std::min(D[i], dk[(size_t)k * I + i]);
         }
         for (int64_t i = 0; i < I; ++i) {
@@ -419,32 +723,40 @@ cudaError_t skfr_run(const uint8_t *bed, int64_t pitch, int64_t I, int64_t J, in
                 if (dk[(size_t)k * I + i] < dk[(size_t)best * I + i]) best = k;
             cl[i] = best;
         }
-        /* iterations */
+        int32_t *cur = d_cl.p, *nxt = d_cl2.p;
+        SK_TRY(cudaMemcpyAsync(cur, cl.data(), sizeof(int32_t) * I, cudaMemcpyHostToDevice, st));
+        /* iterations: the host reads one count per iteration */
         int it = 0;
+        bool converged = false;
         for (it = 1; it <= max_iter; ++it) {
-            if ((e = pass())) return e;
-            bool same = true;
-            for (int64_t i = 0; i < I; ++i) {
-                const double *r = sc.data() + (size_t)i * K;
-                int best = 0;
-                for (int k = 1; k < K; ++k)
-                    if (r[k] < r[best]) best = k;
-                cl_new[i] = best;
-                same = same && best == cl[i];
+            SK_TRY(pass(cur));
+            SK_TRY(cudaMemsetAsync(d_changed.p, 0, sizeof(int32_t), st));
+            k_skfr_argmin<<<(unsigned)((I + 255) / 256), 256, 0, st>>>(d_sc.p, I, K, cur, nxt, d_changed.p);
+            SK_TRY(cudaGetLastError());
+            int32_t changed = 0;
+            SK_TRY(cudaMemcpyAsync(&changed, d_changed.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            SK_TRY(cudaStreamSynchronize(st));
+            if (changed == 0) {
+                converged = true;
+                break;
             }
-            if (same) break;
-            cl.swap(cl_new);
+            std::swap(cur, nxt);
         }
         if (it > max_iter) it = max_iter;
-        /* the objective of the final assignment with its sparse centres */
-        if ((e = pass())) return e;
+        /* the objective of the final assignment with its sparse centres: at convergence the last pass
+         * was already of this assignment */
+        if (!converged) SK_TRY(pass(cur));
+        SK_TRY(cudaMemcpyAsync(sc.data(), d_sc.p, sizeof(double) * I * K, cudaMemcpyDeviceToHost, st));
+        SK_TRY(cudaMemcpyAsync(cl.data(), cur, sizeof(int32_t) * I, cudaMemcpyDeviceToHost, st));
+        SK_TRY(cudaMemcpyAsync(kept.data(), d_kept.p, sizeof(int32_t) * nlists * s, cudaMemcpyDeviceToHost, st));
+        SK_TRY(cudaStreamSynchronize(st));
         double obj = x2_total;
         for (int64_t i = 0; i < I; ++i) obj += sc[(size_t)i * K + cl[i]];
         if (!have_best || obj < best_obj) {
             have_best = true;
             best_obj = obj;
             std::copy(cl.begin(), cl.end(), clusters_out);
-            std::vector<int32_t> u(kept.begin(), kept.begin() + (local ? (size_t)K * s : (size_t)s));
+            std::vector<int32_t> u(kept.begin(), kept.end());
             std::sort(u.begin(), u.end());
             u.erase(std::unique(u.begin(), u.end()), u.end());
             *n_aims = (int64_t)u.size();

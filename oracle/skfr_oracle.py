@@ -20,8 +20,9 @@ implementation (csrc/skfr.cu), which this oracle checks exactly:
 - iteration ("global" mode): cluster means theta_kl over all SNPs (from exact integer sums),
   scores r_l = sum_k n_k theta_kl^2, the `sparsity` SNPs of largest score kept (ties to the lower
   index), centres zero elsewhere, each individual reassigned to
-  argmin_k sum_{l kept} theta_kl^2 - 2 x_il theta_kl (summed in FP64 in SNP order; ties to the
-  lower cluster); stop when no assignment changes or after max_iter iterations;
+  argmin_k sum_{l kept} theta_kl^2 - 2 x_il theta_kl (ties to the lower cluster), the sum in FP64
+  over each ASLICE kept SNPs in SNP order, the slice sums then added in order; stop when no
+  assignment changes or after max_iter iterations;
 - "local" mode: each cluster keeps its own `sparsity` SNPs by n_k theta_kl^2 and is scored on
   them; the AIMs are the union of the kept sets;
 - objective: the within-cluster sum of squares with the sparse centres,
@@ -32,7 +33,8 @@ from __future__ import annotations
 
 import numpy as np
 
-SLICE = 4096          # SNPs per partial sum of the seeding distances
+SLICE = 1024          # SNPs per partial sum of the seeding distances
+ASLICE = 1024         # kept SNPs per partial sum of the reassignment scores
 MASK64 = (1 << 64) - 1
 
 
@@ -148,19 +150,30 @@ def top_s(score: np.ndarray, s: int) -> np.ndarray:
     return np.sort(order[: min(s, score.shape[0])])
 
 
-def reassign(codes: np.ndarray, xt: np.ndarray, theta: np.ndarray, kept: list[np.ndarray]):
-    """argmin_k sum_{l in kept[k]} theta_kl^2 - 2 x_il theta_kl (FP64, SNP order) and the minimum"""
+def scores(codes: np.ndarray, xt: np.ndarray, theta: np.ndarray, kept: list[np.ndarray]) -> np.ndarray:
+    """sc[i, k] = sum_{l in kept[k]} theta_kl^2 - 2 x_il theta_kl: FP64 sums over each ASLICE kept
+    SNPs in SNP order, the slice sums added in order"""
     I = codes.shape[0]
     K = theta.shape[0]
     sc = np.zeros((I, K))
     for k in range(K):
-        acc = np.zeros(I)
-        for l in kept[k]:
-            t = theta[k, l]
-            acc += t * t - 2.0 * xt[l, codes[:, l]] * t
-        sc[:, k] = acc
+        lst = kept[k]
+        total = np.zeros(I)
+        for p0 in range(0, len(lst), ASLICE):
+            part = np.zeros(I)
+            for l in lst[p0:p0 + ASLICE]:
+                t = theta[k, l]
+                part += t * t - 2.0 * xt[l, codes[:, l]] * t
+            total += part
+        sc[:, k] = total
+    return sc
+
+
+def reassign(codes: np.ndarray, xt: np.ndarray, theta: np.ndarray, kept: list[np.ndarray]):
+    """argmin_k of the scores (ties to the lower cluster) and the minimum"""
+    sc = scores(codes, xt, theta, kept)
     c = np.argmin(sc, axis=1).astype(np.int32)
-    return c, sc[np.arange(I), c]
+    return c, sc[np.arange(codes.shape[0]), c]
 
 
 def skfr(data: np.ndarray, I: int, K: int, sparsity: int, *, mode: str = "global", max_iter: int = 50,
@@ -194,15 +207,7 @@ def skfr(data: np.ndarray, I: int, K: int, sparsity: int, *, mode: str = "global
             kept = [top_s((nk[:, None] * theta * theta).sum(0), sparsity)] * K
         else:
             kept = [top_s(nk[k] * theta[k] * theta[k], sparsity) for k in range(K)]
-        sc = np.zeros(I)
-        for k in range(K):
-            m = c == k
-            acc = np.zeros(int(m.sum()))
-            cm = codes[m]
-            for l in kept[k]:
-                t = theta[k, l]
-                acc += t * t - 2.0 * xt[l, cm[:, l]] * t
-            sc[m] = acc
+        sc = scores(codes, xt, theta, kept)[np.arange(I), c]
         obj = x2_total
         for v in sc:
             obj += v

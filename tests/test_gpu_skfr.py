@@ -26,9 +26,14 @@ def _cohort(oa, I, J, K, seed, alpha=0.05):
     (301, 2003, 3, 150, "local", 1),
     (437, 5000, 4, 300, "global", 3),      # two seeding slices, partial words
     (250, 1200, 6, 100, "local", 2),
+    (300, 6000, 3, 2500, "global", 1),     # three reassignment slices of 1024 kept SNPs
+    (260, 5000, 4, 1500, "local", 1),      # two slices per cluster list
+    (200, 2500, 16, 1100, "global", 1),    # the largest K
+    (150, 800, 2, 5000, "local", 1),       # sparsity above J: every SNP kept
+    (90, 700, 1, 100, "global", 1),        # one cluster
 ])
 def test_skfr_matches_oracle(oa, I, J, K, s, mode, tries):
-    g, _ = _cohort(oa, I, J, K, seed=40 + K, alpha=0.1)
+    g, _ = _cohort(oa, I, J, max(K, 2), seed=40 + K, alpha=0.1)
     c, aims, obj, it = oa.skfr(g, K, s, mode=mode, tries=tries, rng=17)
     c_o, aims_o, obj_o, it_o = S.skfr(g.data, g.I, K, s, mode=mode, tries=tries, seed=17)
     assert np.array_equal(c, c_o)
