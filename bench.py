@@ -58,6 +58,11 @@ def _args():
                     help="report the mixed form's errors against the FP64 form (default for c3)")
     ap.add_argument("--cpu-ttc", action="store_true",
                     help="also time the oracle to convergence on the whole cohort (default for c1)")
+    ap.add_argument("--skfr", type=int, default=None, metavar="SPARSITY",
+                    help="time the SKFR AIM pre-selection (admix_skfr) with this sparsity on the cohort instead")
+    ap.add_argument("--skfr-mode", default="global", choices=["global", "local"])
+    ap.add_argument("--skfr-cpu", action="store_true",
+                    help="also time the SKFR oracle on the same cohort and check the result (default for c1)")
     ap.add_argument("--pass-only", default=None,
                     choices=["loglik", "q_sweep", "p_sweep", "q_qp", "p_qp", "em"],
                     help="set up the cohort and launch one pass warmup+steps times (for profilers)")
@@ -87,6 +92,58 @@ def run_pass_only(args):
         ms = d_cu.time_pass(pid, max(1, args.steps))
     print(json.dumps({"pass": args.pass_only, "config": spec.name, "I": spec.I, "J": spec.J, "K": spec.K,
                       "form": args.form, "ms_per_launch": ms}), flush=True)
+    return 0
+
+
+def run_skfr(args):
+    """SKFR AIM pre-selection on the cohort (the step run_admixture runs when `sparsity` is given):
+    warmup + steps calls of admix_skfr on one handle, each timed on the host clock around the call
+    (the call is host-orchestrated: k-means++ draws and one convergence count per iteration cross to
+    the host), the median reported.  With --skfr-cpu (default for c1) the oracle runs the same
+    selection on the host and the device result is checked against it."""
+    import ctypes as C
+    import torch
+    import numpy as np
+    import openadmixture_b200 as oa
+    from openadmixture_b200 import _native as N
+    torch.cuda.set_device(0)
+    spec = oa.COHORTS[args.config].scaled(I=args.I, J=args.J)
+    qt, pt = oa.truth(spec)
+    g = oa.genotypes_device(spec, qt, pt)
+    K, s, local = spec.K, int(args.skfr), args.skfr_mode == "local"
+    cap = min(spec.J, s * (K if local else 1))
+    seed = 7
+    d = oa.AdmixData(spec.I, spec.J, K, 1, rng=0)
+    times = []
+    with oa.CuAdmixData(d, g) as h:
+        for rep in range(max(0, args.warmup) + max(1, args.steps)):
+            cl = np.empty(spec.I, np.int32)
+            aims = np.empty(max(cap, 1), np.int32)
+            n, obj, it = C.c_int64(0), C.c_double(0.0), C.c_int32(0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            h._chk(N.admix_lib().admix_skfr(h.handle, K, s, N.ADMIX_SKFR_LOCAL if local else N.ADMIX_SKFR_GLOBAL, 50, 1,
+                                            seed, N.i32ptr(cl), N.i32ptr(aims), cap, C.byref(n), C.byref(obj),
+                                            C.byref(it)))
+            torch.cuda.synchronize()
+            if rep >= args.warmup:
+                times.append(time.perf_counter() - t0)
+    true = np.argmax(qt, axis=1)
+    purity = float(sum(np.bincount(true[cl == k], minlength=K).max() for k in range(K) if (cl == k).any()) / spec.I)
+    sec = float(np.median(times))
+    out = {"skfr": args.skfr_mode, "config": spec.name, "I": spec.I, "J": spec.J, "K": K, "sparsity": s,
+           "s_per_run": sec, "runs": len(times), "s_runs": [round(t, 4) for t in times], "iterations": it.value, "ms_per_iteration": 1e3 * sec / it.value,
+           "n_aims": n.value, "objective": obj.value, "purity_vs_truth": purity, "seed": seed}
+    if args.skfr_cpu or args.config == "c1":
+        import skfr_oracle as S
+        host = g.to_host()
+        t0 = time.perf_counter()
+        c_o, a_o, obj_o, it_o = S.skfr(np.asarray(host.data), spec.I, K, s, mode=args.skfr_mode, seed=seed)
+        cpu = time.perf_counter() - t0
+        out["cpu_oracle"] = {"s_per_run": cpu, "cores": 1, "kind": "port",
+                             "identical": bool(np.array_equal(c_o, cl) and np.array_equal(a_o, aims[: n.value])
+                                               and it_o == it.value and abs(obj_o - obj.value) <= 1e-12 * abs(obj_o))}
+    print(json.dumps(out), flush=True)
     return 0
 
 
@@ -734,6 +791,8 @@ def main():
         return run_reference(args, rank, world)
     if args.pass_only:
         return run_pass_only(args)
+    if args.skfr is not None:
+        return run_skfr(args)
     if args.config == "c4":
         return run_batch(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)

@@ -13,18 +13,20 @@
  *     32-bit word of a column) and a slice of SKFR_SLICE SNPs, adding table entries staged in
  *     shared memory in FP64, the slice sums added in slice order (k_skfr_dist, k_skfr_dist_sum);
  *   - per iteration, the cluster sums of every SNP as exact integers: membership bit masks per
- *     16-individual word and the cluster sizes (k_skfr_masks), then per SNP and cluster one popcount
- *     of the dosage bits and one of the missing bits under the mask (k_skfr_sums, one thread per SNP
- *     streaming its column, masks broadcast from shared memory); centres and feature scores in FP64
- *     (k_skfr_means);
+ *     16-individual word and the cluster sizes (k_skfr_masks), then per SNP and cluster but the last
+ *     one popcount of the dosage bits per word and one of the missing bits per two words under the
+ *     masks (k_skfr_sums, one thread per SNP streaming its column, masks broadcast from shared
+ *     memory); the last cluster's sums are the SNP's totals less the others'; centres and feature
+ *     scores in FP64 (k_skfr_means);
  *   - the `sparsity` largest scores of each kept list (ties to the lower index) by a radix select
  *     on the scores' bit patterns and an index-order compaction, one block per list (k_skfr_select);
- *   - the reassignment scores of every individual on the kept SNPs: one thread per individual and
- *     slice of SKFR_ASLICE kept SNPs, FP64 sums in SNP order with the terms of SKFR_ACHUNK SNPs at a
- *     time in shared memory (k_skfr_assign_shared: one list for all clusters, each code read once;
- *     k_skfr_assign_own: each cluster's own list), the slice sums then added in order
- *     (k_skfr_assign_sum); the argmin over clusters and the count of changed assignments
- *     (k_skfr_argmin).
+ *   - the reassignment scores of every individual on the kept SNPs: the terms of each two
+ *     consecutive kept SNPs added for all 16 code pairs (k_skfr_pairs), then one thread per
+ *     individual and slice of SKFR_ASLICE kept SNPs adds one pair entry per two SNPs in FP64, in SNP
+ *     order, with the pair tables of a chunk in shared memory (k_skfr_assign_shared: one list for all
+ *     clusters, each code read once; k_skfr_assign_own: each cluster's own list), the slice sums then
+ *     added in order (k_skfr_assign_sum); the argmin over clusters and the count of changed
+ *     assignments (k_skfr_argmin).
  * The host keeps the sequential k-means++ draws from a splitmix64 stream, reads one count per
  * iteration for the convergence test, and sums the objective in individual order at the end of a
  * try.  Every FP64 operation whose rounding the oracle reproduces is written with explicit
@@ -43,7 +45,7 @@ constexpr int SKFR_SLICE = 1024;     /* SNPs per partial sum of the seeding dist
 constexpr int SKFR_DCHUNK = 128;     /* SNPs whose squared differences are staged in shared memory at a time */
 constexpr int SKFR_WCHUNK = 256;     /* 16-individual words of masks staged per shared-memory chunk */
 constexpr int SKFR_ASLICE = 1024;    /* kept SNPs per partial sum of the reassignment scores */
-constexpr int SKFR_ACHUNK = 64;      /* kept SNPs whose terms are staged in shared memory at a time */
+constexpr int SKFR_ACHUNK = 32;      /* kept SNPs whose pair tables are staged in shared memory at a time */
 constexpr int SKFR_SEL_THREADS = 1024;
 
 __device__ __forceinline__ uint32_t col_word(const uint8_t *bed, int64_t pitch, int64_t l, int64_t w)
@@ -175,13 +177,13 @@ __global__ void k_skfr_masks(const int32_t *__restrict__ cl, int64_t I, int64_t 
 }
 
 /* one word of a column: dosage sums and missing counts under each cluster's mask */
-template <int K>
+template <int KC>
 __device__ __forceinline__ void sums_word(uint32_t x, const uint32_t (*ms)[SKFR_WCHUNK], int w, int32_t *sg, int32_t *sm)
 {
     const uint32_t hi = (x >> 1) & 0x55555555u, lo = x & 0x55555555u;
     const uint32_t h2 = hi & lo, mi = ~hi & lo;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
+    for (int k = 0; k < KC; ++k) {
         /* dosage = hi + (hi & lo), both on the even bits: one count of (hi & m) | ((hi & lo & m) << 1) */
         const uint32_t m = ms[k][w];
         sg[k] += __popc((hi & m) | ((h2 & m) << 1));
@@ -189,22 +191,39 @@ __device__ __forceinline__ void sums_word(uint32_t x, const uint32_t (*ms)[SKFR_
     }
 }
 
-/* per SNP l and cluster k: S = sum of the members' dosages, M = members with a missing code
- * (one thread per SNP, its column streamed 64 bytes at a time, masks staged in shared memory) */
-template <int K>
+/* two words: the missing bits (even bits only) of the second shifted onto the odd bits, one count */
+template <int KC>
+__device__ __forceinline__ void sums_pair(uint32_t x0, uint32_t x1, const uint32_t (*ms)[SKFR_WCHUNK], int w, int32_t *sg,
+                                          int32_t *sm)
+{
+    const uint32_t hi0 = (x0 >> 1) & 0x55555555u, lo0 = x0 & 0x55555555u;
+    const uint32_t hi1 = (x1 >> 1) & 0x55555555u, lo1 = x1 & 0x55555555u;
+    const uint32_t h20 = hi0 & lo0, mi0 = ~hi0 & lo0, h21 = hi1 & lo1, mi1 = ~hi1 & lo1;
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+        const uint32_t m0 = ms[k][w], m1 = ms[k][w + 1];
+        sg[k] += __popc((hi0 & m0) | ((h20 & m0) << 1)) + __popc((hi1 & m1) | ((h21 & m1) << 1));
+        sm[k] += __popc((mi0 & m0) | ((mi1 & m1) << 1));
+    }
+}
+
+/* per SNP l and cluster k < KC (all clusters but the last): S = sum of the members' dosages,
+ * M = members with a missing code (one thread per SNP, its column streamed 64 bytes at a time, masks
+ * staged in shared memory) */
+template <int KC>
 __global__ void __launch_bounds__(128)
 k_skfr_sums(const uint8_t *__restrict__ bed, int64_t pitch, int64_t nw, int64_t J, const uint32_t *__restrict__ mask,
             int32_t *__restrict__ S, int32_t *__restrict__ M)
 {
-    __shared__ uint32_t ms[K][SKFR_WCHUNK];
+    __shared__ uint32_t ms[KC][SKFR_WCHUNK];
     const int64_t l = (int64_t)blockIdx.x * 128 + threadIdx.x;
-    int32_t sg[K], sm[K];
+    int32_t sg[KC], sm[KC];
 #pragma unroll
-    for (int k = 0; k < K; ++k) sg[k] = sm[k] = 0;
+    for (int k = 0; k < KC; ++k) sg[k] = sm[k] = 0;
     for (int64_t w0 = 0; w0 < nw; w0 += SKFR_WCHUNK) {
         const int nwc = (int)min((int64_t)SKFR_WCHUNK, nw - w0);
         __syncthreads();
-        for (int t = threadIdx.x; t < K * SKFR_WCHUNK; t += 128) {
+        for (int t = threadIdx.x; t < KC * SKFR_WCHUNK; t += 128) {
             const int k = t / SKFR_WCHUNK, w = t - k * SKFR_WCHUNK;
             ms[k][w] = w < nwc ? mask[(size_t)k * nw + w0 + w] : 0u;
         }
@@ -219,22 +238,22 @@ k_skfr_sums(const uint8_t *__restrict__ bed, int64_t pitch, int64_t nw, int64_t 
                 for (int u = 0; u < 4; ++u) v[u] = *(const uint4 *)(col + (size_t)(w + 4 * u) * 4);
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    sums_word<K>(v[u].x, ms, w + 4 * u, sg, sm);
-                    sums_word<K>(v[u].y, ms, w + 4 * u + 1, sg, sm);
-                    sums_word<K>(v[u].z, ms, w + 4 * u + 2, sg, sm);
-                    sums_word<K>(v[u].w, ms, w + 4 * u + 3, sg, sm);
+                    sums_pair<KC>(v[u].x, v[u].y, ms, w + 4 * u, sg, sm);
+                    sums_pair<KC>(v[u].z, v[u].w, ms, w + 4 * u + 2, sg, sm);
                 }
             }
             for (; w < nwc; w += 4) {
                 const uint4 v = *(const uint4 *)(col + (size_t)w * 4);
-                const uint32_t xs[4] = {v.x, v.y, v.z, v.w};
-                for (int q = 0; q < 4 && w + q < nwc; ++q) sums_word<K>(xs[q], ms, w + q, sg, sm);
+                if (w + 1 < nwc) sums_pair<KC>(v.x, v.y, ms, w, sg, sm);
+                else sums_word<KC>(v.x, ms, w, sg, sm);
+                if (w + 3 < nwc) sums_pair<KC>(v.z, v.w, ms, w + 2, sg, sm);
+                else if (w + 2 < nwc) sums_word<KC>(v.z, ms, w + 2, sg, sm);
             }
         }
     }
     if (l < J) {
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
+        for (int k = 0; k < KC; ++k) {
             S[(size_t)k * J + l] = sg[k];
             M[(size_t)k * J + l] = sm[k];
         }
@@ -242,21 +261,34 @@ k_skfr_sums(const uint8_t *__restrict__ bed, int64_t pitch, int64_t nw, int64_t 
 }
 
 /* theta_kl = (a_l S_kl - b_l n_kl) / N_k (n_kl = N_k - M_kl non-missing members) and the feature
- * scores: global r_l = sum_k N_k theta_kl^2, local r_kl = N_k theta_kl^2 */
-__global__ void k_skfr_means(const int32_t *__restrict__ S, const int32_t *__restrict__ M, const double *__restrict__ ab,
-                             const int32_t *__restrict__ Nk, int K, int64_t J, int local, double *__restrict__ theta,
-                             double *__restrict__ score)
+ * scores: global r_l = sum_k N_k theta_kl^2, local r_kl = N_k theta_kl^2.  S and M hold clusters
+ * 0..K-2; the last cluster's are the SNP's totals (class counts cnt) less theirs. */
+__global__ void k_skfr_means(const int32_t *__restrict__ S, const int32_t *__restrict__ M, const int64_t *__restrict__ cnt,
+                             int64_t I, const double *__restrict__ ab, const int32_t *__restrict__ Nk, int K, int64_t J,
+                             int local, double *__restrict__ theta, double *__restrict__ score)
 {
     const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= J) return;
     const double a = ab[2 * l], b = ab[2 * l + 1];
+    int64_t s_last = cnt[3 * l + 1] + 2 * cnt[3 * l + 2];
+    int64_t m_last = I - cnt[3 * l] - cnt[3 * l + 1] - cnt[3 * l + 2];
     double r = 0.0;
     for (int k = 0; k < K; ++k) {
+        int64_t sk, mk;
+        if (k < K - 1) {
+            sk = S[(size_t)k * J + l];
+            mk = M[(size_t)k * J + l];
+            s_last -= sk;
+            m_last -= mk;
+        } else {
+            sk = s_last;
+            mk = m_last;
+        }
         double t = 0.0;
         const double nk = (double)Nk[k];
         if (nk > 0.0) {
-            const double n = nk - (double)M[(size_t)k * J + l];
-            t = __ddiv_rn(__dsub_rn(__dmul_rn(a, (double)S[(size_t)k * J + l]), __dmul_rn(b, n)), nk);
+            const double n = nk - (double)mk;
+            t = __ddiv_rn(__dsub_rn(__dmul_rn(a, (double)sk), __dmul_rn(b, n)), nk);
         }
         theta[(size_t)k * J + l] = t;
         const double rk = __dmul_rn(__dmul_rn(nk, t), t);
@@ -379,33 +411,54 @@ k_skfr_select(const double *__restrict__ score, int64_t J, int64_t s, int32_t *_
     }
 }
 
-/* per cluster k, kept SNP (list position p, list k * kstride: one shared list when kstride is 0) and
- * code: terms[k][p][code] = theta^2 - (2 x) theta, x = xt[l][code] */
-__global__ void k_skfr_terms(const double *__restrict__ theta, const double *__restrict__ xt, const int32_t *__restrict__ kept,
-                             int64_t nkept, int64_t kstride, int K, int64_t J, double *__restrict__ terms)
+/* Pair tables of the reassignment terms.  For cluster k and pair r of its kept list (list k * kstride:
+ * one shared list when kstride is 0; list positions q = 2r and q + 1) and codes c1, c2:
+ * pt[k][r][4 c1 + c2] = T(q, c1) + T(q + 1, c2), with T(p, c) = theta_kl^2 - (2 x_l,c) theta_kl for l
+ * the SNP at position p; an odd last position alone gives T(q, c1) for every c2. */
+__global__ void k_skfr_pairs(const double *__restrict__ theta, const double *__restrict__ xt, const int32_t *__restrict__ kept,
+                             int64_t nkept, int64_t kstride, int K, int64_t J, double *__restrict__ pt)
 {
+    const int64_t npair = (nkept + 1) / 2;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int64_t)K * nkept) return;
-    const int k = (int)(t / nkept);
-    const int64_t l = kept[k * kstride + (t - k * nkept)];
-    const double th = theta[(size_t)k * J + l], tt = __dmul_rn(th, th);
-    for (int c = 0; c < 4; ++c)
-        terms[4 * t + c] = __dsub_rn(tt, __dmul_rn(__dmul_rn(2.0, xt[4 * l + c]), th));
+    if (t >= (int64_t)K * npair) return;
+    const int k = (int)(t / npair);
+    const int64_t r = t - k * npair;
+    const int32_t *kl = kept + k * kstride;
+    const bool two = 2 * r + 1 < nkept;
+    double a[4], b[4];
+    {
+        const int64_t l = kl[2 * r];
+        const double th = theta[(size_t)k * J + l], tt = __dmul_rn(th, th);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a[c] = __dsub_rn(tt, __dmul_rn(__dmul_rn(2.0, xt[4 * l + c]), th));
+    }
+    if (two) {
+        const int64_t l = kl[2 * r + 1];
+        const double th = theta[(size_t)k * J + l], tt = __dmul_rn(th, th);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) b[c] = __dsub_rn(tt, __dmul_rn(__dmul_rn(2.0, xt[4 * l + c]), th));
+    }
+    double *o = pt + (size_t)t * 16;
+#pragma unroll
+    for (int c1 = 0; c1 < 4; ++c1)
+#pragma unroll
+        for (int c2 = 0; c2 < 4; ++c2) o[4 * c1 + c2] = two ? __dadd_rn(a[c1], b[c2]) : a[c1];
 }
 
 /* Reassignment scores, one shared kept list (global mode): thread = individual i, blockIdx.y = slice
- * of SKFR_ASLICE list positions; part[y][i][k] = sum over the slice (list order, FP64 from 0) of
- * terms[k][p][code_ip].  The terms of SKFR_ACHUNK positions are staged in shared memory as
- * [p][code][k] with an odd row stride, so the four codes of one position fall in different banks;
- * each code is read once for all K clusters. */
+ * of SKFR_ASLICE list positions; part[y][i][k] = sum over the slice's pairs (list order, FP64 from 0)
+ * of pt[k][pair][4 code_q + code_q+1].  The pair tables of SKFR_ACHUNK positions are staged in
+ * shared memory as [pair][code pair][k] with an odd row stride, so the 16 code pairs of one pair fall
+ * in different banks; each code is read once for all K clusters. */
 template <int K>
 __global__ void __launch_bounds__(128)
 k_skfr_assign_shared(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, const int32_t *__restrict__ kept,
-                     int64_t nkept, const double *__restrict__ terms, double *__restrict__ part)
+                     int64_t nkept, const double *__restrict__ pt, double *__restrict__ part)
 {
     constexpr int KS = K | 1;
-    __shared__ double ts[SKFR_ACHUNK * 4 * KS];
+    __shared__ double ts[(SKFR_ACHUNK / 2) * 16 * KS];
     __shared__ int32_t ls[SKFR_ACHUNK];
+    const int64_t npair = (nkept + 1) / 2;
     const int64_t i = (int64_t)blockIdx.x * 128 + threadIdx.x;
     const int64_t p0 = (int64_t)blockIdx.y * SKFR_ASLICE, p1 = min(nkept, p0 + SKFR_ASLICE);
     const int sh = (int)(i & 3) * 2;
@@ -413,30 +466,34 @@ k_skfr_assign_shared(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, 
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
-    for (int64_t q0 = p0; q0 < p1; q0 += SKFR_ACHUNK) {
-        const int n = (int)min((int64_t)SKFR_ACHUNK, p1 - q0);
+    for (int64_t q0 = p0; q0 < p1; q0 += SKFR_ACHUNK) {          /* q0 is even */
+        const int n = (int)min((int64_t)SKFR_ACHUNK, p1 - q0), np = (n + 1) / 2;
+        const int64_t r0 = q0 / 2;
         __syncthreads();
-        for (int t = threadIdx.x; t < n * 4 * K; t += 128) {
-            const int k = t / (n * 4), r = t - k * (n * 4);          /* r = position * 4 + code */
-            ts[r * KS + k] = terms[((size_t)k * nkept + q0) * 4 + r];
+        for (int t = threadIdx.x; t < np * 16 * K; t += 128) {
+            const int k = t / (np * 16), e = t - k * (np * 16);       /* e = pair * 16 + code pair */
+            ts[e * KS + k] = pt[((size_t)k * npair + r0) * 16 + e];
         }
-        for (int t = threadIdx.x; t < n; t += 128) ls[t] = kept[q0 + t];
+        /* an odd last position is paired with itself: its table ignores the second code */
+        for (int t = threadIdx.x; t < 2 * np; t += 128) ls[t] = kept[q0 + min(t, n - 1)];
         __syncthreads();
         if (i < I) {
             int pp = 0;
-            for (; pp + 8 <= n; pp += 8) {
+            for (; pp + 4 <= np; pp += 4) {
                 uint32_t c[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) c[u] = base[(size_t)ls[pp + u] * pitch];
+                for (int u = 0; u < 8; ++u) c[u] = base[(size_t)ls[2 * pp + u] * pitch];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const double *tp = ts + ((pp + u) * 4 + ((c[u] >> sh) & 3)) * KS;
+                for (int u = 0; u < 4; ++u) {
+                    const int cp = (int)(((c[2 * u] >> sh) & 3u) * 4 + ((c[2 * u + 1] >> sh) & 3u));
+                    const double *tp = ts + ((pp + u) * 16 + cp) * KS;
 #pragma unroll
                     for (int k = 0; k < K; ++k) acc[k] = __dadd_rn(acc[k], tp[k]);
                 }
             }
-            for (; pp < n; ++pp) {
-                const double *tp = ts + (pp * 4 + ((base[(size_t)ls[pp] * pitch] >> sh) & 3)) * KS;
+            for (; pp < np; ++pp) {
+                const uint32_t c0 = base[(size_t)ls[2 * pp] * pitch], c1 = base[(size_t)ls[2 * pp + 1] * pitch];
+                const double *tp = ts + (pp * 16 + (int)(((c0 >> sh) & 3u) * 4 + ((c1 >> sh) & 3u))) * KS;
 #pragma unroll
                 for (int k = 0; k < K; ++k) acc[k] = __dadd_rn(acc[k], tp[k]);
             }
@@ -450,37 +507,43 @@ k_skfr_assign_shared(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, 
 }
 
 /* Reassignment scores, each cluster its own kept list (local mode): as k_skfr_assign_shared with
- * blockIdx.z = cluster k, its list kept[k] and terms[k]. */
+ * blockIdx.z = cluster k, its list kept[k] and pair tables pt[k]. */
 __global__ void __launch_bounds__(128)
 k_skfr_assign_own(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, const int32_t *__restrict__ kept,
-                  int64_t nkept, int K, const double *__restrict__ terms, double *__restrict__ part)
+                  int64_t nkept, int K, const double *__restrict__ pt, double *__restrict__ part)
 {
-    __shared__ double ts[SKFR_ACHUNK * 4];
+    __shared__ double ts[(SKFR_ACHUNK / 2) * 16];
     __shared__ int32_t ls[SKFR_ACHUNK];
     const int k = blockIdx.z;
+    const int64_t npair = (nkept + 1) / 2;
     const int64_t i = (int64_t)blockIdx.x * 128 + threadIdx.x;
     const int64_t p0 = (int64_t)blockIdx.y * SKFR_ASLICE, p1 = min(nkept, p0 + SKFR_ASLICE);
     const int sh = (int)(i & 3) * 2;
     const uint8_t *base = bed + (size_t)(i >> 2);
     const int32_t *kl = kept + (size_t)k * nkept;
-    const double *tk = terms + (size_t)k * nkept * 4;
+    const double *tk = pt + (size_t)k * npair * 16;
     double acc = 0.0;
     for (int64_t q0 = p0; q0 < p1; q0 += SKFR_ACHUNK) {
-        const int n = (int)min((int64_t)SKFR_ACHUNK, p1 - q0);
+        const int n = (int)min((int64_t)SKFR_ACHUNK, p1 - q0), np = (n + 1) / 2;
+        const int64_t r0 = q0 / 2;
         __syncthreads();
-        for (int t = threadIdx.x; t < n * 4; t += 128) ts[t] = tk[q0 * 4 + t];
-        for (int t = threadIdx.x; t < n; t += 128) ls[t] = kl[q0 + t];
+        for (int t = threadIdx.x; t < np * 16; t += 128) ts[t] = tk[r0 * 16 + t];
+        for (int t = threadIdx.x; t < 2 * np; t += 128) ls[t] = kl[q0 + min(t, n - 1)];
         __syncthreads();
         if (i < I) {
             int pp = 0;
-            for (; pp + 8 <= n; pp += 8) {
+            for (; pp + 4 <= np; pp += 4) {
                 uint32_t c[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) c[u] = base[(size_t)ls[pp + u] * pitch];
+                for (int u = 0; u < 8; ++u) c[u] = base[(size_t)ls[2 * pp + u] * pitch];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) acc = __dadd_rn(acc, ts[(pp + u) * 4 + ((c[u] >> sh) & 3)]);
+                for (int u = 0; u < 4; ++u)
+                    acc = __dadd_rn(acc, ts[(pp + u) * 16 + (int)(((c[2 * u] >> sh) & 3u) * 4 + ((c[2 * u + 1] >> sh) & 3u))]);
             }
-            for (; pp < n; ++pp) acc = __dadd_rn(acc, ts[pp * 4 + ((base[(size_t)ls[pp] * pitch] >> sh) & 3)]);
+            for (; pp < np; ++pp) {
+                const uint32_t c0 = base[(size_t)ls[2 * pp] * pitch], c1 = base[(size_t)ls[2 * pp + 1] * pitch];
+                acc = __dadd_rn(acc, ts[pp * 16 + (int)(((c0 >> sh) & 3u) * 4 + ((c1 >> sh) & 3u))]);
+            }
         }
     }
     if (i < I) part[((size_t)blockIdx.y * I + i) * K + k] = acc;
@@ -531,17 +594,21 @@ struct SplitMix64 {
 /* the kernels templated on the cluster count, for one K */
 template <int K>
 struct SkfrK {
+    /* sums of clusters 0..K-2 (none for one cluster: the totals are its sums) */
     static cudaError_t sums(const uint8_t *bed, int64_t pitch, int64_t nw, int64_t J, const uint32_t *mask, int32_t *S,
                             int32_t *M, cudaStream_t st)
     {
-        k_skfr_sums<K><<<(unsigned)((J + 127) / 128), 128, 0, st>>>(bed, pitch, nw, J, mask, S, M);
-        return cudaGetLastError();
+        if constexpr (K > 1) {
+            k_skfr_sums<K - 1><<<(unsigned)((J + 127) / 128), 128, 0, st>>>(bed, pitch, nw, J, mask, S, M);
+            return cudaGetLastError();
+        }
+        return cudaSuccess;
     }
     static cudaError_t assign_shared(const uint8_t *bed, int64_t pitch, int64_t I, const int32_t *kept, int64_t nkept,
-                                     const double *terms, double *part, cudaStream_t st)
+                                     const double *pt, double *part, cudaStream_t st)
     {
         const dim3 grid((unsigned)((I + 127) / 128), (unsigned)((nkept + SKFR_ASLICE - 1) / SKFR_ASLICE));
-        k_skfr_assign_shared<K><<<grid, 128, 0, st>>>(bed, pitch, I, kept, nkept, terms, part);
+        k_skfr_assign_shared<K><<<grid, 128, 0, st>>>(bed, pitch, I, kept, nkept, pt, part);
         return cudaGetLastError();
     }
 };
@@ -564,9 +631,9 @@ cudaError_t sums_for_k(int K, const uint8_t *bed, int64_t pitch, int64_t nw, int
 }
 
 cudaError_t assign_shared_for_k(int K, const uint8_t *bed, int64_t pitch, int64_t I, const int32_t *kept, int64_t nkept,
-                                const double *terms, double *part, cudaStream_t st)
+                                const double *pt, double *part, cudaStream_t st)
 {
-    SKFR_DISPATCH(K, assign_shared(bed, pitch, I, kept, nkept, terms, part, st))
+    SKFR_DISPATCH(K, assign_shared(bed, pitch, I, kept, nkept, pt, part, st))
 }
 #undef SKFR_DISPATCH
 
@@ -597,7 +664,7 @@ cudaError_t skfr_run(const uint8_t *bed, int64_t pitch, int64_t I, int64_t J, in
     const int nlists = local ? K : 1;                 /* kept lists: one for all clusters, or one per cluster */
     if ((int64_t)nslice > 65535 || (int64_t)naslice > 65535 || J > INT32_MAX) return cudaErrorInvalidValue;
     DevBuf<int64_t> d_cnt;
-    DevBuf<double> d_xt, d_ab, d_sq, d_partial, d_D, d_theta, d_score, d_terms, d_apart, d_sc;
+    DevBuf<double> d_xt, d_ab, d_sq, d_partial, d_D, d_theta, d_score, d_pt, d_apart, d_sc;
     DevBuf<uint32_t> d_mask;
     DevBuf<int32_t> d_cl, d_cl2, d_nk, d_changed, d_S, d_M, d_kept;
     SK_TRY(d_cnt.alloc(3 * J));
@@ -608,7 +675,8 @@ cudaError_t skfr_run(const uint8_t *bed, int64_t pitch, int64_t I, int64_t J, in
     SK_TRY(d_D.alloc(I));
     SK_TRY(d_theta.alloc((size_t)K * J));
     SK_TRY(d_score.alloc((size_t)nlists * J));
-    SK_TRY(d_terms.alloc((size_t)K * s * 4));
+    const int64_t npair = (s + 1) / 2;                /* kept-list pairs */
+    SK_TRY(d_pt.alloc((size_t)K * npair * 16));
     SK_TRY(d_apart.alloc((size_t)naslice * I * K));
     SK_TRY(d_sc.alloc((size_t)I * K));
     SK_TRY(d_mask.alloc((size_t)K * nw));
@@ -669,26 +737,26 @@ cudaError_t skfr_run(const uint8_t *bed, int64_t pitch, int64_t I, int64_t J, in
         SK_TRY(cudaMemcpyAsync(out, d_D.p, sizeof(double) * I, cudaMemcpyDeviceToHost, st));
         return cudaStreamSynchronize(st);
     };
-    /* for the assignment dcl: cluster sizes, centres, scores, kept lists, terms and sc[i][k] (no sync) */
+    /* for the assignment dcl: cluster sizes, centres, scores, kept lists, pair tables and sc[i][k] (no sync) */
     auto pass = [&](const int32_t *dcl) -> cudaError_t {
         SK_TRY(cudaMemsetAsync(d_nk.p, 0, sizeof(int32_t) * K, st));
         k_skfr_masks<<<(unsigned)((nw + 127) / 128), 128, 0, st>>>(dcl, I, nw, K, d_mask.p, d_nk.p);
         SK_TRY(cudaGetLastError());
         SK_TRY(sums_for_k(K, bed, pitch, nw, J, d_mask.p, d_S.p, d_M.p, st));
-        k_skfr_means<<<(unsigned)((J + 255) / 256), 256, 0, st>>>(d_S.p, d_M.p, d_ab.p, d_nk.p, K, J, local, d_theta.p,
-                                                                d_score.p);
+        k_skfr_means<<<(unsigned)((J + 255) / 256), 256, 0, st>>>(d_S.p, d_M.p, d_cnt.p, I, d_ab.p, d_nk.p, K, J, local,
+                                                                d_theta.p, d_score.p);
         SK_TRY(cudaGetLastError());
         k_skfr_select<<<(unsigned)nlists, SKFR_SEL_THREADS, 0, st>>>(d_score.p, J, s, d_kept.p);
         SK_TRY(cudaGetLastError());
-        k_skfr_terms<<<(unsigned)((K * s + 255) / 256), 256, 0, st>>>(d_theta.p, d_xt.p, d_kept.p, s, local ? s : 0, K, J,
-                                                                     d_terms.p);
+        k_skfr_pairs<<<(unsigned)((K * npair + 255) / 256), 256, 0, st>>>(d_theta.p, d_xt.p, d_kept.p, s, local ? s : 0, K,
+                                                                         J, d_pt.p);
         SK_TRY(cudaGetLastError());
         if (local) {
             const dim3 grid((unsigned)((I + 127) / 128), (unsigned)naslice, (unsigned)K);
-            k_skfr_assign_own<<<grid, 128, 0, st>>>(bed, pitch, I, d_kept.p, s, K, d_terms.p, d_apart.p);
+            k_skfr_assign_own<<<grid, 128, 0, st>>>(bed, pitch, I, d_kept.p, s, K, d_pt.p, d_apart.p);
             SK_TRY(cudaGetLastError());
         } else {
-            SK_TRY(assign_shared_for_k(K, bed, pitch, I, d_kept.p, s, d_terms.p, d_apart.p, st));
+            SK_TRY(assign_shared_for_k(K, bed, pitch, I, d_kept.p, s, d_pt.p, d_apart.p, st));
         }
         k_skfr_assign_sum<<<(unsigned)((I * K + 255) / 256), 256, 0, st>>>(d_apart.p, I * K, naslice, d_sc.p);
         return cudaGetLastError();

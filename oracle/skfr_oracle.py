@@ -21,7 +21,8 @@ implementation (csrc/skfr.cu), which this oracle checks exactly:
   scores r_l = sum_k n_k theta_kl^2, the `sparsity` SNPs of largest score kept (ties to the lower
   index), centres zero elsewhere, each individual reassigned to
   argmin_k sum_{l kept} theta_kl^2 - 2 x_il theta_kl (ties to the lower cluster), the sum in FP64
-  over each ASLICE kept SNPs in SNP order, the slice sums then added in order; stop when no
+  over each ASLICE kept SNPs in SNP order, two SNPs at a time (the terms of list positions 2r and
+  2r+1 added first, an odd last position alone), the slice sums then added in order; stop when no
   assignment changes or after max_iter iterations;
 - "local" mode: each cluster keeps its own `sparsity` SNPs by n_k theta_kl^2 and is scored on
   them; the AIMs are the union of the kept sets;
@@ -152,18 +153,27 @@ def top_s(score: np.ndarray, s: int) -> np.ndarray:
 
 def scores(codes: np.ndarray, xt: np.ndarray, theta: np.ndarray, kept: list[np.ndarray]) -> np.ndarray:
     """sc[i, k] = sum_{l in kept[k]} theta_kl^2 - 2 x_il theta_kl: FP64 sums over each ASLICE kept
-    SNPs in SNP order, the slice sums added in order"""
+    SNPs in SNP order, two list positions at a time (their terms added first), the slice sums
+    added in order"""
     I = codes.shape[0]
     K = theta.shape[0]
     sc = np.zeros((I, K))
+
+    def term(k, l):
+        t = theta[k, l]
+        return t * t - 2.0 * xt[l, codes[:, l]] * t
+
     for k in range(K):
         lst = kept[k]
         total = np.zeros(I)
         for p0 in range(0, len(lst), ASLICE):
             part = np.zeros(I)
-            for l in lst[p0:p0 + ASLICE]:
-                t = theta[k, l]
-                part += t * t - 2.0 * xt[l, codes[:, l]] * t
+            sl = lst[p0:p0 + ASLICE]
+            for q in range(0, len(sl), 2):
+                t = term(k, sl[q])
+                if q + 1 < len(sl):
+                    t = t + term(k, sl[q + 1])
+                part += t
             total += part
         sc[:, k] = total
     return sc

@@ -27,8 +27,8 @@ def _cohort(oa, I, J, K, seed, alpha=0.05):
     (437, 5000, 4, 300, "global", 3),      # two seeding slices, partial words
     (250, 1200, 6, 100, "local", 2),
     (300, 6000, 3, 2500, "global", 1),     # three reassignment slices of 1024 kept SNPs
-    (260, 5000, 4, 1500, "local", 1),      # two slices per cluster list
-    (200, 2500, 16, 1100, "global", 1),    # the largest K
+    (260, 5000, 4, 1501, "local", 1),      # two slices per cluster list, an odd last pair
+    (200, 2500, 16, 1101, "global", 1),    # the largest K, an odd last pair
     (150, 800, 2, 5000, "local", 1),       # sparsity above J: every SNP kept
     (90, 700, 1, 100, "global", 1),        # one cluster
 ])
