@@ -445,11 +445,37 @@ __global__ void k_skfr_pairs(const double *__restrict__ theta, const double *__r
         for (int c2 = 0; c2 < 4; ++c2) o[4 * c1 + c2] = two ? __dadd_rn(a[c1], b[c2]) : a[c1];
 }
 
+/* The codes of a chunk's kept SNPs for a block's 128 individuals (32 bytes per SNP): thread t loads
+ * the 8 bytes 8 (t & 3) .. 8 (t & 3) + 7 of list position t >> 2 (positions past the chunk's n repeat
+ * its last SNP).  The 32 bytes from i0 / 4 stay inside the column's 16-byte pitch but for the last
+ * block, whose overrun (at most 16 bytes, for individuals beyond I) falls in the next column or in
+ * the 64 bytes after the last one. */
+__device__ __forceinline__ uint2 load_codes(const uint8_t *__restrict__ bed, int64_t pitch, int64_t i0,
+                                            const int32_t *__restrict__ kl, int64_t q0, int n)
+{
+    const int pos = min((int)(threadIdx.x >> 2), n - 1);
+    return *(const uint2 *)(bed + (size_t)kl[q0 + pos] * pitch + (size_t)(i0 >> 2) + 8u * (threadIdx.x & 3u));
+}
+
+/* The loaded codes interleaved by pair: cp[r][2m] = byte m of position 2r, cp[r][2m + 1] = byte m of
+ * position 2r + 1 (the partner thread t ^ 4 holds the other position of the pair).  Every thread of
+ * the block calls it. */
+__device__ __forceinline__ void store_codes(uint8_t (*cp)[64], uint2 v)
+{
+    const uint2 o = make_uint2(__shfl_xor_sync(0xffffffffu, v.x, 4), __shfl_xor_sync(0xffffffffu, v.y, 4));
+    const int pos = threadIdx.x >> 2, seg = threadIdx.x & 3;
+    const bool even = (pos & 1) == 0;
+    const uint32_t a = even ? v.x : o.y, b = even ? o.x : v.y;   /* position 2r's and 2r+1's 4 bytes */
+    *(uint2 *)&cp[pos >> 1][seg * 16 + (even ? 0 : 8)] = make_uint2(__byte_perm(a, b, 0x5140), __byte_perm(a, b, 0x7362));
+}
+
 /* Reassignment scores, one shared kept list (global mode): thread = individual i, blockIdx.y = slice
  * of SKFR_ASLICE list positions; part[y][i][k] = sum over the slice's pairs (list order, FP64 from 0)
- * of pt[k][pair][4 code_q + code_q+1].  The pair tables of SKFR_ACHUNK positions are staged in
- * shared memory as [pair][code pair][k] with an odd row stride, so the 16 code pairs of one pair fall
- * in different banks; each code is read once for all K clusters. */
+ * of pt[k][pair][4 code_q + code_q+1].  Per chunk of SKFR_ACHUNK positions the block stages the pair
+ * tables as [pair][code pair][k] with an odd row stride (the 16 code pairs of one pair fall in
+ * different banks) and the chunk's codes interleaved by pair (one 16-bit load per pair and thread),
+ * the codes of the next chunk loaded while this one is summed; each code is read once for all K
+ * clusters. */
 template <int K>
 __global__ void __launch_bounds__(128)
 k_skfr_assign_shared(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, const int32_t *__restrict__ kept,
@@ -457,15 +483,15 @@ k_skfr_assign_shared(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, 
 {
     constexpr int KS = K | 1;
     __shared__ double ts[(SKFR_ACHUNK / 2) * 16 * KS];
-    __shared__ int32_t ls[SKFR_ACHUNK];
+    __shared__ __align__(16) uint8_t cp[SKFR_ACHUNK / 2][64];
     const int64_t npair = (nkept + 1) / 2;
-    const int64_t i = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.x * 128, i = i0 + threadIdx.x;
     const int64_t p0 = (int64_t)blockIdx.y * SKFR_ASLICE, p1 = min(nkept, p0 + SKFR_ASLICE);
-    const int sh = (int)(i & 3) * 2;
-    const uint8_t *base = bed + (size_t)(i >> 2);
+    const int sh = (int)(threadIdx.x & 3) * 2, cb = 2 * (int)(threadIdx.x >> 2);
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    uint2 cv = load_codes(bed, pitch, i0, kept, p0, (int)min((int64_t)SKFR_ACHUNK, p1 - p0));
     for (int64_t q0 = p0; q0 < p1; q0 += SKFR_ACHUNK) {          /* q0 is even */
         const int n = (int)min((int64_t)SKFR_ACHUNK, p1 - q0), np = (n + 1) / 2;
         const int64_t r0 = q0 / 2;
@@ -474,26 +500,16 @@ k_skfr_assign_shared(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, 
             const int k = t / (np * 16), e = t - k * (np * 16);       /* e = pair * 16 + code pair */
             ts[e * KS + k] = pt[((size_t)k * npair + r0) * 16 + e];
         }
-        /* an odd last position is paired with itself: its table ignores the second code */
-        for (int t = threadIdx.x; t < 2 * np; t += 128) ls[t] = kept[q0 + min(t, n - 1)];
+        store_codes(cp, cv);
+        if (q0 + SKFR_ACHUNK < p1)
+            cv = load_codes(bed, pitch, i0, kept, q0 + SKFR_ACHUNK, (int)min((int64_t)SKFR_ACHUNK, p1 - q0 - SKFR_ACHUNK));
         __syncthreads();
         if (i < I) {
-            int pp = 0;
-            for (; pp + 4 <= np; pp += 4) {
-                uint32_t c[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) c[u] = base[(size_t)ls[2 * pp + u] * pitch];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int cp = (int)(((c[2 * u] >> sh) & 3u) * 4 + ((c[2 * u + 1] >> sh) & 3u));
-                    const double *tp = ts + ((pp + u) * 16 + cp) * KS;
-#pragma unroll
-                    for (int k = 0; k < K; ++k) acc[k] = __dadd_rn(acc[k], tp[k]);
-                }
-            }
-            for (; pp < np; ++pp) {
-                const uint32_t c0 = base[(size_t)ls[2 * pp] * pitch], c1 = base[(size_t)ls[2 * pp + 1] * pitch];
-                const double *tp = ts + (pp * 16 + (int)(((c0 >> sh) & 3u) * 4 + ((c1 >> sh) & 3u))) * KS;
+#pragma unroll 4
+            for (int pp = 0; pp < np; ++pp) {
+                /* an odd last position is paired with itself: its table ignores the second code */
+                const uint32_t v = *(const uint16_t *)&cp[pp][cb];
+                const double *tp = ts + (pp * 16 + (int)(((v >> sh) & 3u) * 4u + ((v >> (sh + 8)) & 3u))) * KS;
 #pragma unroll
                 for (int k = 0; k < K; ++k) acc[k] = __dadd_rn(acc[k], tp[k]);
             }
@@ -513,36 +529,30 @@ k_skfr_assign_own(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, con
                   int64_t nkept, int K, const double *__restrict__ pt, double *__restrict__ part)
 {
     __shared__ double ts[(SKFR_ACHUNK / 2) * 16];
-    __shared__ int32_t ls[SKFR_ACHUNK];
+    __shared__ __align__(16) uint8_t cp[SKFR_ACHUNK / 2][64];
     const int k = blockIdx.z;
     const int64_t npair = (nkept + 1) / 2;
-    const int64_t i = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.x * 128, i = i0 + threadIdx.x;
     const int64_t p0 = (int64_t)blockIdx.y * SKFR_ASLICE, p1 = min(nkept, p0 + SKFR_ASLICE);
-    const int sh = (int)(i & 3) * 2;
-    const uint8_t *base = bed + (size_t)(i >> 2);
+    const int sh = (int)(threadIdx.x & 3) * 2, cb = 2 * (int)(threadIdx.x >> 2);
     const int32_t *kl = kept + (size_t)k * nkept;
     const double *tk = pt + (size_t)k * npair * 16;
     double acc = 0.0;
+    uint2 cv = load_codes(bed, pitch, i0, kl, p0, (int)min((int64_t)SKFR_ACHUNK, p1 - p0));
     for (int64_t q0 = p0; q0 < p1; q0 += SKFR_ACHUNK) {
         const int n = (int)min((int64_t)SKFR_ACHUNK, p1 - q0), np = (n + 1) / 2;
         const int64_t r0 = q0 / 2;
         __syncthreads();
         for (int t = threadIdx.x; t < np * 16; t += 128) ts[t] = tk[r0 * 16 + t];
-        for (int t = threadIdx.x; t < 2 * np; t += 128) ls[t] = kl[q0 + min(t, n - 1)];
+        store_codes(cp, cv);
+        if (q0 + SKFR_ACHUNK < p1)
+            cv = load_codes(bed, pitch, i0, kl, q0 + SKFR_ACHUNK, (int)min((int64_t)SKFR_ACHUNK, p1 - q0 - SKFR_ACHUNK));
         __syncthreads();
         if (i < I) {
-            int pp = 0;
-            for (; pp + 4 <= np; pp += 4) {
-                uint32_t c[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) c[u] = base[(size_t)ls[2 * pp + u] * pitch];
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    acc = __dadd_rn(acc, ts[(pp + u) * 16 + (int)(((c[2 * u] >> sh) & 3u) * 4 + ((c[2 * u + 1] >> sh) & 3u))]);
-            }
-            for (; pp < np; ++pp) {
-                const uint32_t c0 = base[(size_t)ls[2 * pp] * pitch], c1 = base[(size_t)ls[2 * pp + 1] * pitch];
-                acc = __dadd_rn(acc, ts[pp * 16 + (int)(((c0 >> sh) & 3u) * 4 + ((c1 >> sh) & 3u))]);
+#pragma unroll 4
+            for (int pp = 0; pp < np; ++pp) {
+                const uint32_t v = *(const uint16_t *)&cp[pp][cb];
+                acc = __dadd_rn(acc, ts[pp * 16 + (int)(((v >> sh) & 3u) * 4u + ((v >> (sh + 8)) & 3u))]);
             }
         }
     }
