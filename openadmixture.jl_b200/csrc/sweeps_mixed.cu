@@ -32,6 +32,11 @@ constexpr uint32_t MX_WAIT_LIMIT = 1u << 22;   /* polls; an MMA batch completes 
  * the row's FP64 partials and the next MMA starts a fresh sum, so no FP32 partial sum sees more
  * than 4 * MX_HBLOCK MMA accumulations (whose rounding is not to nearest) whatever J or I is. */
 constexpr int MX_HBLOCK = 256;
+/* The Hessian diagonal columns and the gradient accumulator are read into FP64 (and the diagonal
+ * cleared) every MX_DRAIN chunks: each such FP32 sum covers at most 4 * MX_DRAIN accumulations.
+ * MX_HBLOCK is a multiple of MX_DRAIN, so a block drain always follows a diagonal drain. */
+constexpr int MX_DRAIN = 2;
+static_assert(MX_HBLOCK % MX_DRAIN == 0, "block drains coincide with diagonal drains");
 
 /* Column order of the Hessian accumulators (T = K (K + 1) / 2 pairs): the K diagonal pairs first
  * (column k = pair (k, k)), then the off-diagonal pairs (a, b), b < a, in the packed order of the
@@ -59,7 +64,7 @@ __device__ __forceinline__ void col_pair(int K, int col, int &ka, int &kb)
 }
 
 /* add (or, for the first block, store) the Hessian accumulator's columns K .. T+K-1 (off-diagonal
- * pairs and diagonal residuals; the diagonal columns 0..K-1 are drained every chunk) of this
+ * pairs and diagonal residuals; the diagonal columns 0..K-1 are drained every MX_DRAIN chunks) of this
  * thread's lane into the FP64 entries o[col_out(K, e)] */
 template <int K, int N, int T>
 __device__ __forceinline__ void hess_drain(uint32_t taddr, double *o, bool first, bool valid)
@@ -143,16 +148,16 @@ __device__ __forceinline__ uint4 interleave8(uint2 a, uint2 b)
  *   gradient   D[128 x NDG] = dz_hi * [p_hi | p_lo]^T + dz_lo * [p_hi | 0]^T, the gradient sum_j dz p_k
  *              with dz = z1 - z2 and both factors split into two BF16 parts (hi*hi + lo*hi in
  *              columns 0..K-1, hi*lo in K..2K-1: about 2^-17 relative), a fresh FP32 sum every
- *              chunk that the producers add into FP64;
+ *              MX_DRAIN chunks that the producers add into FP64;
  * and on the CUDA cores, per cell: the code lookup, one reciprocal, z1, z2, w1, w2, dz and its
  * split, and sum_j z2 (FP32 per chunk, FP64 across chunks).  The gradient is
  * sum_j (z1 - z2) p_k + z2 (= sum_j z1 p_k + z2 (1 - p_k)).
  *
  * The compensated diagonal: the tensor core's FP32 accumulation rounds toward zero, so a sum
- * carried over many chunks drifts low (about 5e-5 relative over 256 chunks).  After every chunk
- * the producers read the Hessian's K diagonal columns, add them into FP64 and store zeros back
- * (tcgen05.st), so each chunk's diagonal is a fresh FP32 sum of four accumulations carried on in
- * FP64.  The off-diagonal entries keep the MX_HBLOCK drains.
+ * carried over many chunks drifts low (about 5e-5 relative over 256 chunks).  Every MX_DRAIN
+ * chunks the producers read the Hessian's K diagonal columns, add them into FP64 and store zeros
+ * back (tcgen05.st), so the diagonal is a sum of fresh FP32 sums of 4 * MX_DRAIN accumulations
+ * carried on in FP64.  The off-diagonal entries keep the MX_HBLOCK drains.
  *
  * Everything that depends on P alone -- the BF16 pair-product tiles, the TF32 hi / lo split of
  * [p ; 1-p], the gradient B blocks -- is built once per sweep by k_q_pack, one "package" per
@@ -167,9 +172,10 @@ constexpr int MQ_THREADS = 128;    /* one thread per individual = accumulator ro
 #endif
 constexpr int MQ_NPKG = ADMIX_MQ_NPKG;   /* package buffers */
 
-/* The gradient accumulator of a chunk: NDG columns, sum_j dz_hi p_hi + dz_lo p_hi in columns 0..K-1
- * and sum_j dz_hi p_lo in columns K..2K-1.  It starts afresh every chunk and the producers add it
- * into FP64, so no FP32 partial of the gradient sees more than one chunk's accumulations. */
+/* The gradient accumulator: NDG columns, sum_j dz_hi p_hi + dz_lo p_hi in columns 0..K-1 and
+ * sum_j dz_hi p_lo in columns K..2K-1.  It starts afresh every MX_DRAIN chunks and the producers
+ * add it into FP64, so no FP32 partial of the gradient sees more than MX_DRAIN chunks'
+ * accumulations. */
 template <int K> struct DGShape {
     static constexpr int NDG = K <= 8 ? 16 : 32;
 };
@@ -229,18 +235,24 @@ __device__ __forceinline__ void bf16_split(float x, uint16_t &hi, uint16_t &lo)
     lo = (uint16_t)(pack_bf16x2(r, 0.f) & 0xFFFFu);
 }
 
-/* BF16 pair of non-negative x, y rounded with dither: the 16 dropped bits plus d (< 2^16) carry into
- * the kept ones, so x rounds up with probability (dropped bits + d) / 2^16 -- without bias when d
- * is uniform on [0, 2^16) and independent of x.  Round to nearest is biased for these operands:
- * applied to the Hessian weights it biased the BF16 Hessian diagonal by -3e-6 (Q side) and
- * -4.5e-5 (P side) relative, the same in an exact-arithmetic emulation of the rounding alone. */
-__device__ __forceinline__ uint32_t pack_bf16x2_dither(float x, float y, uint32_t dx, uint32_t dy)
+/* BF16 pair (x in the low half) of non-negative x, y rounded with dither (stochastic rounding,
+ * the sm_100a conversion cvt.rs): rbits[15:0] are added below the 16 dropped bits of x and
+ * rbits[31:16] below those of y, and the sums are truncated, so x rounds up with probability
+ * (dropped bits + d) / 2^16 -- without bias when d is uniform on [0, 2^16) and independent of x.
+ * (Measured on a B200: identical, bit for bit, to adding d to the FP32 bit pattern and keeping
+ * the high 16 bits.)  Round to nearest is biased for these operands: applied to the Hessian
+ * weights it biased the BF16 Hessian diagonal by -3e-6 (Q side) and -4.5e-5 (P side) relative,
+ * the same in an exact-arithmetic emulation of the rounding alone. */
+__device__ __forceinline__ uint32_t pack_bf16x2_dither(float x, float y, uint32_t rbits)
 {
-    return __byte_perm(__float_as_uint(x) + dx, __float_as_uint(y) + dy, 0x7632);
+    uint32_t r;
+    asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(y), "f"(x), "r"(rbits));
+    return r;
 }
 
 /* Dither stream of one accumulator row: a 32-bit LCG stepped once per cell pair; the pair's two
- * cells use its high 16 bits and their complement modulo 2^16 (antithetic) */
+ * cells use its high 16 bits (first cell, rbits[15:0]) and their complement modulo 2^16 (second
+ * cell, rbits[31:16]: antithetic) */
 __device__ __forceinline__ uint32_t dither_seed(int64_t row, int64_t slice)
 {
     return (uint32_t)row * 2654435761u + (uint32_t)slice * 40503u + 12345u;
@@ -248,7 +260,7 @@ __device__ __forceinline__ uint32_t dither_seed(int64_t row, int64_t slice)
 __device__ __forceinline__ uint32_t dither_step(uint32_t &st)
 {
     st = st * 1664525u + 1013904223u;
-    return st >> 16;
+    return __byte_perm(st, st ^ 0x80000000u, 0x7632);
 }
 
 /* BF16 pair of the rounding residuals x - bf16(x), y - bf16(y) (bf16 rounding to nearest) */
@@ -360,21 +372,23 @@ __device__ __forceinline__ void issue_qp(uint32_t tmem, const uint8_t *sm, const
  * a_dz: the A tile DZ0 (DZ1 follows at +A_BYTES); b_base: the package's two gradient B blocks.
  * Shared by both sides (P side: p -> q). */
 template <int K, uint32_t A_BYTES, uint32_t A_LBO, uint32_t DGB_BYTES, uint32_t DG_LBO>
-__device__ __forceinline__ void issue_grad(uint32_t tmem_dg, uint32_t a_dz, uint32_t b_base, int ks)
+__device__ __forceinline__ void issue_grad(uint32_t tmem_dg, uint32_t a_dz, uint32_t b_base, int ks, uint32_t first_acc)
 {
     constexpr uint32_t id = idesc_bf16_f32(128, DGShape<K>::NDG);
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
         const uint64_t ad = umma_desc_kmajor(a_dz + t * A_BYTES + ks * 2 * A_LBO, A_LBO, 128);
         const uint64_t bd = umma_desc_kmajor(b_base + t * DGB_BYTES + ks * 2 * DG_LBO, DG_LBO, 128);
-        tc_mma_bf16(tmem_dg, ad, bd, id, (t > 0 || ks > 0) ? 1u : 0u);
+        tc_mma_bf16(tmem_dg, ad, bd, id, (t > 0 || ks > 0) ? 1u : first_acc);
     }
 }
 
 /* Warp roles: warps 0-3 are producers (thread = accumulator row), warp 4 is the controller
  * (bulk copies, genotype staging, MMA issue).  No CTA-wide barrier inside the chunk loop: the
  * roles hand off through mbarriers.  Every wait is bounded; after a failed wait a thread sets
- * the shared abort flag and both roles run to the end without waiting. */
+ * the shared abort flag and both roles run to the end without waiting.  The controller issues
+ * the global loads of a chunk's genotypes one chunk before it stages them, so their latency does
+ * not hold up its MMA issue (Q sweep at I=200k, J=100k, K=8: 27.8 -> 25.7 ms). */
 constexpr int MQ_CTA = MQ_THREADS + 32;
 
 template <int K>
@@ -457,15 +471,19 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
         /* ---------------------------------------------------------------- controller warp */
         const bool leader = lane == 0;
         /* genotypes of chunk c into G buffer c & 1: lane l loads SNP jc + l (32 bytes: the CTA's 128
-         * individuals); lanes 2m, 2m+1 exchange and write pair m interleaved as [byte][2] */
-        auto stage_g = [&](int c) {
+         * individuals) into a0 / a1 one chunk before the staging, where lanes 2m, 2m+1 exchange and
+         * write pair m interleaved as [byte][2] */
+        uint4 a0 = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), a1 = a0;
+        auto load_g = [&](int c) {
             const int64_t jc = j0 + (int64_t)c * MQ_JC;
-            uint4 a0 = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u), a1 = a0;
+            a0 = a1 = make_uint4(0x55555555u, 0x55555555u, 0x55555555u, 0x55555555u);
             if (jc + lane < j1) {
                 const uint4 *src = (const uint4 *)(bed + (size_t)(jc + lane) * pitch + (size_t)(i0 / 4));
                 a0 = __ldg(src);
                 a1 = __ldg(src + 1);
             }
+        };
+        auto stage_g = [&](int c) {   /* the loaded genotypes of chunk c */
             uint4 b0, b1;                                   /* the partner lane's bytes */
             b0.x = __shfl_xor_sync(0xffffffffu, a0.x, 1); b0.y = __shfl_xor_sync(0xffffffffu, a0.y, 1);
             b0.z = __shfl_xor_sync(0xffffffffu, a0.z, 1); b0.w = __shfl_xor_sync(0xffffffffu, a0.w, 1);
@@ -488,8 +506,9 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             }
         };
         for (int c = 0; c < min(nchunk, MQ_NPKG); ++c) copy_pkg(c);
-        if (nchunk > 0) stage_g(0);
-        if (nchunk > 1) stage_g(1);
+        if (nchunk > 0) { load_g(0); stage_g(0); }
+        if (nchunk > 1) { load_g(1); stage_g(1); }
+        if (nchunk > 2) load_g(2);
         if (nchunk > 0 && wait(&bar_p[0], 0u) && leader) {
             tc_fence_after_sync();
             issue_qp<K>(tmem, sm, sm + C::OFF_PKG);
@@ -508,7 +527,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || term > 0 || ks > 0) ? 1u : 0u);
             }
             issue_grad<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase + 2 * C::A_BYTES,
-                                                                         bbase + C::PK_DG, ks);
+                                                                         bbase + C::PK_DG, ks, (c % MX_DRAIN != 0) ? 1u : 0u);
         };
         for (int c = 0; c < nchunk && ok; ++c) {
             /* the first K-step (SNPs 0-15) of chunk c as soon as the producers wrote it, so its MMAs
@@ -535,6 +554,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                 }
                 /* the producers are done with G buffer c & 1: stage chunk c+2 into it */
                 if (c + 2 < nchunk) stage_g(c + 2);
+                if (c + 3 < nchunk) load_g(c + 3);
             }
             /* package c is free once the MMAs of chunk c are done: fetch chunk c+NPKG into it */
             if (c + MQ_NPKG < nchunk && wait(bar_h, (uint32_t)(c & 1))) {
@@ -610,9 +630,9 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     const float2 w1 = __fmul2_rn(z1, r1), w2 = __fmul2_rn(z2, r2);
                     const float2 dz = __ffma2_rn(z2, make_float2(-1.f, -1.f), z1);
                     zs = __fadd2_rn(zs, z2);
-                    const uint32_t d0 = dither_step(dst), d1 = d0 ^ 0x8000u;
-                    w1p[e] = pack_bf16x2_dither(w1.x, w1.y, d0, d1);
-                    w2p[e] = pack_bf16x2_dither(w2.x, w2.y, d0, d1);
+                    const uint32_t rb = dither_step(dst);
+                    w1p[e] = pack_bf16x2_dither(w1.x, w1.y, rb);
+                    w2p[e] = pack_bf16x2_dither(w2.x, w2.y, rb);
                     /* dz = hi + lo in BF16: hi rounded to nearest, lo the BF16 of the remainder */
                     const uint32_t h = pack_bf16x2(dz.x, dz.y);
                     const float2 hf = make_float2(__uint_as_float(h << 16), __uint_as_float(h & 0xFFFF0000u));
@@ -628,7 +648,7 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     /* all of chunk c-1's MMAs are done: its diagonal and gradient sums (and, at a block
                      * boundary, the Hessian block), and the A tiles' second half is free */
                     if (c > 0 && wait(bar_h, (uint32_t)((c - 1) & 1))) {
-                        drain_dg();
+                        if (c % MX_DRAIN == 0) drain_dg();
                         if (c % MX_HBLOCK == 0) {   /* the Hessian block of chunks c-MX_HBLOCK .. c-1 */
                             tc_fence_after_sync();
                             hess_drain<K, N, T>(tmem + lane_base + C::COL_H,
@@ -712,9 +732,10 @@ k_sweep_q_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
  * chunks of 32 individuals.  Per chunk:
  *   qp, om     D[128 x 32] = Ptile * Qchunk^T and (1-P)tile * Qchunk^T, TF32 split form;
  *   Hessian    D[128 x N] += C * QQ^T in BF16, C = nm (g/qp^2 + (2-g)/(1-qp)^2), diagonal pairs
- *              in the first K columns, read, added into FP64 and cleared after every chunk;
+ *              in the first K columns, read, added into FP64 and cleared every MX_DRAIN chunks;
  *   gradient   D[128 x NDG] = dz_hi * [q_hi | q_lo]^T + dz_lo * [q_hi | 0]^T (the gradient
- *              sum_i dz q_k, dz = nm (g/qp - (2-g)/(1-qp))), afresh every chunk and added into FP64;
+ *              sum_i dz q_k, dz = nm (g/qp - (2-g)/(1-qp))), afresh every MX_DRAIN chunks and
+ *              added into FP64;
  * and per cell on the CUDA cores the code (from the thread's own genotype word), one reciprocal,
  * C, dz and its BF16 split.  The Q-derived tiles of each chunk (QQ in BF16, Q split into TF32
  * hi / lo, the gradient B blocks, q in FP32 for the EM mode) are built once per sweep by
@@ -982,7 +1003,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
             const uint64_t bd = umma_desc_kmajor(bbase + ks * 2 * C::B_LBO, C::B_LBO, C::B_SBO);
             tc_mma_bf16(tmem + C::COL_H, ad, bd, idesc, (c % MX_HBLOCK != 0 || ks > 0) ? 1u : 0u);
             issue_grad<K, C::A_BYTES, C::A_LBO, C::DGB_BYTES, C::DG_LBO>(tmem + C::COL_DG, abase + C::A_BYTES,
-                                                                         bbase + C::PK_DG, ks);
+                                                                         bbase + C::PK_DG, ks, (c % MX_DRAIN != 0) ? 1u : 0u);
         };
         for (int c = 0; c < nchunk && ok; ++c) {
             if constexpr (!EMS) {   /* the first K-step (individuals 0-15) as soon as it is written */
@@ -1096,8 +1117,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     } else {
                         const float2 cw = __ffma2_rn(z1, r1, __fmul2_rn(z2, r2));   /* nm (g/qp^2 + (2-g)/(1-qp)^2) */
                         const float2 dz = __ffma2_rn(z2, make_float2(-1.f, -1.f), z1);   /* nm (g/qp - (2-g)/(1-qp)) */
-                        const uint32_t d0 = dither_step(dst);
-                        cp[e] = pack_bf16x2_dither(cw.x, cw.y, d0, d0 ^ 0x8000u);
+                        cp[e] = pack_bf16x2_dither(cw.x, cw.y, dither_step(dst));
                         /* dz = hi + lo in BF16: hi rounded to nearest, lo the BF16 of the remainder */
                         const uint32_t h = pack_bf16x2(dz.x, dz.y);
                         const float2 hf = make_float2(__uint_as_float(h << 16), __uint_as_float(h & 0xFFFF0000u));
@@ -1112,7 +1132,7 @@ k_sweep_p_mixed(const uint8_t *__restrict__ bed, int64_t I, int64_t J, int64_t p
                     *(uint4 *)(At + 2 * C::A_BYTES + kc * C::A_LBO + 16 * tid) = make_uint4(d1p[0], d1p[1], d1p[2], d1p[3]);
                     if (kc == 1) {   /* as on the Q side: drain chunk c-1, then release the first K-step */
                         if (c > 0 && wait(bar_h, (uint32_t)((c - 1) & 1))) {
-                            drain_dg();
+                            if (c % MX_DRAIN == 0) drain_dg();
                             if (c % MX_HBLOCK == 0) {
                                 tc_fence_after_sync();
                                 hess_drain<K, N, T>(tmem + lane_base + C::COL_H,
