@@ -51,8 +51,8 @@ extern "C" {
 #define ADMIX_FLAG_MIXED          2u  /* mixed-precision form: the iteration's Q/P gradient / Hessian
                                           sweeps (tcgen05 BF16 Hessians, FP32 gradient cells, FP64
                                           sums), its log-likelihoods (FP32 cells, FP64 reduction) and
-                                          admix_init_em's EM sums; admix_loglik, admix_em_q/_p, the
-                                          QPs and the QN step stay FP64.  A mixed call whose
+                                          admix_init_em's EM sums and its final ll_new; admix_loglik,
+                                          admix_em_q/_p, the QPs and the QN step stay FP64.  A mixed call whose
                                           tensor-core pipeline wait runs out returns ADMIX_ERR_CUDA. */
 
 #define ADMIX_FLAG_MEAN_IMPUTE    4u  /* AdmixData(...; skipmissing=false) (structs.jl:105): the loops
@@ -131,7 +131,8 @@ int admix_loglik(admix_ctx *h, int32_t which, double *out);
 int admix_em_q(admix_ctx *h);
 int admix_em_p(admix_ctx *h);
 /* init_em! (algorithms_outer.jl:12-45): `iters` EM iterations, ll_hist[iters] (may be NULL),
- * then sets ll_new. */
+ * then sets ll_new (with ADMIX_FLAG_MIXED from the mixed log-likelihood pass that the iterations
+ * use, not from admix_loglik's FP64 pass). */
 int admix_init_em(admix_ctx *h, int32_t iters, double *ll_hist);
 
 /* Gradient / Hessian sweep of the Q block at (q of which_q, p of which_p), written to the

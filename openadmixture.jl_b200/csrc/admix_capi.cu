@@ -627,7 +627,13 @@ static int enq_init_em(admix_ctx *h, int32_t iters, double *ll_hist)
             CK(h, cudaMemcpyAsync(ll_hist + it, &h->sc->ll_tmp, sizeof(double), cudaMemcpyDeviceToHost, h->st));
         }
     }
-    CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new));   /* FP64: the first QN iteration's ll_prev */
+    /* the first QN iteration's ll_prev, from the same pass as the iteration's own log-likelihoods
+     * (the mixed pass in the mixed form: -1.5e-9 relative from the FP64 pass, at C5 0.05 s
+     * instead of 0.58 s); the last reported value is that pass at the same point */
+    if (ll_hist && iters > 0)
+        CK(h, cudaMemcpyAsync(&h->sc->ll_new, &h->sc->ll_tmp, sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    else
+        CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new, true));
     return ADMIX_OK;
 }
 
@@ -802,8 +808,8 @@ int admix_run_qn(admix_ctx *h, int32_t n_iter, double rtol, int32_t iter_offset,
     if (iter_offset < 0) return fail(h, ADMIX_ERR_ARG, "iter_offset must be >= 0");
     int rc = read_scalars(h);
     if (rc != ADMIX_OK) return rc;
-    if (isnan(h->sc_host->ll_new)) {   /* algorithms_outer.jl:76-83 */
-        CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new));
+    if (isnan(h->sc_host->ll_new)) {   /* algorithms_outer.jl:76-83 (the iteration's own pass) */
+        CK(h, enq_loglik(h, ADMIX_X, &h->sc->ll_new, true));
         CK(h, cudaStreamSynchronize(h->st));
     }
     int done = 0, conv = 0;
@@ -1261,7 +1267,7 @@ int admix_batch_run_qn(admix_batch *b, int32_t n_iter, double rtol, int32_t *n_d
     for (admix_ctx *h : b->m) {
         BCK(b, cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
         BCK(b, cudaStreamSynchronize(h->st));
-        if (isnan(h->sc_host->ll_new)) BCK(b, enq_loglik(h, ADMIX_X, &h->sc->ll_new));
+        if (isnan(h->sc_host->ll_new)) BCK(b, enq_loglik(h, ADMIX_X, &h->sc->ll_new, true));
     }
     rc = batch_sync_members(b);
     if (rc != ADMIX_OK) return rc;
