@@ -1658,21 +1658,56 @@ SweepPlan plan_rows(int64_t rows, int64_t cols, int sms, int per_sm, int64_t uni
     return pl;
 }
 
-/* resident CTAs per SM of the mixed kernels (occupancy at their shared memory; needs
- * prepare_mixed(K) first), cached per kernel and K; `fallback` when it cannot be queried */
-template <int K>
-int resident_t(int kind)
+/* Resident CTAs per SM of one kernel, from its registers (allocated per warp in units of 256),
+ * its static and dynamic shared memory (plus the per-CTA reservation), its threads and its tensor
+ * memory columns (512 per SM).  The occupancy query answered one CTA per SM for all three mixed
+ * kernels on a B200 while three (sweeps) and four (log-likelihood) run, as ncu's active warps
+ * show, so the plans use this count, or the query's if that is larger.  0 when the kernel's
+ * attributes cannot be read. */
+template <typename F>
+int resident_est(F *kern, int threads, uint32_t dyn_smem, uint32_t tmem_cols)
 {
-    int n = 0;
-    cudaError_t e;
-    if (kind == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_q_mixed<K>, MQ_CTA, MQ<K>::SMEM);
-    else if (kind == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_p_mixed<K, false>, MP_CTA, MP<K>::SMEM);
-    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_loglik_mixed<K>, LT_CTA, LT<K>::SMEM);
-    if (e != cudaSuccess) {
+    cudaFuncAttributes a;
+    int dev = 0, regs_sm = 0, smem_sm = 0, thr_sm = 0, res_blk = 0;
+    if (cudaFuncGetAttributes(&a, kern) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&res_blk, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    return n;
+    const int warps = (threads + 31) / 32;
+    const int regs_warp = (a.numRegs * 32 + 255) / 256 * 256;
+    int n = thr_sm / threads;
+    if (regs_warp > 0) n = std::min(n, regs_sm / regs_warp / warps);
+    n = std::min(n, smem_sm / (int)(a.sharedSizeBytes + dyn_smem + (size_t)res_blk));
+    n = std::min(n, (int)(512u / tmem_cols));
+    return std::max(n, 0);
+}
+
+/* resident CTAs per SM of the mixed kernels (needs prepare_mixed(K) first), cached per kernel
+ * and K; 0 when it cannot be determined */
+template <int K>
+int resident_t(int kind)
+{
+    int n = 0, est = 0;
+    cudaError_t e;
+    if (kind == 0) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_q_mixed<K>, MQ_CTA, MQ<K>::SMEM);
+        est = resident_est(k_sweep_q_mixed<K>, MQ_CTA, MQ<K>::SMEM, MQ<K>::NCOLS);
+    } else if (kind == 1) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sweep_p_mixed<K, false>, MP_CTA, MP<K>::SMEM);
+        est = resident_est(k_sweep_p_mixed<K, false>, MP_CTA, MP<K>::SMEM, MP<K>::NCOLS);
+    } else {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_loglik_mixed<K>, LT_CTA, LT<K>::SMEM);
+        est = resident_est(k_loglik_mixed<K>, LT_CTA, LT<K>::SMEM, LT<K>::NCOLS);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    return std::max(n, est);
 }
 
 int resident(int kind, int K, int fallback)
@@ -1698,16 +1733,18 @@ cudaError_t prepare_mixed(int K)
     return e;
 }
 
-/* One CTA per 128 individuals and SNP slice. */
+/* One CTA per 128 individuals and SNP slice.  Slices are multiples of MX_DRAIN chunks, so the
+ * chunks whose FP32 gradient and diagonal sums are drained together are the same pairs for every
+ * split, and another split (batch autotuning) only regroups FP64 sums. */
 SweepPlan plan_sweep_q_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax)
 {
-    return plan_rows(I, J, sms, resident(0, K, 3), MQ_JC, smax);
+    return plan_rows(I, J, sms, resident(0, K, 3), (int64_t)MX_DRAIN * MQ_JC, smax);
 }
 
-/* One CTA per 128 SNPs and individual slice (slices are multiples of 64 individuals). */
+/* One CTA per 128 SNPs and individual slice (slices are multiples of MX_DRAIN chunks, as above). */
 SweepPlan plan_sweep_p_mixed(int K, int64_t I, int64_t J, int sms, int64_t smax)
 {
-    return plan_rows(J, I, sms, resident(1, K, 3), MP_IC, smax);
+    return plan_rows(J, I, sms, resident(1, K, 3), (int64_t)MX_DRAIN * MP_IC, smax);
 }
 
 /* One CTA per 128 SNPs and individual slice (slices are multiples of 32 individuals). */
