@@ -371,37 +371,63 @@ cudaError_t colsum(const float *dY, int64_t M, int64_t N, float *db, cudaStream_
 }
 
 /* closed-form P step from Q: p_kj = sum_i nm q_ki g_ij / (2 sum_i nm q_ki), clamped to
- * [1e-5, 1-1e-5] like project_p! (projections.jl:69-74).  Thread = SNP, q staged 64 at a time. */
+ * [1e-5, 1-1e-5] like project_p! (projections.jl:69-74).  Thread = SNP; q staged through shared
+ * memory 64 individuals at a time as (k, k+1) pairs, both sums accumulated in FP32 pairs (one
+ * paired FMA per k pair and cell); a missing cell adds zeros, so no thread branches on the
+ * genotype, and one byte load serves four cells.  Each sum is the same per-k FP32 sequence as
+ * a per-cell loop that skips the missing cells. */
 template <int K>
 __global__ void __launch_bounds__(128)
 k_warm_p(const uint8_t *__restrict__ bed, int64_t pitch, int64_t I, int64_t J, const double *__restrict__ q,
          double *__restrict__ p)
 {
-    __shared__ float qs[64 * K];
+    constexpr int KH = (K + 1) / 2;                  /* k pairs (odd K: the last pair's second half is 0) */
+    __shared__ __align__(16) float2 qs[64 * KH];
     const int64_t j = (int64_t)blockIdx.x * 128 + threadIdx.x;
-    float num[K], den[K];
+    const uint8_t *col = bed + (size_t)(j < J ? j : 0) * pitch;
+    float2 num[KH], den[KH];   /* sum_i q_ki g_ij and sum_i nm q_ki */
 #pragma unroll
-    for (int k = 0; k < K; ++k) { num[k] = 0.f; den[k] = 0.f; }
+    for (int kh = 0; kh < KH; ++kh) num[kh] = den[kh] = make_float2(0.f, 0.f);
     for (int64_t i0 = 0; i0 < I; i0 += 64) {
         const int n = (int)min((int64_t)64, I - i0);
         __syncthreads();
-        for (int t = threadIdx.x; t < n * K; t += 128) qs[t] = (float)q[(size_t)K * i0 + t];
+        for (int t = threadIdx.x; t < 64 * KH; t += 128) {
+            const int ii = t / KH, k = 2 * (t - ii * KH);
+            float a = 0.f, b = 0.f;
+            if (ii < n) {
+                a = (float)q[(size_t)K * (i0 + ii) + k];
+                if (k + 1 < K) b = (float)q[(size_t)K * (i0 + ii) + k + 1];
+            }
+            qs[t] = make_float2(a, b);
+        }
         __syncthreads();
         if (j < J) {
-            for (int ii = 0; ii < n; ++ii) {
-                const int64_t i = i0 + ii;
-                const int c = (bed[(size_t)j * pitch + (i >> 2)] >> ((i & 3) << 1)) & 3;
-                if (c == 1) continue;
-                const float g = c == 0 ? 0.f : (float)(c - 1);
+            for (int ib = 0; 4 * ib < n; ++ib) {
+                const uint32_t byte = col[(size_t)(i0 >> 2) + ib];
 #pragma unroll
-                for (int k = 0; k < K; ++k) { num[k] = fmaf(qs[ii * K + k], g, num[k]); den[k] += 2.f * qs[ii * K + k]; }
+                for (int t = 0; t < 4; ++t) {
+                    const int ii = 4 * ib + t;
+                    if (ii >= n) break;
+                    const uint32_t c = (byte >> (2 * t)) & 3u;
+                    const float g = c == 3u ? 2.f : (c == 2u ? 1.f : 0.f);   /* codes 00 -> 0, 10 -> 1, 11 -> 2 */
+                    const float nm = c == 1u ? 0.f : 1.f;                    /* 01: missing */
+                    const float2 g2 = make_float2(g, g), n2 = make_float2(nm, nm);
+#pragma unroll
+                    for (int kh = 0; kh < KH; ++kh) {
+                        const float2 qv = qs[ii * KH + kh];
+                        num[kh] = __ffma2_rn(qv, g2, num[kh]);
+                        den[kh] = __ffma2_rn(qv, n2, den[kh]);
+                    }
+                }
             }
         }
     }
     if (j < J)
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const double v = den[k] > 0.f ? (double)num[k] / (double)den[k] : 0.5;
+            const float nk = (k & 1) ? num[k >> 1].y : num[k >> 1].x;
+            const float dk = 2.f * ((k & 1) ? den[k >> 1].y : den[k >> 1].x);
+            const double v = dk > 0.f ? (double)nk / (double)dk : 0.5;
             p[(size_t)K * j + k] = fmin(fmax(v, 1e-5), 1.0 - 1e-5);
         }
 }
