@@ -534,9 +534,10 @@ def run_ours(args, rank, world, local_rank):
         roof["tensor_peak_tflops"] = bf16_sus
         roof["tensor_frac"] = roof["tensor_tflops"] / bf16_sus
         roof["note"] = ("mixed form: the Hessian contraction runs on tcgen05 (tensor_tflops against the "
-                        "sustained bf16 peak: tensor_frac); the sweep is bound by the FP32 producer work per "
-                        "cell on the CUDA cores, not by HBM or the tensor pipe; frac is the HBM fraction of "
-                        "its packed-genotype stream")
+                        "sustained bf16 peak: tensor_frac); the sweep is bound by the per-chunk hand-offs "
+                        "between the producer warps' FP32 cell work, the controller's MMA issue and the "
+                        "tensor core (issue activity about 55 %), not by HBM or the tensor pipe; frac is the "
+                        "HBM fraction of its packed-genotype stream")
     if args.stream_block:
         # 6 genotype passes per iteration, each streamed host -> device once
         roof["stream_h2d_gbs"] = 6 * bytes_bed / (ms_max / args.steps / 1e3) / 1e9
