@@ -167,10 +167,7 @@ __device__ __forceinline__ uint4 interleave8(uint2 a, uint2 b)
 
 constexpr int MQ_JC = 32;          /* SNPs per chunk = 2 BF16 MMA K-steps */
 constexpr int MQ_THREADS = 128;    /* one thread per individual = accumulator row */
-#ifndef ADMIX_MQ_NPKG
-#define ADMIX_MQ_NPKG 2
-#endif
-constexpr int MQ_NPKG = ADMIX_MQ_NPKG;   /* package buffers */
+constexpr int MQ_NPKG = 2;   /* package buffers (a third one leaves room for two CTAs per SM only: slower) */
 
 /* The gradient accumulator: NDG columns, sum_j dz_hi p_hi + dz_lo p_hi in columns 0..K-1 and
  * sum_j dz_hi p_lo in columns K..2K-1.  It starts afresh every MX_DRAIN chunks and the producers
